@@ -1,0 +1,367 @@
+#!/usr/bin/env python
+"""Particle-pushes/s of the 512x512 3rd-order electrostatic PIC step.
+
+Workload (one "step" = one cycle of the reference's time loop: deposit,
+Poisson solve to 1e-8 relative residual, gather + Boris push + absorbing
+walls, compaction, density-restoring re-injection):
+  512 x 512 grid, 3rd-order B-spline weighting, x Dirichlet (phi = 0) with
+  absorbing particles, y periodic; electrons + Xe+ (m_i = 1836 * 131.29 m_e),
+  256 particles/cell/species (67.1 M each, 134 M total), Maxwellian loads
+  (Te = 10 eV, Ti = 0.1 eV), n = 5e10 cm^-3, dx = 0.5 Debye length,
+  Bz = 0.02 T, dt * w_pe = 0.05, flux-Maxwellian re-injection at x = 0 of
+  every absorbed particle. Seeded synthetic data (the reference's
+  splitmix64/PCG32 loader, master seed 0).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Prints one JSON line (rank 0). --impl reference times the reference's CPU
+algorithm (the C++ oracle restatement, OpenMP on all host cores) on a
+bounded sample of the same workload.
+"""
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+EC = 4.803204197e-10
+ME = 9.10938188e-28
+KB = 1.3806503e-16
+EV_K = 11604.0
+BYTES_PER_PUSH = 48  # read + write of cell, ox, oy, vx, vy, vz (6 x 4 B)
+METRIC = "particle-pushes/s incl. field solve"
+
+
+def workload(ppc=256, ngx=512, ngy=512, steps=1000, log_output=0):
+    n = 5e10
+    te_erg = 10.0 * 1.6021764262e-12
+    lam_d = math.sqrt(te_erg / (4 * math.pi * n * EC ** 2))
+    wpe = math.sqrt(4 * math.pi * n * EC ** 2 / ME)
+    dx = 0.5 * lam_d
+    dt = 0.05 / wpe
+    npart = ppc * ngx * ngy
+    src = [{"ParticleName": name, "GenerateType": "fluxMaxwellianAtXmin", "SrcSetMethod": "AbsorbedParticleNumber",
+            "GenerateTemp": t} for name, t in (("electron", 10.0), ("ion_Xe1", 0.1))]
+    return {
+        "FlagForEquation": {"Particle": 2, "EMField": 1, "MCCollision": 0},
+        "ParamForTimeIntegration": {"Start": 0, "End": steps, "TimeStep": dt, "LogOutput": log_output,
+                                    "ParticleOutput": 0, "FieldOutput": 0, "ProgressOutput": 0,
+                                    "ProjectName": "es512_o3", "RestartName": "es512_o3"},
+        "ParamForComputing": {"MaximumParticleNumber": int(npart * 1.02) + 4096, "ThreadGroupSize": 256,
+                              "MaxiterForPoisson": 100, "ToleranceForPoisson": 1e-8},
+        "ParamForField": {"NumberOfGridX": ngx, "NumberOfGridY": ngy, "GridSizeOfX": dx, "GridSizeOfY": dx,
+                          "InitializeTypeOfE": "Uniform", "AmplitudeOfE": [0.0, 0.0, 0.0],
+                          "InitializeTypeOfB": "Uniform", "AmplitudeOfB": [0.0, 0.0, 200.0],
+                          "WeightingOrder": 3, "BorisOrder": 2},
+        "ParamForParticle": [
+            {"ParticleName": "electron", "pNumSetMethod": "PtclNumPerCell", "pNumValue": ppc, "Charge": -EC,
+             "Mass": ME, "WeightSetMethod": "InitialNumDens", "WeightValue": n,
+             "GenerateType": "uniform-Gaussian", "InitialTemp": 10.0},
+            {"ParticleName": "ion_Xe1", "pNumSetMethod": "PtclNumPerCell", "pNumValue": ppc, "Charge": EC,
+             "Mass": 1836 * 131.29 * ME, "WeightSetMethod": "InitialNumDens", "WeightValue": n,
+             "GenerateType": "uniform-Gaussian", "InitialTemp": 0.1}],
+        "SourceForParticle": src,
+        "BoundaryConditionForParticle": [
+            {"RegionName": "Xmin", "BCType": "Delete"}, {"RegionName": "Xmax", "BCType": "Delete"},
+            {"RegionName": "Ymin", "BCType": "periodic"}, {"RegionName": "Ymax", "BCType": "periodic"}],
+        "BoundaryConditionForField": [
+            {"RegionName": "Xmin", "BCType": "Dirichlet", "Value": 0.0},
+            {"RegionName": "Xmax", "BCType": "Dirichlet", "Value": 0.0},
+            {"RegionName": "Ymin", "BCType": "periodic"}, {"RegionName": "Ymax", "BCType": "periodic"}],
+    }
+
+
+def config_block(ppc):
+    return {"workload": f"es-pic 512x512, order 3, Dirichlet-x absorbing + periodic-y, {ppc} ppc/species "
+                        f"({2 * ppc * 512 * 512 / 1e6:.1f} M particles), Bz 0.02 T, dt*wpe 0.05, "
+                        "flux re-injection at x=0, Poisson rel. residual 1e-8",
+            "grid": [512, 512], "weighting_order": 3, "ppc_per_species": ppc,
+            "particles": 2 * ppc * 512 * 512, "poisson_tol": 1e-8,
+            "l2": "inputs larger than L2 (particle state 3.2 GB per step)"}
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def load_traffic():
+    """DRAM bytes per pushed particle of the push kernel from the committed ncu summary."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "push_es512_o3_traffic.json")) as f:
+            return json.load(f)
+    except Exception:
+        return None
+
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+        self.t = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        if self.t:
+            self.t.join(timeout=2)
+        sm, smax, reasons, power = [], None, set(), []
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+                power.append(float(parts[3]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        sm.sort()
+        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm), "power_w_max": max(power) if power else None}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def cpu_baseline_run(steps, warmup, ppc_sample, threads=None):
+    """The oracle (C++ restatement of the reference's CPU arithmetic, OpenMP)
+    on the same grid/physics with ppc_sample particles per cell per species."""
+    from oracle import config as ocfg
+    from oracle import lib as L
+    cond = workload(ppc=ppc_sample)
+    sim = L.OracleSim(ocfg.parse(cond), real64=False)
+    sim.load_initial()
+    sim.reset_charge()
+    for s in range(2):
+        sim.deposit(s)
+    sim.solve_poisson(0.0)
+    for c in range(warmup):
+        sim.cycle(c + 1, faithful=False)
+    n0 = sim.pnum(0) + sim.pnum(1)
+    t0 = time.perf_counter()
+    for c in range(steps):
+        sim.cycle(warmup + c + 1, faithful=False)
+    el = time.perf_counter() - t0
+    n1 = sim.pnum(0) + sim.pnum(1)
+    pushes = 0.5 * (n0 + n1) * steps
+    return pushes / el, el, L.num_threads()
+
+
+def run_reference(args):
+    world, rank, _ = dist_setup()
+    if rank != 0:
+        return 0
+    ppc = args.ref_ppc
+    value, el, cores = cpu_baseline_run(args.steps, args.warmup, ppc)
+    line = {"metric": METRIC, "value": value, "unit": "particle-pushes/s", "impl": "reference",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * el / max(args.steps, 1), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded reference loader)",
+            "config": config_block(256),
+            "cpu_baseline": {"value": value, "unit": "particle-pushes/s", "cores": cores, "kind": "port",
+                             "sample": f"full 512x512 grid and field solve, {ppc} ppc/species "
+                                       f"({2 * ppc * 512 * 512 / 1e6:.1f} M particles) per step; the "
+                                       "reference's Metal/AMGCL build does not exist on Linux, so its CPU "
+                                       "algorithm is the oracle's C++ restatement"},
+            "e2e": {"value": value, "unit": "particle-pushes/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_b200(args):
+    world, rank, local = dist_setup()
+    import numpy as np
+    import torch
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        pg = dist
+    from gample_b200 import capi
+
+    def barrier():
+        if pg:
+            pg.barrier()
+        torch.cuda.synchronize()
+
+    ppc = args.ppc
+    cond = workload(ppc=ppc)
+    sim = capi.Sim(cond)
+    sim.initialize()
+    if args.warmup:
+        sim.run(args.warmup)
+    n0 = sim.count(0) + sim.count(1)
+    clocks = ClockSampler(local)
+    barrier()
+    clocks.start()
+    l0 = capi.kernel_launches()
+    ms = sim.time_cycles(args.steps)
+    launches = capi.kernel_launches() - l0
+    barrier()
+    clk = clocks.stop()
+    n1 = sim.count(0) + sim.count(1)
+    ms_max = ms
+    if pg:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        ms_max = float(t.item())
+    pushes_rank = 0.5 * (n0 + n1) * args.steps
+    value = pushes_rank * world / (ms_max / 1e3)
+
+    # Roofline of the dominant kernel (push + fused deposit): a few more
+    # cycles with per-phase CUDA events on the library's stream.
+    sim.set_profiling(True)
+    prof_cycles = max(2, min(5, args.steps))
+    sim.run(prof_cycles)
+    ph = sim.phase_times()
+    sim.set_profiling(False)
+    n_prof = sim.count(0) + sim.count(1)
+    push_ms_per_launch = ph["push"] / (2 * prof_cycles)
+    particles_per_launch = n_prof / 2
+    peak, peak_kind = load_peaks()
+    achieved = BYTES_PER_PUSH * particles_per_launch / (push_ms_per_launch / 1e3) / 1e9
+    tr = load_traffic()
+    traffic = tr["dram_bytes_per_particle"] * particles_per_launch if tr else None
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": traffic, "peak_kind": peak_kind, "kernel": "k_push (gather+Boris+BC+fused deposit)",
+                "algorithmic_bytes_per_particle": BYTES_PER_PUSH,
+                "phase_ms_per_step": {k: v / prof_cycles for k, v in ph.items()}}
+    sim.close()
+    del sim
+
+    # End to end through the C ABI with host buffers: restart-style upload of
+    # the initial particle state from pinned host memory, initial solve, K
+    # logged cycles (CSV/XML written every cycle), download of the final
+    # state to pinned host memory.
+    e2e = None
+    if rank == 0 or True:
+        src = capi.Sim(cond)
+        states = [src.particles(s) for s in range(2)]
+        src.close()
+        del src
+        pinned = []
+        for st in states:
+            t = torch.empty(st.nbytes, dtype=torch.uint8, pin_memory=True)
+            np.frombuffer(t.numpy(), dtype=np.uint8)[:] = st.view(np.uint8)
+            pinned.append((t, len(st)))
+        out_pinned = [torch.empty(int(st.nbytes * 1.02) + 4096 * 24, dtype=torch.uint8, pin_memory=True)
+                      for st in states]
+        with tempfile.TemporaryDirectory() as td:
+            c2 = dict(cond)
+            c2["ParamForTimeIntegration"] = dict(cond["ParamForTimeIntegration"], LogOutput=1)
+            barrier()
+            t0 = time.perf_counter()
+            sim2 = capi.Sim(c2, log_name=os.path.join(td, "es512"))
+            h2d = 0
+            for s, (t, n) in enumerate(pinned):
+                capi.check(capi.lib().gp_particle_upload(sim2.h, s, t.data_ptr(), n))
+                h2d += n * 24
+            sim2.initialize()
+            sim2.run(args.steps)
+            d2h = 0
+            for s in range(2):
+                n = sim2.count(s)
+                got = capi.C.c_uint32()
+                capi.check(capi.lib().gp_particle_download(sim2.h, s, out_pinned[s].data_ptr(),
+                                                           out_pinned[s].numel() // 24, capi.C.byref(got)))
+                d2h += got.value * 24
+            n_e2e = 0.5 * (sum(len(s) for s in states) + sim2.count(0) + sim2.count(1))
+            sim2.close()
+            el = time.perf_counter() - t0
+        # per-step diagnostics read back by the logger: solve stats (8 doubles)
+        # and two species counters (2 x 48 B)
+        diag = 64 + 96
+        e2e = {"value": n_e2e * args.steps * world / el, "unit": "particle-pushes/s",
+               "h2d_bytes_per_step": int(h2d / args.steps), "d2h_bytes_per_step": int(d2h / args.steps + diag),
+               "wall_s": el, "includes": "sim create + restart upload + initial solve + K logged cycles + "
+                                         "final download"}
+    cpu = None
+    if world == 1 and rank == 0 and not args.no_cpu_baseline:
+        v, el, cores = cpu_baseline_run(args.cpu_steps, 1, args.cpu_ppc)
+        cpu = {"value": v, "unit": "particle-pushes/s", "cores": cores, "kind": "port",
+               "sample": f"oracle C++ restatement, full 512x512 grid + Poisson (FP64 CG to 1e-8), "
+                         f"{args.cpu_ppc} ppc/species ({2 * args.cpu_ppc * 512 * 512 / 1e6:.1f} M particles), "
+                         f"{args.cpu_steps} steps after 1 warm-up step, {el:.1f} s"}
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "particle-pushes/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic (seeded reference loader, splitmix64/PCG32)", "config": config_block(ppc),
+                "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
+                "gpu_launches": launches, "gpu_launches_per_step": launches / args.steps,
+                "poisson": {"iterations_last_step": None}}
+        print(json.dumps(line), flush=True)
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--ppc", type=int, default=256)
+    ap.add_argument("--cpu-ppc", type=int, default=256)
+    ap.add_argument("--cpu-steps", type=int, default=2)
+    ap.add_argument("--ref-ppc", type=int, default=16)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_b200(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

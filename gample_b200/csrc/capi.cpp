@@ -1,0 +1,402 @@
+// capi.cpp -- extern "C" entry points declared in include/gample_gpu.h.
+#include <cstring>
+#include <exception>
+#include <string>
+
+#include "../../include/gample_gpu.h"
+#include "simulation.hpp"
+
+#include <atomic>
+
+namespace gample {
+namespace {
+std::atomic<unsigned long long> g_launches{0};
+}
+void note_kernel_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+unsigned long long kernel_launches() { return g_launches.load(std::memory_order_relaxed); }
+}  // namespace gample
+
+struct gp_init {
+  gample::Init init;
+};
+struct gp_sim {
+  std::unique_ptr<gample::Simulation> sim;
+};
+
+namespace {
+
+thread_local std::string g_error;
+
+template <typename F>
+gp_status guarded(F&& f) {
+  try {
+    return f();
+  } catch (const gample::ConfigError& e) {
+    g_error = e.what();
+    return GP_ERR_CONFIG;
+  } catch (const gample::CudaError& e) {
+    g_error = e.what();
+    return GP_ERR_CUDA;
+  } catch (const std::invalid_argument& e) {
+    g_error = e.what();
+    return GP_ERR_ARGUMENT;
+  } catch (const std::runtime_error& e) {
+    g_error = e.what();
+    return std::string(e.what()).find("pNum") != std::string::npos ? GP_ERR_CAPACITY : GP_ERR_INTERNAL;
+  } catch (const std::exception& e) {
+    g_error = e.what();
+    return GP_ERR_INTERNAL;
+  } catch (...) {
+    g_error = "unknown error";
+    return GP_ERR_INTERNAL;
+  }
+}
+
+gample::Particle* species(gp_sim* sim, int s) {
+  if (!sim || !sim->sim) throw std::invalid_argument("null simulation handle");
+  if (s < 0 || s >= int(sim->sim->ptrs.size())) throw std::invalid_argument("species index out of range");
+  return sim->sim->ptrs[s];
+}
+gample::Simulation& S(gp_sim* sim) {
+  if (!sim || !sim->sim) throw std::invalid_argument("null simulation handle");
+  return *sim->sim;
+}
+const gample::Simulation& S(const gp_sim* sim) {
+  if (!sim || !sim->sim) throw std::invalid_argument("null simulation handle");
+  return *sim->sim;
+}
+
+void fill(gp_solve_stats* out, const gample::SolveStats& st) {
+  if (!out) return;
+  out->iterations = st.iterations;
+  out->error = st.error;
+  out->mean_cathode = st.meanCathode;
+  out->electric_energy = st.energy;
+  out->electric_energy_increment = st.EEincrement;
+  out->joule_heating = st.joule;
+  for (int i = 0; i < 3; ++i) out->probe[i] = st.probe[i];
+  out->field_energy_cgs = st.field_energy_cgs;
+}
+void fill(gp_flow_stats* out, const gample::FlowStats& fs) {
+  if (!out) return;
+  out->particle_number = fs.particleNumber;
+  out->pulled = fs.pulledPtclNum;
+  for (int i = 0; i < 4; ++i) out->pinum[i] = fs.pinum[i];
+  out->invalid = fs.invalid;
+  out->kinetic_energy = fs.totalKineticEnergy;
+  out->kinetic_energy_increment = fs.totalKEincrement;
+}
+
+struct FieldBuf {
+  void* dev;
+  size_t bytes;
+};
+FieldBuf field_buf(gample::EMField& f, int which) {
+  switch (which) {
+    case GP_FIELD_RHO: return {f.rho.get(), f.rho.bytes()};
+    case GP_FIELD_EX: return {f.Ex.get(), f.Ex.bytes()};
+    case GP_FIELD_EY: return {f.Ey.get(), f.Ey.bytes()};
+    case GP_FIELD_BZ: return {f.Bz.get(), f.Bz.bytes()};
+    case GP_FIELD_JX: return {f.jx.get(), f.jx.bytes()};
+    case GP_FIELD_JY: return {f.jy.get(), f.jy.bytes()};
+    case GP_FIELD_PHI: return {f.phi.get(), f.phi.bytes()};
+    case GP_FIELD_SOL: return {f.sol.get(), f.sol.bytes()};
+    default: throw std::invalid_argument("unknown field selector");
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* gp_last_error(void) { return g_error.c_str(); }
+unsigned long long gp_kernel_launches(void) { return gample::kernel_launches(); }
+const char* gp_version(void) { return "gample_b200 0.1 (sm_100a)"; }
+int gp_device_count(void) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return n;
+}
+
+gp_status gp_init_parse_file(const char* path, gp_init** out) {
+  return guarded([&] {
+    if (!path || !out) throw std::invalid_argument("null argument");
+    auto* h = new gp_init{gample::Init::parseInputFile(path)};
+    *out = h;
+    return GP_OK;
+  });
+}
+gp_status gp_init_parse_json(const char* text, gp_init** out) {
+  return guarded([&] {
+    if (!text || !out) throw std::invalid_argument("null argument");
+    auto* h = new gp_init{gample::Init::parseString(text)};
+    *out = h;
+    return GP_OK;
+  });
+}
+gp_status gp_init_dump(const gp_init* init, char* buf, size_t cap, size_t* len) {
+  return guarded([&] {
+    if (!init) throw std::invalid_argument("null init");
+    std::string s = init->init.dump();
+    if (len) *len = s.size() + 1;
+    if (buf && cap) {
+      size_t n = s.size() < cap - 1 ? s.size() : cap - 1;
+      std::memcpy(buf, s.data(), n);
+      buf[n] = '\0';
+    }
+    return GP_OK;
+  });
+}
+void gp_init_free(gp_init* init) { delete init; }
+
+gp_status gp_sim_create(const gp_init* init, const char* log_name, int flags, gp_sim** out) {
+  return guarded([&] {
+    if (!init || !out) throw std::invalid_argument("null argument");
+    auto* h = new gp_sim;
+    try {
+      h->sim = std::make_unique<gample::Simulation>(init->init, log_name ? log_name : "",
+                                                    (flags & GP_SIM_REFERENCE_ORDER) == 0);
+    } catch (...) {
+      delete h;
+      throw;
+    }
+    *out = h;
+    return GP_OK;
+  });
+}
+void gp_sim_free(gp_sim* sim) {
+  try {
+    delete sim;
+  } catch (...) {
+  }
+}
+gp_status gp_sim_initialize(gp_sim* sim) {
+  return guarded([&] {
+    S(sim).initialize();
+    return GP_OK;
+  });
+}
+gp_status gp_sim_run(gp_sim* sim, int ncycles) {
+  return guarded([&] {
+    if (ncycles < 0) throw std::invalid_argument("negative cycle count");
+    S(sim).run(ncycles);
+    return GP_OK;
+  });
+}
+gp_status gp_sim_cycle_number(const gp_sim* sim, int* cycle, double* time) {
+  return guarded([&] {
+    if (cycle) *cycle = S(sim).cycle_no;
+    if (time) *time = S(sim).time;
+    return GP_OK;
+  });
+}
+gp_status gp_sim_last_solve(const gp_sim* sim, gp_solve_stats* out) {
+  return guarded([&] {
+    fill(out, S(sim).last_solve);
+    return GP_OK;
+  });
+}
+gp_status gp_sim_last_flow(const gp_sim* sim, int s, gp_flow_stats* out) {
+  return guarded([&] {
+    const auto& v = S(sim).last_flow;
+    if (s < 0 || s >= int(v.size())) throw std::invalid_argument("species index out of range");
+    fill(out, v[s]);
+    return GP_OK;
+  });
+}
+gp_status gp_sim_synchronize(gp_sim* sim) {
+  return guarded([&] {
+    GP_CUDA(cudaStreamSynchronize(S(sim).stream));
+    return GP_OK;
+  });
+}
+gp_status gp_sim_time_cycles(gp_sim* sim, int ncycles, float* ms) {
+  return guarded([&] {
+    auto& s = S(sim);
+    cudaEvent_t a, b;
+    GP_CUDA(cudaEventCreate(&a));
+    GP_CUDA(cudaEventCreate(&b));
+    GP_CUDA(cudaEventRecord(a, s.stream));
+    for (int i = 0; i < ncycles; ++i) s.cycle();
+    GP_CUDA(cudaEventRecord(b, s.stream));
+    GP_CUDA(cudaEventSynchronize(b));
+    float t = 0;
+    GP_CUDA(cudaEventElapsedTime(&t, a, b));
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    if (ms) *ms = t;
+    return GP_OK;
+  });
+}
+gp_status gp_sim_set_profiling(gp_sim* sim, int on) {
+  return guarded([&] {
+    S(sim).set_profiling(on != 0);
+    return GP_OK;
+  });
+}
+gp_status gp_sim_phase_times(gp_sim* sim, double out[5]) {
+  return guarded([&] {
+    if (!out) throw std::invalid_argument("null output");
+    S(sim).phase_times(out);
+    return GP_OK;
+  });
+}
+
+gp_status gp_field_dims(const gp_sim* sim, int* ngx, int* ngy, int* ngb, int* nkx, int* nky) {
+  return guarded([&] {
+    const auto& f = *S(sim).field;
+    if (ngx) *ngx = f.dims.ngx;
+    if (ngy) *ngy = f.dims.ngy;
+    if (ngb) *ngb = f.dims.ngb;
+    if (nkx) *nkx = f.layout.nkx;
+    if (nky) *nky = f.layout.nky;
+    return GP_OK;
+  });
+}
+gp_status gp_field_reset_charge(gp_sim* sim) {
+  return guarded([&] {
+    S(sim).field->resetChargeDensity();
+    return GP_OK;
+  });
+}
+gp_status gp_field_solve_poisson(gp_sim* sim, double dt, gp_solve_stats* out) {
+  return guarded([&] {
+    auto& s = S(sim);
+    s.last_solve = s.field->solvePoisson(dt, s.logger.get());
+    fill(out, s.last_solve);
+    return GP_OK;
+  });
+}
+gp_status gp_field_download(gp_sim* sim, int which, void* host, size_t bytes) {
+  return guarded([&] {
+    auto& s = S(sim);
+    if (which == GP_FIELD_RHO || which == GP_FIELD_JX || which == GP_FIELD_JY) {
+      // In the deterministic mode rho/jx/jy are combined from the
+      // fixed-point sums on demand.
+      s.field->finalizeCharge();
+    }
+    FieldBuf fb = field_buf(*s.field, which);
+    if (!host || bytes != fb.bytes) throw std::invalid_argument("buffer size does not match the field extent");
+    GP_CUDA(cudaMemcpyAsync(host, fb.dev, bytes, cudaMemcpyDeviceToHost, s.stream));
+    GP_CUDA(cudaStreamSynchronize(s.stream));
+    return GP_OK;
+  });
+}
+gp_status gp_field_upload(gp_sim* sim, int which, const void* host, size_t bytes) {
+  return guarded([&] {
+    auto& s = S(sim);
+    FieldBuf fb = field_buf(*s.field, which);
+    if (!host || bytes != fb.bytes) throw std::invalid_argument("buffer size does not match the field extent");
+    GP_CUDA(cudaMemcpyAsync(fb.dev, host, bytes, cudaMemcpyHostToDevice, s.stream));
+    GP_CUDA(cudaStreamSynchronize(s.stream));
+    if (which == GP_FIELD_BZ) s.field->bz_uniform = false;  // arbitrary Bz: gather it
+    return GP_OK;
+  });
+}
+gp_status gp_field_set_solver(gp_sim* sim, double tol, int maxiter) {
+  return guarded([&] {
+    if (!(tol > 0) || maxiter < 0) throw std::invalid_argument("tolerance must be > 0 and maxiter >= 0");
+    S(sim).field->tol = tol;
+    S(sim).field->maxiter = maxiter;
+    return GP_OK;
+  });
+}
+
+gp_status gp_particle_update(gp_sim* sim, int s, double dt, int fused_deposit) {
+  return guarded([&] {
+    species(sim, s)->update(dt, *S(sim).field, fused_deposit != 0);
+    return GP_OK;
+  });
+}
+gp_status gp_particle_reduce(gp_sim* sim, int s, gp_flow_stats* out) {
+  return guarded([&] {
+    auto fs = species(sim, s)->reduce(S(sim).logger.get());
+    S(sim).last_flow[s] = fs;
+    fill(out, fs);
+    return GP_OK;
+  });
+}
+gp_status gp_particle_integrate_charge(gp_sim* sim, int s) {
+  return guarded([&] {
+    species(sim, s)->integrateChargeDensity(*S(sim).field);
+    return GP_OK;
+  });
+}
+gp_status gp_particle_count(gp_sim* sim, int s, uint32_t* n) {
+  return guarded([&] {
+    if (!n) throw std::invalid_argument("null output");
+    *n = species(sim, s)->pNum();
+    return GP_OK;
+  });
+}
+gp_status gp_particle_download(gp_sim* sim, int s, gp_particle_state* host, uint32_t capacity, uint32_t* n) {
+  return guarded([&] {
+    auto* p = species(sim, s);
+    const uint32_t cnt = p->pNum();
+    if (n) *n = cnt;
+    if (host) {
+      if (capacity < cnt) throw std::invalid_argument("capacity smaller than pNum");
+      static_assert(sizeof(gp_particle_state) == sizeof(gample::kern::ParticleStateAoS), "record size");
+      p->download_aos(reinterpret_cast<gample::kern::ParticleStateAoS*>(host), cnt);
+    }
+    return GP_OK;
+  });
+}
+gp_status gp_particle_upload(gp_sim* sim, int s, const gp_particle_state* host, uint32_t n) {
+  return guarded([&] {
+    if (n && !host) throw std::invalid_argument("null input");
+    species(sim, s)->upload_aos(reinterpret_cast<const gample::kern::ParticleStateAoS*>(host), n);
+    return GP_OK;
+  });
+}
+gp_status gp_particle_download_raw(gp_sim* sim, int s, int32_t* cell, float* ox, float* oy, float* vx, float* vy,
+                                   float* vz, uint32_t capacity, uint32_t* n) {
+  return guarded([&] {
+    auto* p = species(sim, s);
+    const uint32_t cnt = p->pNum();
+    if (n) *n = cnt;
+    if (capacity < cnt && (cell || ox || oy || vx || vy || vz))
+      throw std::invalid_argument("capacity smaller than pNum");
+    auto cp = [&](void* dst, const void* src, size_t elem) {
+      if (dst && cnt) GP_CUDA(cudaMemcpyAsync(dst, src, cnt * elem, cudaMemcpyDeviceToHost, p->stream));
+    };
+    cp(cell, p->cell.get(), 4);
+    cp(ox, p->ox.get(), 4);
+    cp(oy, p->oy.get(), 4);
+    cp(vx, p->vx.get(), 4);
+    cp(vy, p->vy.get(), 4);
+    cp(vz, p->vz.get(), 4);
+    GP_CUDA(cudaStreamSynchronize(p->stream));
+    return GP_OK;
+  });
+}
+
+gp_status gp_collision_artificial_ionization(gp_sim* sim, double dt, int* addn) {
+  return guarded([&] {
+    auto& s = S(sim);
+    int a = s.collision->artificialIonization(dt, s.ptrs, s.logger.get());
+    if (addn) *addn = a;
+    return GP_OK;
+  });
+}
+gp_status gp_collision_hollow_cathode(gp_sim* sim, double dt, int* addn) {
+  return guarded([&] {
+    auto& s = S(sim);
+    int a = s.collision->hollowCathode(dt, s.ptrs, s.logger.get());
+    if (addn) *addn = a;
+    return GP_OK;
+  });
+}
+gp_status gp_collision_flux_reinjection(gp_sim* sim, double dt, int* addn) {
+  return guarded([&] {
+    auto& s = S(sim);
+    int a = s.collision->fluxReinjection(dt, s.ptrs, s.logger.get());
+    if (addn) *addn = a;
+    return GP_OK;
+  });
+}
+
+}  // extern "C"

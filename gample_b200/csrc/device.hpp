@@ -1,0 +1,122 @@
+// device.hpp -- host-side CUDA plumbing: error checks and owned device arrays.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <stdexcept>
+#include <string>
+#include <utility>
+
+namespace gample {
+
+struct CudaError : std::runtime_error {
+  cudaError_t code;
+  CudaError(cudaError_t c, const std::string& what) : std::runtime_error(what), code(c) {}
+};
+
+#define GP_CUDA(call)                                                                               \
+  do {                                                                                              \
+    cudaError_t gp_err_ = (call);                                                                   \
+    if (gp_err_ != cudaSuccess)                                                                     \
+      throw ::gample::CudaError(gp_err_, std::string(#call) + " failed at " + __FILE__ + ":" +      \
+                                             std::to_string(__LINE__) + ": " +                      \
+                                             cudaGetErrorString(gp_err_));                           \
+  } while (0)
+
+// Every kernel launch is followed by GP_LAUNCH_CHECK(), which also counts it
+// (gp_kernel_launches() in the C ABI).
+void note_kernel_launch();
+unsigned long long kernel_launches();
+#define GP_LAUNCH_CHECK()              \
+  do {                                 \
+    ::gample::note_kernel_launch();    \
+    GP_CUDA(cudaGetLastError());       \
+  } while (0)
+
+// Owned device allocation of n elements of T (not initialised unless asked).
+template <typename T>
+class DeviceArray {
+ public:
+  DeviceArray() = default;
+  explicit DeviceArray(size_t n, bool zero = false) { resize(n, zero); }
+  ~DeviceArray() { release(); }
+  DeviceArray(const DeviceArray&) = delete;
+  DeviceArray& operator=(const DeviceArray&) = delete;
+  DeviceArray(DeviceArray&& o) noexcept : p_(o.p_), n_(o.n_) {
+    o.p_ = nullptr;
+    o.n_ = 0;
+  }
+  DeviceArray& operator=(DeviceArray&& o) noexcept {
+    if (this != &o) {
+      release();
+      p_ = o.p_;
+      n_ = o.n_;
+      o.p_ = nullptr;
+      o.n_ = 0;
+    }
+    return *this;
+  }
+  void resize(size_t n, bool zero = false) {
+    release();
+    if (n) {
+      GP_CUDA(cudaMalloc(&p_, n * sizeof(T)));
+      n_ = n;
+      if (zero) GP_CUDA(cudaMemset(p_, 0, n * sizeof(T)));
+    }
+  }
+  // Grow to at least n elements keeping the first `keep` elements.
+  void grow(size_t n, size_t keep, cudaStream_t s) {
+    if (n <= n_) return;
+    T* q = nullptr;
+    GP_CUDA(cudaMalloc(&q, n * sizeof(T)));
+    if (p_ && keep) GP_CUDA(cudaMemcpyAsync(q, p_, keep * sizeof(T), cudaMemcpyDeviceToDevice, s));
+    GP_CUDA(cudaStreamSynchronize(s));
+    release();
+    p_ = q;
+    n_ = n;
+  }
+  void zero(cudaStream_t s) {
+    if (n_) GP_CUDA(cudaMemsetAsync(p_, 0, n_ * sizeof(T), s));
+  }
+  T* get() const { return p_; }
+  size_t size() const { return n_; }
+  size_t bytes() const { return n_ * sizeof(T); }
+
+ private:
+  void release() {
+    if (p_) cudaFree(p_);
+    p_ = nullptr;
+    n_ = 0;
+  }
+  T* p_ = nullptr;
+  size_t n_ = 0;
+};
+
+// Pinned host buffer for asynchronous diagnostics read-back.
+template <typename T>
+class PinnedArray {
+ public:
+  PinnedArray() = default;
+  explicit PinnedArray(size_t n) { resize(n); }
+  ~PinnedArray() {
+    if (p_) cudaFreeHost(p_);
+  }
+  PinnedArray(const PinnedArray&) = delete;
+  PinnedArray& operator=(const PinnedArray&) = delete;
+  void resize(size_t n) {
+    if (p_) cudaFreeHost(p_);
+    p_ = nullptr;
+    n_ = n;
+    if (n) GP_CUDA(cudaMallocHost(&p_, n * sizeof(T)));
+  }
+  T* get() const { return p_; }
+  T& operator[](size_t i) { return p_[i]; }
+  size_t size() const { return n_; }
+
+ private:
+  T* p_ = nullptr;
+  size_t n_ = 0;
+};
+
+}  // namespace gample

@@ -1,0 +1,175 @@
+// kernels.hpp -- host-callable launchers of the sm_100a kernels.
+//
+// Data layout in HBM:
+//  * particles: structure of arrays, one entry per particle slot:
+//      cell  int32  packed (iy << 16) | ix of the containing cell in the
+//                   reference's ghost-offset grid units; a negative value
+//                   -f marks a particle flagged f (1..4 = left through Xmin,
+//                   Xmax, Ymin, Ymax; 5 = invalid state) awaiting compaction
+//      ox,oy float  offset inside the cell, in [0, 1)
+//      vx,vy,vz float velocity in cm/s
+//    i.e. x_ref = ix + ox reproduces the reference's grid-unit position
+//    (src/Particle.mm:589-594) without its loss of precision far from 0.
+//  * fields: the reference's staggered arrays with its extents and strides
+//    (rho (nx+1)(ny+1), Ex (nx+2)(ny+1), Ey (nx+1)(ny+2), Bz (nx+2)(ny+2),
+//    phi double (nx+3)(ny+3); src/EMField.mm:127-144).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+namespace gample {
+namespace kern {
+
+// Field boundary codes (same values as gample::FieldBC).
+constexpr int FBC_PERIODIC_C = 0, FBC_DIRICHLET_C = 1, FBC_NEUMANN_C = 2;
+
+struct GridDims {
+  int ngx, ngy, ngb;
+  int nx, ny;  // ngx + 2 ngb, ngy + 2 ngb
+};
+
+struct ParticleArrays {
+  int32_t* cell;
+  float* ox;
+  float* oy;
+  float* vx;
+  float* vy;
+  float* vz;
+};
+
+// Per-species counters kept in device memory (written by the push and
+// compaction kernels, read by the host only for diagnostics).
+struct SpeciesCounters {
+  uint32_t n;        // live particle count (pNum)
+  uint32_t n_dead;   // particles flagged by the last push
+  uint32_t wall[4];  // flagged through Xmin, Xmax, Ymin, Ymax
+  uint32_t invalid;  // flagged for a non-finite or out-of-grid state
+  uint32_t n_injected;
+  uint32_t n_pulled; // removed by the last compaction (which consumes n_dead)
+  double ke;         // sum of 0.5 m v^2 w over particles still live (erg)
+};
+
+struct PushConsts {
+  float constE, constB, constX, constY;  // src/Particle.mm:617-621
+  int bc[4];                             // particle BC code per wall
+  float scale;                           // deposit weight q w / (dx dy)
+  float bz_uniform;                      // used when the Bz gather is skipped
+  double ke_half_m, ke_w;                // 0.5 * m and w for the kinetic energy
+};
+
+struct DepositTargets {
+  float* rho;
+  float* jx;
+  float* jy;
+  long long* acc_rho;  // deterministic mode: per-species fixed-point sums
+  long long* acc_jx;
+  long long* acc_jy;
+};
+
+struct FieldPtrs {
+  const float* Ex;
+  const float* Ey;
+  const float* Bz;
+};
+
+// ------------------------------------------------------------- particles
+// Gather + Boris + move + boundary conditions for particles [0, n) where n
+// is read from counters->n; optionally deposits the new positions (live
+// particles only). Writes the dead bitmap (bit k = particle k flagged) and
+// the flag counters, and accumulates the kinetic energy of live particles.
+void push(int order, int boris_order, bool deposit, bool det, bool current, bool bz_uniform, GridDims g,
+          ParticleArrays p, FieldPtrs f, PushConsts c, DepositTargets d, SpeciesCounters* counters,
+          uint32_t* dead_bits, uint32_t n_bound, cudaStream_t s);
+
+// Deposit particles [0, counters->n) (src/Particle.mm:281-389), or with
+// injected_only the particles appended since the last push,
+// [n - n_injected, n).
+void deposit(int order, bool det, bool current, GridDims g, ParticleArrays p, float scale, DepositTargets d,
+             const SpeciesCounters* counters, uint32_t n_bound, bool injected_only, cudaStream_t s);
+
+// Remove flagged particles, filling each hole (ascending) with the last
+// live particle (descending) -- the permutation of src/Particle.mm:893-966.
+// Updates counters->n. scratch must hold compact_scratch_words(n_bound).
+size_t compact_scratch_words(uint32_t n_bound);
+void compact(ParticleArrays p, SpeciesCounters* counters, const uint32_t* dead_bits, uint32_t* scratch,
+             uint32_t n_bound, cudaStream_t s);
+
+// Reference 24-byte records <-> device SoA.
+struct ParticleStateAoS {
+  float x, y, vx, vy, vz;
+  int piflag;
+};
+void aos_to_soa(const ParticleStateAoS* in, uint32_t n, ParticleArrays p, cudaStream_t s);
+void soa_to_aos(ParticleArrays p, uint32_t n, ParticleStateAoS* out, cudaStream_t s);
+
+// ------------------------------------------------------------- generation
+struct RNGState {
+  unsigned long long state, inc;
+};
+// Seed slots [from, to) as the reference's host loop does
+// (src/Collision.mm:283-294): slot i takes the (2i+1)-th and (2i+2)-th
+// outputs of splitmix64 started at master_seed.
+void seed_rng(RNGState* states, uint64_t master_seed, uint32_t from, uint32_t to, cudaStream_t s);
+
+struct GenParams {  // src/Collision.h:22-38
+  float Xmin, Xmax, Ymin, Ymax;
+  float ele_genU[3];
+  float ele_vth;
+  float ion_genU[3];
+  float ion_vth;
+  float dx, dy, ngb;
+};
+// Kernel artificialIonization (src/Collision.mm:63-174): addn particles
+// (electron, and a colocated ion unless genType == 3) appended after the
+// current counts. Device counts are advanced by addn.
+void generate(int gen_type, uint32_t addn, GenParams prm, RNGState* states, ParticleArrays ele,
+              SpeciesCounters* ele_cnt, ParticleArrays* ion, SpeciesCounters* ion_cnt, cudaStream_t s);
+// Flux-Maxwellian re-injection at Xmin of `addn` particles of one species
+// (build addition; no reference counterpart).
+struct RefluxParams {
+  float Xmin, Ymin, Ymax, vth, u0, u1, u2, dt, dx, dy, ngb;
+};
+void reflux(uint32_t addn, RefluxParams prm, RNGState* states, ParticleArrays p, SpeciesCounters* cnt,
+            cudaStream_t s);
+
+// ------------------------------------------------------------- fields
+void zero_f32(float* p, size_t n, cudaStream_t s);
+// rho = sum_s double(acc_s) * (scale_s * 2^-40), rounded to float
+// (species in order); same for the currents with an extra factor c.
+void combine_fixed_point(const long long* const* acc, const float* scales, int nspecies, size_t n, double extra,
+                         float* out, cudaStream_t s);
+// Ghost-charge folding (src/EMField.mm:751-850).
+void fold_ghosts(float* rho, GridDims g, const int fbc[4], cudaStream_t s);
+
+struct PoissonLayout {
+  int nkx, nky, ikmin, jkmin;  // src/EMField.mm:246-271
+  int fbc[4];
+  double Cx, Cy, Cd;
+  double phiXmin, phiXmax, phiYmin, phiYmax;  // statV
+  bool periodic_x, periodic_y;
+};
+// b = rhs_BC - 4 pi rho (src/EMField.mm:852-861) in FP64; accumulates
+// sum(b) and sum(b^2) into sums[0..1].
+void build_rhs(const float* rho, GridDims g, PoissonLayout L, double* b, double* sums, cudaStream_t s);
+void subtract_mean(double* v, int n, const double* sum, cudaStream_t s);
+// sums[0..1] = sum(v), sum(v^2)
+void vec_sums(const double* v, int n, double* sums, cudaStream_t s);
+
+// phi (nx+3)(ny+3) from the solution vector (src/EMField.mm:873-1077).
+void phi_fill(const double* sol, GridDims g, PoissonLayout L, float dx, double cathode_pos, double* cathode_mean,
+              double* phi, cudaStream_t s);
+// Ex, Ey = -grad phi (src/EMField.mm:1080-1094) and the energy / Joule
+// sums (src/EMField.mm:1096-1111) into sums[0] (sum E^2), sums[1] (sum E.j).
+void gradient_energy(const double* phi, GridDims g, float dx, float dy, float* Ex, float* Ey, const float* jx,
+                     const float* jy, double* sums, cudaStream_t s);
+// Probe values for the timeseries CSV (src/EMField.mm:1130-1134).
+void probe(const double* phi, const float* Ex, const float* Ey, GridDims g, double* out3, cudaStream_t s);
+
+// ------------------------------------------------------------- utilities
+void fill_f32(float* p, size_t n, float v, cudaStream_t s);
+void fill_f64(double* p, size_t n, double v, cudaStream_t s);
+
+}  // namespace kern
+}  // namespace gample

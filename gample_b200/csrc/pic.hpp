@@ -1,0 +1,180 @@
+// pic.hpp -- C++ host objects of the PIC step, mirroring gample's classes.
+//
+//   EMField   src/EMField.{h,mm}   staggered fields, Poisson solve, diagnostics
+//   Particle  src/Particle.{h,mm}  one species: push, deposit, reduce
+//   Collision src/Collision.{h,mm} initial load and particle sources
+//   XmlLogger src/XmlLogger.h      XML log and timeseries CSV
+//
+// Each object owns its device memory and issues work on one CUDA stream;
+// results stay in HBM and are copied back only for diagnostics and I/O.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <array>
+#include <fstream>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "device.hpp"
+#include "init.hpp"
+#include "kernels.hpp"
+#include "multigrid.hpp"
+
+namespace gample {
+
+// src/XmlLogger.h:89-93 (value rounded to float, std::scientific)
+std::string fmtSci(float v, int prec);
+
+// src/XmlLogger.h:8-86
+class XmlLogger {
+ public:
+  XmlLogger(const std::string& logName, const std::string& csvHeader);
+  ~XmlLogger();
+  void swichLog(bool on) { on_ = on; }
+  bool on() const { return on_; }
+  void logCycleStart(int cycle, double time);
+  void logSection(const std::string& name, const std::map<std::string, std::string>& data);
+  void csvOutput(const std::string& data);
+  void logCycleEnd();
+  void logComment(const std::string& comment);
+
+ private:
+  std::ofstream xml_, csv_;
+  bool on_ = false;
+};
+
+struct SolveStats {
+  int iterations = 0;
+  double error = 0;         // relative residual
+  double meanCathode = 0;   // V
+  double energy = 0;        // erg/m (src/EMField.mm:1112: no 1/(4 pi))
+  double EEincrement = 0;
+  double joule = 0;
+  double probe[3] = {0, 0, 0};  // phi1 (statV), Ex1, Ey1 (statV/cm)
+  double field_energy_cgs = 0;  // sum E^2/(8 pi) dx dy (physical)
+};
+
+struct FlowStats {
+  uint32_t particleNumber = 0;
+  uint32_t pulledPtclNum = 0;
+  int pinum[4] = {0, 0, 0, 0};  // charge-weighted counts per wall
+  uint32_t invalid = 0;
+  double totalKineticEnergy = 0;  // erg
+  double totalKEincrement = 0;
+};
+
+class Particle;
+
+class EMField {
+ public:
+  EMField(const Init& init, cudaStream_t s, int nspecies);  // src/EMField.mm:105-656
+  void resetChargeDensity();                               // src/EMField.mm:1363-1378
+  SolveStats solvePoisson(double dt, XmlLogger* logger);   // src/EMField.mm:745-1136
+  // Combine the fixed-point accumulators (deterministic mode) into rho/jx/jy.
+  void finalizeCharge();
+
+  kern::GridDims dims{};
+  float dx = 0, dy = 0;
+  bool det = false;      // deterministic fixed-point deposit
+  bool charge_dirty = false;  // fixed-point sums not yet combined into rho/jx/jy
+  bool current = false;  // jx, jy deposited (Darwin or FlagForCurDens)
+  bool bz_uniform = false;
+  float bz_value = 0;
+  int fbc[4] = {0, 0, 0, 0};
+  double cathodePos = -1;
+  kern::PoissonLayout layout{};
+  int maxiter = 200;
+  double tol = 1e-7;
+
+  DeviceArray<float> rho, jx, jy, Ex, Ey, Ez, Bx, By, Bz;
+  DeviceArray<double> phi, sol, b, diag;  // diag: [0..1] rhs sums [2..3] E sums [4] cathode mean [5..7] probe
+  std::vector<DeviceArray<long long>> acc_rho, acc_jx, acc_jy;
+  std::vector<float> species_scale;
+  std::unique_ptr<PoissonMG> mg;
+  double lastEE = 0;
+  MGResult last_mg;
+  cudaStream_t stream;
+
+  kern::DepositTargets targets(int s);
+  size_t n_rho() const { return size_t(dims.nx + 1) * (dims.ny + 1); }
+  size_t n_ex() const { return size_t(dims.nx + 2) * (dims.ny + 1); }
+  size_t n_ey() const { return size_t(dims.nx + 1) * (dims.ny + 2); }
+  size_t n_bz() const { return size_t(dims.nx + 2) * (dims.ny + 2); }
+  size_t n_phi() const { return size_t(dims.nx + 3) * (dims.ny + 3); }
+
+ private:
+  PinnedArray<double> host_diag_;
+  void load1dField(const std::string& path, std::vector<float>& out, size_t need) const;  // :658-687
+};
+
+class Particle {
+ public:
+  Particle(const Init& init, int s, cudaStream_t stream);  // src/Particle.mm:407-611
+  // src/Particle.mm:615-891; with fused_deposit the new positions are also
+  // deposited into fld (next step's charge).
+  void update(double dt, EMField& fld, bool fused_deposit);
+  FlowStats reduce(XmlLogger* logger);                   // src/Particle.mm:893-1002
+  void integrateChargeDensity(EMField& fld, bool injected_only = false);  // src/Particle.mm:1004-1130
+
+  uint32_t pNum();  // synchronous read of the device count
+  void setPNum(uint32_t n);
+  void upload_aos(const kern::ParticleStateAoS* host, uint32_t n);
+  void download_aos(kern::ParticleStateAoS* host, uint32_t n);
+  kern::ParticleArrays arrays() const;
+  kern::SpeciesCounters counters();  // synchronous
+
+  std::string pName;
+  int index = 0;
+  float m = 0, q = 0, w = 0;
+  uint32_t pNumMax = 0;
+  uint32_t n_bound = 0;  // host-side upper bound of the device count
+  int order = 1, boris = 2;
+  int pbc[4] = {0, 0, 0, 0};
+  double lastKE = 0;
+  int pinum[4] = {0, 0, 0, 0};
+  uint32_t last_pulled = 0;
+  double last_dt = 0;
+
+  DeviceArray<int32_t> cell;
+  DeviceArray<float> ox, oy, vx, vy, vz;
+  DeviceArray<uint32_t> dead_bits, scratch;
+  DeviceArray<kern::SpeciesCounters> cnt;
+  cudaStream_t stream;
+
+ private:
+  PinnedArray<kern::SpeciesCounters> host_cnt_;
+  double dx_ = 0, dy_ = 0;
+};
+
+class Collision {
+ public:
+  // src/Collision.mm:189-462: sets up the sources and loads the initial
+  // particles of every species (overwriting them) from the splitmix64/PCG32
+  // stream.
+  Collision(const Init& init, std::vector<Particle*>& ptcls, cudaStream_t stream);
+  int artificialIonization(double dt, std::vector<Particle*>& ptcls, XmlLogger* logger);  // :464-566
+  int hollowCathode(double dt, std::vector<Particle*>& ptcls, XmlLogger* logger);         // :568-678
+  // Build addition: re-inject absorbed particles at Xmin (GenerateType
+  // fluxMaxwellianAtXmin).
+  int fluxReinjection(double dt, std::vector<Particle*>& ptcls, XmlLogger* logger);
+  // libc++ minstd_rand + generate_canonical<double, 53> (src/Collision.mm:183, 482-487)
+  double uniform01();
+
+  DeviceArray<kern::RNGState> states;
+  uint32_t initialized = 0;
+  uint64_t master_seed = 0;
+  cudaStream_t stream;
+
+ private:
+  void ensure_states(uint32_t n);
+  const Init& init_;
+  uint64_t minstd_ = 1;
+  bool existAI_ = false, existHC_ = false;
+  int ai_source_ = -1, hc_source_ = -1;
+  std::vector<int> reflux_sources_;
+};
+
+}  // namespace gample

@@ -1,0 +1,160 @@
+// pic_particle.cpp -- Particle host object (one species).
+#include <cmath>
+#include <cstring>
+#include <stdexcept>
+
+#include "pic.hpp"
+
+namespace gample {
+
+Particle::Particle(const Init& init, int s, cudaStream_t st) : stream(st), host_cnt_(1) {
+  if (s < 0 || s >= int(init.paramForParticle.size())) throw ConfigError("species index out of range");
+  const ParamForParticle& pp = init.paramForParticle[s];
+  const ParamForField& fp = init.paramForField;
+  index = s;
+  pName = pp.pName;
+  pNumMax = init.paramForComputing.pNumMax;
+  m = float(pp.m);
+  q = float(pp.q);
+  w = float(pp.w);
+  order = fp.weightOrder;
+  boris = fp.BorisOrder;
+  dx_ = fp.dx;
+  dy_ = fp.dy;
+  if (boris != 2 && boris != 4 && boris != 6) throw ConfigError("BorisOrder must be 2, 4 or 6");
+  // src/Particle.mm:459-514 (an unknown BC string is fatal there too)
+  auto codes = init.particleBCCodes();
+  for (int w2 = 0; w2 < 4; ++w2) {
+    if (codes[w2] == PBC_INVALID) throw ConfigError("[FatalError] invalid particle boundary");
+    pbc[w2] = codes[w2];
+  }
+  // src/Particle.mm:544-547
+  if (pp.pNum > pNumMax) throw ConfigError("pNum > pNumMax for " + pName);
+  if (fp.ngx + 2 * fp.ngb + 2 > 65535 || fp.ngy + 2 * fp.ngb + 2 > 32767)
+    throw ConfigError("grid too large for the packed cell index");
+  const size_t cap = pNumMax;
+  cell.resize(cap);
+  ox.resize(cap);
+  oy.resize(cap);
+  vx.resize(cap);
+  vy.resize(cap);
+  vz.resize(cap);
+  dead_bits.resize((cap + 31) / 32 + 1, true);
+  scratch.resize(kern::compact_scratch_words(uint32_t(cap)), true);
+  cnt.resize(1, true);
+  n_bound = 0;
+  // The reference loads pNum particles on the CPU here (src/Particle.mm:568-597)
+  // from std::random_device and Collision's init then overwrites them
+  // (src/Collision.mm:315-336); the build loads only through Collision.
+}
+
+kern::ParticleArrays Particle::arrays() const {
+  return kern::ParticleArrays{cell.get(), ox.get(), oy.get(), vx.get(), vy.get(), vz.get()};
+}
+
+kern::SpeciesCounters Particle::counters() {
+  GP_CUDA(cudaMemcpyAsync(host_cnt_.get(), cnt.get(), sizeof(kern::SpeciesCounters), cudaMemcpyDeviceToHost,
+                          stream));
+  GP_CUDA(cudaStreamSynchronize(stream));
+  return host_cnt_[0];
+}
+
+uint32_t Particle::pNum() {
+  uint32_t n = counters().n;
+  n_bound = n;
+  return n;
+}
+
+void Particle::setPNum(uint32_t n) {
+  if (n > pNumMax) throw std::invalid_argument("pNum > pNumMax");
+  kern::SpeciesCounters c{};
+  c.n = n;
+  GP_CUDA(cudaMemcpyAsync(cnt.get(), &c, sizeof(c), cudaMemcpyHostToDevice, stream));
+  GP_CUDA(cudaStreamSynchronize(stream));
+  n_bound = n;
+}
+
+void Particle::upload_aos(const kern::ParticleStateAoS* host, uint32_t n) {
+  if (n > pNumMax) throw std::invalid_argument("pNum > pNumMax");
+  if (n) {
+    DeviceArray<kern::ParticleStateAoS> tmp(n);
+    GP_CUDA(cudaMemcpyAsync(tmp.get(), host, size_t(n) * sizeof(*host), cudaMemcpyHostToDevice, stream));
+    kern::aos_to_soa(tmp.get(), n, arrays(), stream);
+    GP_CUDA(cudaStreamSynchronize(stream));
+  }
+  setPNum(n);
+}
+
+void Particle::download_aos(kern::ParticleStateAoS* host, uint32_t n) {
+  if (!n) return;
+  DeviceArray<kern::ParticleStateAoS> tmp(n);
+  kern::soa_to_aos(arrays(), n, tmp.get(), stream);
+  GP_CUDA(cudaMemcpyAsync(host, tmp.get(), size_t(n) * sizeof(*host), cudaMemcpyDeviceToHost, stream));
+  GP_CUDA(cudaStreamSynchronize(stream));
+}
+
+void Particle::update(double dt, EMField& fld, bool fused_deposit) {
+  kern::PushConsts c{};
+  // src/Particle.mm:617-621
+  c.constE = float(0.5 * double(q) * dt / double(m));
+  c.constB = float(0.5 * double(q) * dt / double(m) / phys::c);
+  c.constX = float(dt / double(fld.dx));
+  c.constY = float(dt / double(fld.dy));
+  for (int i = 0; i < 4; ++i) c.bc[i] = pbc[i];
+  c.scale = float(double(q * w) / (dx_ * dy_));  // src/Particle.mm:540
+  c.bz_uniform = fld.bz_value;
+  c.ke_half_m = 0.5 * double(m);
+  c.ke_w = double(w);
+  fld.species_scale[index] = c.scale;
+  if (fused_deposit && fld.det) fld.charge_dirty = true;
+  last_dt = dt;
+  kern::FieldPtrs f{fld.Ex.get(), fld.Ey.get(), fld.Bz.get()};
+  kern::push(order, boris, fused_deposit, fld.det, fld.current, fld.bz_uniform, fld.dims, arrays(), f, c,
+             fld.targets(index), cnt.get(), dead_bits.get(), n_bound, stream);
+}
+
+FlowStats Particle::reduce(XmlLogger* logger) {
+  kern::compact(arrays(), cnt.get(), dead_bits.get(), scratch.get(), n_bound, stream);
+  kern::SpeciesCounters c = counters();
+  FlowStats fs;
+  // src/Particle.mm:915: counts in units of the charge sign
+  const int unit = int(q / float(phys::ec));
+  for (int i = 0; i < 4; ++i) {
+    pinum[i] = int(c.wall[i]) * unit;
+    fs.pinum[i] = pinum[i];
+  }
+  fs.particleNumber = c.n;
+  fs.pulledPtclNum = c.n_pulled;
+  fs.invalid = c.invalid;
+  fs.totalKineticEnergy = c.ke;
+  fs.totalKEincrement = c.ke - lastKE;
+  lastKE = c.ke;
+  last_pulled = c.n_pulled;
+  n_bound = c.n;
+  if (logger && logger->on()) {
+    // src/Particle.mm:990-1001
+    std::map<std::string, std::string> data = {
+        {"particleNumber", std::to_string(fs.particleNumber)},
+        {"pulledPtclNum", std::to_string(fs.pulledPtclNum)},
+        {"Xmin", std::to_string(fs.pinum[0])},
+        {"Xmax", std::to_string(fs.pinum[1])},
+        {"Ymin", std::to_string(fs.pinum[2])},
+        {"Ymax", std::to_string(fs.pinum[3])},
+        {"totalKineticEnergy", fmtSci(float(fs.totalKineticEnergy * phys::ergtoev), 6)},
+        {"totalKEincrement", fmtSci(float(fs.totalKEincrement * phys::ergtoev), 6)},
+    };
+    if (fs.invalid) data["invalidPtclNum"] = std::to_string(fs.invalid);
+    logger->logSection("flowout_" + pName, data);
+  }
+  return fs;
+}
+
+void Particle::integrateChargeDensity(EMField& fld, bool injected_only) {
+  const float scale = float(double(q * w) / (dx_ * dy_));  // src/Particle.mm:540
+  fld.species_scale[index] = scale;
+  if (fld.det) fld.charge_dirty = true;
+  kern::deposit(order, fld.det, fld.current, fld.dims, arrays(), scale, fld.targets(index), cnt.get(), n_bound,
+                injected_only, stream);
+}
+
+}  // namespace gample

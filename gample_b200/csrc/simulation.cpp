@@ -1,0 +1,125 @@
+// simulation.cpp -- time loop of the reference's main() (src/main.mm).
+#include "simulation.hpp"
+
+#include <stdexcept>
+
+namespace gample {
+
+Simulation::Simulation(const Init& in, const std::string& log_name, bool fused_step) : init(in), fused(fused_step) {
+  GP_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+  if (!log_name.empty()) logger = std::make_unique<XmlLogger>(log_name, "cycle,time,phi1,Ex1,Ey1");
+  const int ns = init.flagForEquation.Particle;
+  if (ns < 1 || ns > int(init.paramForParticle.size()) || ns > 4)
+    throw ConfigError("FlagForEquation.Particle must be between 1 and the number of listed species (max 4)");
+  for (int s = 0; s < ns; ++s) {  // src/main.mm:96-106
+    particles.push_back(std::make_unique<Particle>(init, s, stream));
+    ptrs.push_back(particles.back().get());
+  }
+  field = std::make_unique<EMField>(init, stream, ns);               // src/main.mm:108-113
+  collision = std::make_unique<Collision>(init, ptrs, stream);        // src/main.mm:117-122
+  last_flow.resize(ns);
+  cycle_no = init.paramForTimeIntegration.Start;
+  time = cycle_no * init.paramForTimeIntegration.TimeStep;
+}
+
+Simulation::~Simulation() {
+  for (auto& e : events_) {
+    cudaEventDestroy(e.second.first);
+    cudaEventDestroy(e.second.second);
+  }
+  particles.clear();
+  field.reset();
+  collision.reset();
+  if (stream) cudaStreamDestroy(stream);
+}
+
+void Simulation::set_profiling(bool on) { profiling_ = on; }
+
+void Simulation::mark(int phase, bool begin) {
+  if (!profiling_) return;
+  if (begin) {
+    GP_CUDA(cudaEventCreate(&open_));
+    GP_CUDA(cudaEventRecord(open_, stream));
+  } else {
+    cudaEvent_t e;
+    GP_CUDA(cudaEventCreate(&e));
+    GP_CUDA(cudaEventRecord(e, stream));
+    events_.push_back({phase, {open_, e}});
+    open_ = nullptr;
+  }
+}
+
+void Simulation::phase_times(double out[PH_COUNT]) {
+  GP_CUDA(cudaStreamSynchronize(stream));
+  for (auto& e : events_) {
+    float ms = 0;
+    GP_CUDA(cudaEventElapsedTime(&ms, e.second.first, e.second.second));
+    acc_[e.first] += ms;
+    cudaEventDestroy(e.second.first);
+    cudaEventDestroy(e.second.second);
+  }
+  events_.clear();
+  for (int i = 0; i < PH_COUNT; ++i) out[i] = acc_[i];
+}
+
+void Simulation::initialize() {
+  // src/main.mm:114-141: the logger is still switched off here.
+  field->resetChargeDensity();
+  for (auto* p : ptrs) p->integrateChargeDensity(*field);
+  last_solve = field->solvePoisson(0.0, logger.get());
+  if (fused) {
+    // The first cycle's charge: same particle positions, fresh accumulators.
+    field->resetChargeDensity();
+    for (auto* p : ptrs) p->integrateChargeDensity(*field);
+  }
+  GP_CUDA(cudaStreamSynchronize(stream));
+}
+
+void Simulation::cycle() {
+  const auto& T = init.paramForTimeIntegration;
+  const double dt = T.TimeStep;
+  ++cycle_no;
+  if (logger) logger->swichLog(T.LogOutput != 0 && cycle_no % T.LogOutput == 0);  // :157-158 (guarded)
+  // Kahan-compensated time (src/main.mm:160-163)
+  const double y = dt - comp;
+  const double t = time + y;
+  comp = (t - time) - y;
+  time = t;
+  if (logger) logger->logCycleStart(cycle_no, time);
+  if (!fused) {
+    mark(PH_DEPOSIT, true);
+    field->resetChargeDensity();
+    for (auto* p : ptrs) p->integrateChargeDensity(*field);
+    mark(PH_DEPOSIT, false);
+  }
+  const int em = init.flagForEquation.EMField;
+  if (em == 1 || em == 2) {
+    mark(PH_SOLVE, true);
+    last_solve = field->solvePoisson(dt, logger.get());
+    mark(PH_SOLVE, false);
+  }
+  if (fused) field->resetChargeDensity();
+  for (size_t s = 0; s < ptrs.size(); ++s) {
+    mark(PH_PUSH, true);
+    ptrs[s]->update(dt, *field, fused);
+    mark(PH_PUSH, false);
+    mark(PH_REDUCE, true);
+    last_flow[s] = ptrs[s]->reduce(logger.get());
+    mark(PH_REDUCE, false);
+  }
+  mark(PH_SOURCE, true);
+  last_ai = collision->artificialIonization(dt, ptrs, logger.get());
+  last_hc = collision->hollowCathode(dt, ptrs, logger.get());
+  last_reflux = collision->fluxReinjection(dt, ptrs, logger.get());
+  if (fused)
+    for (auto* p : ptrs) p->integrateChargeDensity(*field, true);
+  mark(PH_SOURCE, false);
+  if (logger) logger->logCycleEnd();
+}
+
+void Simulation::run(int ncycles) {
+  for (int i = 0; i < ncycles; ++i) cycle();
+  GP_CUDA(cudaStreamSynchronize(stream));
+}
+
+}  // namespace gample

@@ -1,0 +1,156 @@
+/* gample_gpu.h -- C ABI of the B200-native gample particle-in-cell step.
+ *
+ * The reference (tnaoki0630/gample) has no plugin API: its boundary is the
+ * Objective-C method surface of the Init, Particle, EMField and Collision
+ * classes plus the JSON condition schema and the timeseries CSV / XML log.
+ * Each entry point below replaces one of those methods (cited as file:line
+ * inside the gample repository). Plain pointers and sizes only; every call
+ * returns a gp_status (0 = success) and never aborts. gp_last_error() gives
+ * the message of the last failure on the calling thread.
+ *
+ * Threading: a gp_sim owns one CUDA stream on the current device; handles are
+ * not thread-safe. Device work is asynchronous; calls that return host values
+ * synchronise the stream.
+ */
+#ifndef GAMPLE_GPU_H
+#define GAMPLE_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int gp_status;
+#define GP_OK 0
+#define GP_ERR_ARGUMENT 1     /* bad handle, index or size */
+#define GP_ERR_CONFIG 2       /* condition file rejected (Init.mm returns nil) */
+#define GP_ERR_CUDA 3         /* CUDA runtime failure (message in gp_last_error) */
+#define GP_ERR_CAPACITY 4     /* pNum would exceed MaximumParticleNumber */
+#define GP_ERR_INTERNAL 5
+
+typedef struct gp_init gp_init; /* parsed condition (src/Init.h:101-118) */
+typedef struct gp_sim gp_sim;   /* Particle[], EMField, Collision, XmlLogger of one run */
+
+/* Particle record of the reference (src/Particle.h:14-21): x, y in grid units
+ * offset by ngb, velocities in cm/s, piflag 0 = live, 1..4 = left through
+ * Xmin, Xmax, Ymin, Ymax (5 = invalid state, build addition). */
+typedef struct {
+  float x, y, vx, vy, vz;
+  int32_t piflag;
+} gp_particle_state;
+
+typedef struct {
+  int32_t iterations;        /* V-cycles (the reference logs AMGCL CG iterations) */
+  double error;              /* relative residual ||b - A phi|| / ||b|| */
+  double mean_cathode;       /* V */
+  double electric_energy;    /* erg/m as logged by the reference (no 1/(4 pi)) */
+  double electric_energy_increment;
+  double joule_heating;      /* erg/m */
+  double probe[3];           /* phi1 (statV), Ex1, Ey1 (statV/cm) of the CSV */
+  double field_energy_cgs;   /* sum E^2/(8 pi) dx dy, erg/cm */
+} gp_solve_stats;
+
+typedef struct {
+  uint32_t particle_number;  /* pNum after removal */
+  uint32_t pulled;           /* particles removed */
+  int32_t pinum[4];          /* outflow per wall in units of the charge sign */
+  uint32_t invalid;          /* removed for a non-finite / off-grid state */
+  double kinetic_energy;     /* erg */
+  double kinetic_energy_increment;
+} gp_flow_stats;
+
+/* Field selectors for gp_field_download / gp_field_upload (reference extents,
+ * row-major with the reference's strides, src/EMField.mm:133-144). */
+#define GP_FIELD_RHO 0 /* float (nx+1)(ny+1) */
+#define GP_FIELD_EX 1  /* float (nx+2)(ny+1) */
+#define GP_FIELD_EY 2  /* float (nx+1)(ny+2) */
+#define GP_FIELD_BZ 3  /* float (nx+2)(ny+2) */
+#define GP_FIELD_JX 4  /* float (nx+2)(ny+1) */
+#define GP_FIELD_JY 5  /* float (nx+1)(ny+2) */
+#define GP_FIELD_PHI 6 /* double (nx+3)(ny+3) */
+#define GP_FIELD_SOL 7 /* double (nkx+1)(nky+1): Poisson solution vector (src/EMField.mm:97, 410) */
+
+/* ---- Init: -[Init parseInputFile:] (src/Init.mm:27-301) ---- */
+gp_status gp_init_parse_file(const char* path, gp_init** out);
+gp_status gp_init_parse_json(const char* json_text, gp_init** out);
+/* Canonical JSON of the parsed, defaults-merged condition; *len receives the
+ * full length (including the terminating NUL) even if cap is too small. */
+gp_status gp_init_dump(const gp_init* init, char* buf, size_t cap, size_t* len);
+void gp_init_free(gp_init* init);
+
+/* ---- Run objects: src/main.mm:75-122 ----
+ * Builds Particle objects (src/Particle.mm:407-611), EMField
+ * (src/EMField.mm:105-656) and Collision (src/Collision.mm:189-462, which
+ * loads the initial particles). log_name: "<Project>_<tag>" prefix of the
+ * XML log and timeseries CSV, or NULL for none. flags: GP_SIM_* below. */
+#define GP_SIM_REFERENCE_ORDER 1 /* separate deposit pass (no push-fused deposit) */
+gp_status gp_sim_create(const gp_init* init, const char* log_name, int flags, gp_sim** out);
+void gp_sim_free(gp_sim* sim);
+/* Initial deposit and field solve: src/main.mm:136-141. */
+gp_status gp_sim_initialize(gp_sim* sim);
+/* ncycles cycles of the time loop: src/main.mm:155-253. */
+gp_status gp_sim_run(gp_sim* sim, int ncycles);
+gp_status gp_sim_cycle_number(const gp_sim* sim, int* cycle, double* time);
+gp_status gp_sim_last_solve(const gp_sim* sim, gp_solve_stats* out);
+gp_status gp_sim_last_flow(const gp_sim* sim, int species, gp_flow_stats* out);
+gp_status gp_sim_synchronize(gp_sim* sim);
+/* Device-side timing of whole cycles on the run's stream (CUDA events). */
+gp_status gp_sim_time_cycles(gp_sim* sim, int ncycles, float* ms);
+/* Per-phase device time accumulated while profiling is on (ms):
+ * [0] deposit [1] field solve [2] push [3] reduce [4] sources. */
+gp_status gp_sim_set_profiling(gp_sim* sim, int on);
+gp_status gp_sim_phase_times(gp_sim* sim, double out[5]);
+
+/* ---- EMField ---- */
+gp_status gp_field_dims(const gp_sim* sim, int* ngx, int* ngy, int* ngb, int* nkx, int* nky);
+/* -[EMField resetChargeDensity] (src/EMField.mm:1363-1378) */
+gp_status gp_field_reset_charge(gp_sim* sim);
+/* -[EMField solvePoisson:withLogger:] (src/EMField.mm:745-1136) */
+gp_status gp_field_solve_poisson(gp_sim* sim, double dt, gp_solve_stats* out);
+/* Buffer accessors (src/EMField.h:22-37, EMField.mm:1396-1424) */
+gp_status gp_field_download(gp_sim* sim, int which, void* host, size_t bytes);
+gp_status gp_field_upload(gp_sim* sim, int which, const void* host, size_t bytes);
+/* Set the Poisson tolerance / iteration cap (ToleranceForPoisson, MaxiterForPoisson). */
+gp_status gp_field_set_solver(gp_sim* sim, double tol, int maxiter);
+
+/* ---- Particle (species index s) ---- */
+/* -[Particle update:withEMField:withMom:withLogger:] (src/Particle.mm:615-891);
+ * fused_deposit != 0 also deposits the new positions into the field's charge. */
+gp_status gp_particle_update(gp_sim* sim, int s, double dt, int fused_deposit);
+/* -[Particle reduce:] (src/Particle.mm:893-1002) */
+gp_status gp_particle_reduce(gp_sim* sim, int s, gp_flow_stats* out);
+/* -[Particle integrateChargeDensity:withMoment:withLogger:] (src/Particle.mm:1004-1130) */
+gp_status gp_particle_integrate_charge(gp_sim* sim, int s);
+/* pNum (src/Particle.mm:451, paramsBuffer) */
+gp_status gp_particle_count(gp_sim* sim, int s, uint32_t* n);
+/* particleBuffer contents as 24-byte records (src/Particle.h:69-78) */
+gp_status gp_particle_download(gp_sim* sim, int s, gp_particle_state* host, uint32_t capacity, uint32_t* n);
+gp_status gp_particle_upload(gp_sim* sim, int s, const gp_particle_state* host, uint32_t n);
+/* Device representation: packed cell ((iy << 16) | ix, negative = -piflag)
+ * and in-cell offsets; any pointer may be NULL. */
+gp_status gp_particle_download_raw(gp_sim* sim, int s, int32_t* cell, float* ox, float* oy, float* vx, float* vy,
+                                   float* vz, uint32_t capacity, uint32_t* n);
+
+/* ---- Collision ---- */
+/* -[Collision artificialIonization:withParticles:withLogger:] (src/Collision.mm:464-566) */
+gp_status gp_collision_artificial_ionization(gp_sim* sim, double dt, int* addn);
+/* -[Collision hollowCathode:withParticles:withLogger:] (src/Collision.mm:568-678) */
+gp_status gp_collision_hollow_cathode(gp_sim* sim, double dt, int* addn);
+/* Flux-Maxwellian re-injection at Xmin (GenerateType fluxMaxwellianAtXmin);
+ * build addition, no reference counterpart. */
+gp_status gp_collision_flux_reinjection(gp_sim* sim, double dt, int* addn);
+
+/* ---- misc ---- */
+const char* gp_last_error(void);
+const char* gp_version(void);
+/* Number of CUDA devices visible (0 without a GPU); never fails. */
+int gp_device_count(void);
+/* Kernels this library has launched since it was loaded (all runs). */
+unsigned long long gp_kernel_launches(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GAMPLE_GPU_H */

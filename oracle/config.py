@@ -10,6 +10,7 @@ from __future__ import annotations
 
 import json
 import math
+import struct
 
 EC = 4.803204197e-10          # src/Constant.h:4
 C_LIGHT = 2.99792458e10       # src/Constant.h:5
@@ -90,6 +91,11 @@ def _dbl(v):
     return 0.0
 
 
+def _f32(x):
+    """Round to float32 (src/Init.h:27-36 stores these members as float)."""
+    return struct.unpack("f", struct.pack("f", x))[0]
+
+
 def _vec(v):
     return [_dbl(x) for x in v] if isinstance(v, list) else []
 
@@ -132,9 +138,9 @@ def parse(path_or_dict):
     out["comp"] = {"pNumMax": _int(m["MaximumParticleNumber"]) & 0xFFFFFFFF,
                    "threadGroupSize": _int(m["ThreadGroupSize"]),
                    "integrationChunkSize": _int(m["IntegrationChunkSize"]),
-                   "aggrThreshold": _dbl(m["AggregationThreshold"]), "chebDegree": _int(m["ChebyshevDegree"]),
+                   "aggrThreshold": _f32(_dbl(m["AggregationThreshold"])), "chebDegree": _int(m["ChebyshevDegree"]),
                    "amgCycleType": _int(m["AMGCycleType"]), "maxiter": _int(m["MaxiterForPoisson"]),
-                   "tolerance": _dbl(m["ToleranceForPoisson"])}
+                   "tolerance": _f32(_dbl(m["ToleranceForPoisson"]))}
 
     fd = root.get("ParamForField")
     if not isinstance(fd, dict):

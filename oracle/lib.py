@@ -100,6 +100,8 @@ def lib():
             "or_shape_ref_f64": (None, [i, d, dp]),
             "or_pcg_stream": (None, [C.c_uint64, C.c_uint64, i, i, C.POINTER(C.c_uint32)]),
             "or_minstd_uniform": (d, [i, dp]),
+            "or_splitmix64_stream": (None, [C.c_uint64, i, C.POINTER(C.c_uint64)]),
+            "or_pcg32_raw": (None, [C.c_uint64, C.c_uint64, i, C.POINTER(C.c_uint32)]),
             "or_num_threads": (i, []),
         }
         for name, (res, args) in sig.items():
@@ -285,6 +287,18 @@ def shape_ref(order, h, f64=False):
 def pcg_stream(master_seed, first_slot, nslots, ndraws):
     out = np.zeros((nslots, ndraws), np.uint32)
     lib().or_pcg_stream(master_seed, first_slot, nslots, ndraws, _p(out, C.c_uint32))
+    return out
+
+
+def splitmix64_stream(seed, n):
+    out = np.zeros(n, np.uint64)
+    lib().or_splitmix64_stream(seed, n, _p(out, C.c_uint64))
+    return out
+
+
+def pcg32_raw(state, inc, n):
+    out = np.zeros(n, np.uint32)
+    lib().or_pcg32_raw(state, inc, n, _p(out, C.c_uint32))
     return out
 
 

@@ -121,6 +121,8 @@ void or_shape_ref_f32(int order, float h, float* w);
 void or_shape_ref_f64(int order, double h, double* w);
 void or_pcg_stream(uint64_t master_seed, uint64_t first_slot, int nslots, int ndraws, uint32_t* out);
 double or_minstd_uniform(int count, double* out);
+void or_splitmix64_stream(uint64_t seed, int n, uint64_t* out);
+void or_pcg32_raw(uint64_t state, uint64_t inc, int n, uint32_t* out);
 int or_num_threads(void);
 
 #ifdef __cplusplus

@@ -602,9 +602,12 @@ void or_det_deposit_rho(int order, int ngx, int ngy, int ngb, int n, const int32
     shape_build(order, ox[k], wx);
     shape_build(order, oy[k], wy);
     // node-centred x base i2 = ix, y base j1 = iy (src/Particle.mm:360-362)
+    const int ny = ngy + 2 * ngb;
     for (int i = 0; i <= order; ++i)
       for (int j = 0; j <= order; ++j) {
         int ii = ix[k] + (i - ngb), jj = iy[k] + (j - ngb);
+        // nodes past the array carry weight 0 (particle exactly on the far wall)
+        if (ii < 0 || jj < 0 || ii > nx || jj > ny) continue;
         acc[ii + jj * (nx + 1)] += quant40(wx[i] * wy[j]);
       }
   }
@@ -627,13 +630,14 @@ void or_det_deposit_j(int order, int ngx, int ngy, int ngb, int n, const int32_t
     shape_build(order, ox[k], wx2);
     shape_build(order, hy2, wy2);
     const float ux = vx[k] * inv_c, uy = vy[k] * inv_c;
+    const int ny = ngy + 2 * ngb;
     for (int i = 0; i <= order; ++i)
       for (int j = 0; j <= order; ++j) {
         int ii = i1 + (i - ngb + 1), jj = iy[k] + (j - ngb);
-        accx[ii + jj * (nx + 2)] += quant40((wx1[i] * wy1[j]) * ux);
+        if (ii >= 0 && jj >= 0 && ii <= nx + 1 && jj <= ny) accx[ii + jj * (nx + 2)] += quant40((wx1[i] * wy1[j]) * ux);
         ii = ix[k] + (i - ngb);
         jj = j2 + (j - ngb + 1);
-        accy[ii + jj * (nx + 1)] += quant40((wx2[i] * wy2[j]) * uy);
+        if (ii >= 0 && jj >= 0 && ii <= nx && jj <= ny + 1) accy[ii + jj * (nx + 1)] += quant40((wx2[i] * wy2[j]) * uy);
       }
   }
 }
@@ -650,6 +654,15 @@ void or_pcg_stream(uint64_t master_seed, uint64_t first_slot, int nslots, int nd
     RNGState r = st[first_slot + s];
     for (int d = 0; d < ndraws; ++d) out[size_t(s) * ndraws + d] = pcg32(r);
   }
+}
+
+void or_splitmix64_stream(uint64_t seed, int n, uint64_t* out) {
+  for (int i = 0; i < n; ++i) out[i] = splitmix64(seed);
+}
+
+void or_pcg32_raw(uint64_t state, uint64_t inc, int n, uint32_t* out) {
+  RNGState r{state, inc};
+  for (int i = 0; i < n; ++i) out[i] = pcg32(r);
 }
 
 double or_minstd_uniform(int count, double* out) {

@@ -243,18 +243,22 @@ inline void push_one(Particles<R>& P, size_t k, const R* Ex, const R* Ey, const 
   shape_ref<R>(prm.order, hv10, s10);
   shape_ref<R>(prm.order, hv11, s11);
   R Epx = 0, Epy = 0, Epz = 0, Bpx = 0, Bpy = 0, Bpz = 0;
-  const int nx = prm.ngx + 2 * prm.ngb;
+  const int nx = prm.ngx + 2 * prm.ngb, ny = prm.ngy + 2 * prm.ngb;
+  // A particle exactly on the far wall (loader draw of 1.0) reaches one node
+  // past the arrays with weight 0; such taps are skipped (the reference reads
+  // past its buffers there).
+  auto in = [](int a, int b, int w, int h) { return a >= 0 && b >= 0 && a < w && b < h; };
   for (int i = 0; i < prm.order + 1; i++) {
     for (int j = 0; j < prm.order + 1; j++) {
       int ii = i1 + (i - prm.ngb + 1);
       int jj = j1 + (j - prm.ngb);
-      Epx += s00[i] * s01[j] * Ex[ii + jj * (nx + 2)];
+      if (in(ii, jj, nx + 2, ny + 1)) Epx += s00[i] * s01[j] * Ex[ii + jj * (nx + 2)];
       ii = i2 + (i - prm.ngb);
       jj = j2 + (j - prm.ngb + 1);
-      Epy += s10[i] * s11[j] * Ey[ii + jj * (nx + 1)];
+      if (in(ii, jj, nx + 1, ny + 2)) Epy += s10[i] * s11[j] * Ey[ii + jj * (nx + 1)];
       ii = i1 + (i - prm.ngb + 1);
       jj = j2 + (j - prm.ngb + 1);
-      Bpz += s00[i] * s11[j] * Bz[ii + jj * (nx + 2)];
+      if (in(ii, jj, nx + 2, ny + 2)) Bpz += s00[i] * s11[j] * Bz[ii + jj * (nx + 2)];
     }
   }
   const R cE = R(prm.constE), cB = R(prm.constB);
@@ -346,19 +350,21 @@ inline void deposit_one(const Particles<R>& P, size_t k, const Grid& g, int orde
   shape_ref<R>(order, py - R(j1), s01);
   shape_ref<R>(order, px - R(i2), s10);
   shape_ref<R>(order, yh - R(j2), s11);
-  const int nx = g.nx();
+  const int nx = g.nx(), ny = g.ny();
+  auto in = [](int a, int b, int w, int h) { return a >= 0 && b >= 0 && a < w && b < h; };
   for (int i = 0; i < order + 1; i++) {
     for (int j = 0; j < order + 1; j++) {
       int ii = i2 + (i - g.ngb);
       int jj = j1 + (j - g.ngb);
-      rho[ii + jj * (nx + 1)] += s10[i] * s01[j] * scale;
+      // nodes past the arrays carry weight 0 (particle exactly on the far wall)
+      if (in(ii, jj, nx + 1, ny + 1)) rho[ii + jj * (nx + 1)] += s10[i] * s01[j] * scale;
       if (current) {
         ii = i1 + (i - g.ngb + 1);
         jj = j1 + (j - g.ngb);
-        jx[ii + jj * (nx + 2)] += s00[i] * s01[j] * scale * P.vx[k];
+        if (in(ii, jj, nx + 2, ny + 1)) jx[ii + jj * (nx + 2)] += s00[i] * s01[j] * scale * P.vx[k];
         ii = i2 + (i - g.ngb);
         jj = j2 + (j - g.ngb + 1);
-        jy[ii + jj * (nx + 1)] += s10[i] * s11[j] * scale * P.vy[k];
+        if (in(ii, jj, nx + 1, ny + 2)) jy[ii + jj * (nx + 1)] += s10[i] * s11[j] * scale * P.vy[k];
       }
     }
   }
@@ -1061,7 +1067,9 @@ void moments(const Particles<R>& P, const Grid& g, int order, float scale, float
     float vx = float(P.vx[k]), vy = float(P.vy[k]), vz = float(P.vz[k]);
     for (int i = 0; i < order + 1; i++)
       for (int j = 0; j < order + 1; j++) {
-        int idx = (i1 + (i - g.ngb)) + (j1 + (j - g.ngb)) * (nx + 1);
+        const int ii = i1 + (i - g.ngb), jj = j1 + (j - g.ngb);
+        if (ii < 0 || jj < 0 || ii > nx || jj > g.ny()) continue;
+        int idx = ii + jj * (nx + 1);
         float s = sx[i] * sy[j];
         out[0][idx] += s * scale;
         out[1][idx] += s * vx;
