@@ -134,6 +134,9 @@ class ClockSampler:
     def stop(self):
         if not self.proc:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        t_end = time.time() + 3.0
+        while len(self.lines) < 3 and time.time() < t_end and self.proc.poll() is None:
+            time.sleep(0.05)  # short timed regions: keep at least a few samples
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
@@ -248,6 +251,13 @@ def run_b200(args):
     barrier()
     clk = clocks.stop()
     n1 = sim.count(0) + sim.count(1)
+    if args.quick:  # profiling runs: the timed cycles only
+        if rank == 0:
+            print(json.dumps({"quick": True, "ms_per_step": ms / args.steps, "particles": n1,
+                              "pushes_per_s": 0.5 * (n0 + n1) * args.steps / (ms / 1e3),
+                              "gpu_launches": launches}), flush=True)
+        sim.close()
+        return 0
     ms_max = ms
     if pg:
         t = torch.tensor([ms], device="cuda", dtype=torch.float64)
@@ -357,6 +367,7 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--ref-ppc", type=int, default=16)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--quick", action="store_true", help="timed cycles only (for profiler runs)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

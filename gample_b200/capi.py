@@ -18,7 +18,7 @@ LIB_PATH = os.path.join(HERE, "libgample_b200.so")
 GP_OK = 0
 GP_ERR = {1: "argument", 2: "config", 3: "cuda", 4: "capacity", 5: "internal"}
 FIELDS = {"rho": 0, "Ex": 1, "Ey": 2, "Bz": 3, "jx": 4, "jy": 5, "phi": 6, "sol": 7}
-PHASES = ("deposit", "solve", "push", "reduce", "sources")
+PHASES = ("deposit", "solve", "push", "reduce", "sources", "sort")
 
 
 class GpParticleState(C.Structure):
@@ -179,7 +179,7 @@ class Sim:
         check(lib().gp_sim_set_profiling(self.h, int(on)))
 
     def phase_times(self):
-        out = (C.c_double * 5)()
+        out = (C.c_double * 6)()
         check(lib().gp_sim_phase_times(self.h, out))
         return dict(zip(PHASES, list(out)))
 

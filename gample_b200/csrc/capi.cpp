@@ -237,7 +237,7 @@ gp_status gp_sim_set_profiling(gp_sim* sim, int on) {
     return GP_OK;
   });
 }
-gp_status gp_sim_phase_times(gp_sim* sim, double out[5]) {
+gp_status gp_sim_phase_times(gp_sim* sim, double out[6]) {
   return guarded([&] {
     if (!out) throw std::invalid_argument("null output");
     S(sim).phase_times(out);
@@ -363,12 +363,13 @@ gp_status gp_particle_download_raw(gp_sim* sim, int s, int32_t* cell, float* ox,
     auto cp = [&](void* dst, const void* src, size_t elem) {
       if (dst && cnt) GP_CUDA(cudaMemcpyAsync(dst, src, cnt * elem, cudaMemcpyDeviceToHost, p->stream));
     };
-    cp(cell, p->cell.get(), 4);
-    cp(ox, p->ox.get(), 4);
-    cp(oy, p->oy.get(), 4);
-    cp(vx, p->vx.get(), 4);
-    cp(vy, p->vy.get(), 4);
-    cp(vz, p->vz.get(), 4);
+    const auto a = p->arrays();
+    cp(cell, a.cell, 4);
+    cp(ox, a.ox, 4);
+    cp(oy, a.oy, 4);
+    cp(vx, a.vx, 4);
+    cp(vy, a.vy, 4);
+    cp(vz, a.vz, 4);
     GP_CUDA(cudaStreamSynchronize(p->stream));
     return GP_OK;
   });

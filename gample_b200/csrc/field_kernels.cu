@@ -44,6 +44,17 @@ struct AccList {
   const long long* p[4];
   double f[4];
 };
+struct AccListD {
+  const double* p[4];
+};
+
+__global__ void k_combine_f64(AccListD a, int ns, size_t n, float* out) {
+  for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x) {
+    double v = 0.0;
+    for (int s = 0; s < ns; ++s) v = __dadd_rn(v, a.p[s][i]);
+    out[i] = __double2float_rn(v);
+  }
+}
 
 __global__ void k_combine(AccList a, int ns, size_t n, float* out) {
   for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x) {
@@ -289,6 +300,14 @@ void combine_fixed_point(const long long* const* acc, const float* scales, int n
     a.f[i] = double(scales[i]) * 0x1p-40 * extra;
   }
   k_combine<<<grid1d(n), 256, 0, s>>>(a, ns, n, out);
+  GP_LAUNCH_CHECK();
+}
+
+void combine_f64(const double* const* acc, int ns, size_t n, float* out, cudaStream_t s) {
+  AccListD a{};
+  if (ns > 4) throw std::invalid_argument("at most 4 species");
+  for (int i = 0; i < ns; ++i) a.p[i] = acc[i];
+  k_combine_f64<<<grid1d(n), 256, 0, s>>>(a, ns, n, out);
   GP_LAUNCH_CHECK();
 }
 

@@ -48,6 +48,7 @@ struct SpeciesCounters {
   uint32_t invalid;  // flagged for a non-finite or out-of-grid state
   uint32_t n_injected;
   uint32_t n_pulled; // removed by the last compaction (which consumes n_dead)
+  uint32_t n_slow;   // pushed without a shared-memory window (chunk too spread out)
   double ke;         // sum of 0.5 m v^2 w over particles still live (erg)
 };
 
@@ -59,11 +60,15 @@ struct PushConsts {
   double ke_half_m, ke_w;                // 0.5 * m and w for the kinetic energy
 };
 
+// Per-species charge / current accumulators (reference extents). Fast mode:
+// FP64 sums of the FP32 contributions w_x w_y q w / (dx dy) (times v for the
+// currents). Deterministic mode: exact int64 sums of the weights quantised to
+// 2^-40 (currents: of w_x w_y v / c). combine_* turns them into rho/jx/jy.
 struct DepositTargets {
-  float* rho;
-  float* jx;
-  float* jy;
-  long long* acc_rho;  // deterministic mode: per-species fixed-point sums
+  double* f64_rho;
+  double* f64_jx;
+  double* f64_jy;
+  long long* acc_rho;
   long long* acc_jx;
   long long* acc_jy;
 };
@@ -79,6 +84,10 @@ struct FieldPtrs {
 // is read from counters->n; optionally deposits the new positions (live
 // particles only). Writes the dead bitmap (bit k = particle k flagged) and
 // the flag counters, and accumulates the kinetic energy of live particles.
+// Each CTA takes a chunk of consecutive particles, stages the field window
+// covering their stencils in shared memory and accumulates the deposit in a
+// shared-memory window flushed with one global atomic per touched node; the
+// chunks are compact in space because the particles are tile-sorted.
 void push(int order, int boris_order, bool deposit, bool det, bool current, bool bz_uniform, GridDims g,
           ParticleArrays p, FieldPtrs f, PushConsts c, DepositTargets d, SpeciesCounters* counters,
           uint32_t* dead_bits, uint32_t n_bound, cudaStream_t s);
@@ -88,6 +97,14 @@ void push(int order, int boris_order, bool deposit, bool det, bool current, bool
 // [n - n_injected, n).
 void deposit(int order, bool det, bool current, GridDims g, ParticleArrays p, float scale, DepositTargets d,
              const SpeciesCounters* counters, uint32_t n_bound, bool injected_only, cudaStream_t s);
+
+// Counting sort of particles [0, counters->n) by spatial tile (tile x tile
+// cells, row-major over tiles) from src into dst. Order inside a tile is
+// unspecified. bins/offsets hold sort_bins(g, tile) + 1 words each.
+int sort_tile_size(GridDims g);
+int sort_bins(GridDims g, int tile);
+void sort_by_tile(GridDims g, int tile, ParticleArrays src, ParticleArrays dst, const SpeciesCounters* counters,
+                  uint32_t* bins, uint32_t* offsets, uint32_t n_bound, cudaStream_t s);
 
 // Remove flagged particles, filling each hole (ascending) with the last
 // live particle (descending) -- the permutation of src/Particle.mm:893-966.
@@ -140,6 +157,8 @@ void zero_f32(float* p, size_t n, cudaStream_t s);
 // (species in order); same for the currents with an extra factor c.
 void combine_fixed_point(const long long* const* acc, const float* scales, int nspecies, size_t n, double extra,
                          float* out, cudaStream_t s);
+// rho = sum_s acc_s (FP64, species in order), rounded to float.
+void combine_f64(const double* const* acc, int nspecies, size_t n, float* out, cudaStream_t s);
 // Ghost-charge folding (src/EMField.mm:751-850).
 void fold_ghosts(float* rho, GridDims g, const int fbc[4], cudaStream_t s);
 

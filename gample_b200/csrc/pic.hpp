@@ -91,7 +91,10 @@ class EMField {
 
   DeviceArray<float> rho, jx, jy, Ex, Ey, Ez, Bx, By, Bz;
   DeviceArray<double> phi, sol, b, diag;  // diag: [0..1] rhs sums [2..3] E sums [4] cathode mean [5..7] probe
+  // per-species deposit accumulators: int64 fixed point (deterministic mode)
+  // or FP64 (fast mode); combined into rho/jx/jy by finalizeCharge()
   std::vector<DeviceArray<long long>> acc_rho, acc_jx, acc_jy;
+  std::vector<DeviceArray<double>> f64_rho, f64_jx, f64_jy;
   std::vector<float> species_scale;
   std::unique_ptr<PoissonMG> mg;
   double lastEE = 0;
@@ -123,8 +126,14 @@ class Particle {
   void setPNum(uint32_t n);
   void upload_aos(const kern::ParticleStateAoS* host, uint32_t n);
   void download_aos(kern::ParticleStateAoS* host, uint32_t n);
-  kern::ParticleArrays arrays() const;
+  kern::ParticleArrays arrays() const;  // the current buffer
   kern::SpeciesCounters counters();  // synchronous
+  // Reorder the particles by spatial tile (counting sort into the spare
+  // buffer, then swap). The order of particles is otherwise unspecified.
+  void sort();
+  bool needs_sort = true;
+  int sort_interval = 0;  // cycles between sorts; 0 = when too many chunks miss their window
+  int cycles_since_sort = 0;
 
   std::string pName;
   int index = 0;
@@ -138,15 +147,23 @@ class Particle {
   uint32_t last_pulled = 0;
   double last_dt = 0;
 
-  DeviceArray<int32_t> cell;
-  DeviceArray<float> ox, oy, vx, vy, vz;
-  DeviceArray<uint32_t> dead_bits, scratch;
+  struct Buffer {
+    DeviceArray<int32_t> cell;
+    DeviceArray<float> ox, oy, vx, vy, vz;
+    void alloc(size_t n);
+    kern::ParticleArrays view() const;
+  };
+  Buffer buf[2];
+  int cur = 0;
+  DeviceArray<uint32_t> dead_bits, scratch, sort_bins, sort_offsets;
   DeviceArray<kern::SpeciesCounters> cnt;
   cudaStream_t stream;
 
  private:
   PinnedArray<kern::SpeciesCounters> host_cnt_;
   double dx_ = 0, dy_ = 0;
+  kern::GridDims dims_{};
+  int sort_tile_ = 8;
 };
 
 class Collision {

@@ -158,13 +158,22 @@ EMField::EMField(const Init& init, cudaStream_t s, int nspecies) : stream(s), ho
   acc_rho.resize(nspecies);
   acc_jx.resize(nspecies);
   acc_jy.resize(nspecies);
+  f64_rho.resize(nspecies);
+  f64_jx.resize(nspecies);
+  f64_jy.resize(nspecies);
   species_scale.assign(nspecies, 0.0f);
-  if (det) {
-    for (int sp = 0; sp < nspecies; ++sp) {
+  for (int sp = 0; sp < nspecies; ++sp) {
+    if (det) {
       acc_rho[sp].resize(n_rho(), true);
       if (current) {
         acc_jx[sp].resize(n_ex(), true);
         acc_jy[sp].resize(n_ey(), true);
+      }
+    } else {
+      f64_rho[sp].resize(n_rho(), true);
+      if (current) {
+        f64_jx[sp].resize(n_ex(), true);
+        f64_jy[sp].resize(n_ey(), true);
       }
     }
   }
@@ -191,13 +200,15 @@ void EMField::load1dField(const std::string& path, std::vector<float>& out, size
 
 kern::DepositTargets EMField::targets(int s) {
   kern::DepositTargets t{};
-  t.rho = rho.get();
-  t.jx = jx.get();
-  t.jy = jy.get();
-  if (det && s >= 0 && s < int(acc_rho.size())) {
+  if (s < 0 || s >= int(acc_rho.size())) throw std::invalid_argument("species index out of range");
+  if (det) {
     t.acc_rho = acc_rho[s].get();
     t.acc_jx = current ? acc_jx[s].get() : nullptr;
     t.acc_jy = current ? acc_jy[s].get() : nullptr;
+  } else {
+    t.f64_rho = f64_rho[s].get();
+    t.f64_jx = current ? f64_jx[s].get() : nullptr;
+    t.f64_jy = current ? f64_jy[s].get() : nullptr;
   }
   return t;
 }
@@ -206,29 +217,45 @@ void EMField::resetChargeDensity() {
   rho.zero(stream);
   jx.zero(stream);
   jy.zero(stream);
-  if (det)
-    for (size_t s = 0; s < acc_rho.size(); ++s) {
-      acc_rho[s].zero(stream);
-      acc_jx[s].zero(stream);
-      acc_jy[s].zero(stream);
-    }
+  for (size_t s = 0; s < acc_rho.size(); ++s) {
+    acc_rho[s].zero(stream);
+    acc_jx[s].zero(stream);
+    acc_jy[s].zero(stream);
+    f64_rho[s].zero(stream);
+    f64_jx[s].zero(stream);
+    f64_jy[s].zero(stream);
+  }
   charge_dirty = false;
 }
 
 void EMField::finalizeCharge() {
-  if (!det || !charge_dirty) return;
+  if (!charge_dirty) return;
   charge_dirty = false;
   const int ns = int(acc_rho.size());
-  std::vector<const long long*> pr(ns), px(ns), py(ns);
-  for (int s = 0; s < ns; ++s) {
-    pr[s] = acc_rho[s].get();
-    px[s] = acc_jx[s].get();
-    py[s] = acc_jy[s].get();
-  }
-  kern::combine_fixed_point(pr.data(), species_scale.data(), ns, n_rho(), 1.0, rho.get(), stream);
-  if (current) {
-    kern::combine_fixed_point(px.data(), species_scale.data(), ns, n_ex(), phys::c, jx.get(), stream);
-    kern::combine_fixed_point(py.data(), species_scale.data(), ns, n_ey(), phys::c, jy.get(), stream);
+  if (det) {
+    std::vector<const long long*> pr(ns), px(ns), py(ns);
+    for (int s = 0; s < ns; ++s) {
+      pr[s] = acc_rho[s].get();
+      px[s] = acc_jx[s].get();
+      py[s] = acc_jy[s].get();
+    }
+    kern::combine_fixed_point(pr.data(), species_scale.data(), ns, n_rho(), 1.0, rho.get(), stream);
+    if (current) {
+      kern::combine_fixed_point(px.data(), species_scale.data(), ns, n_ex(), phys::c, jx.get(), stream);
+      kern::combine_fixed_point(py.data(), species_scale.data(), ns, n_ey(), phys::c, jy.get(), stream);
+    }
+  } else {
+    std::vector<const double*> pr(ns), px(ns), py(ns);
+    for (int s = 0; s < ns; ++s) {
+      pr[s] = f64_rho[s].get();
+      px[s] = f64_jx[s].get();
+      py[s] = f64_jy[s].get();
+    }
+    kern::combine_f64(pr.data(), ns, n_rho(), rho.get(), stream);
+    if (current) {
+      kern::combine_f64(px.data(), ns, n_ex(), jx.get(), stream);
+      kern::combine_f64(py.data(), ns, n_ey(), jy.get(), stream);
+    }
   }
 }
 

@@ -7,6 +7,19 @@
 
 namespace gample {
 
+void Particle::Buffer::alloc(size_t n) {
+  cell.resize(n);
+  ox.resize(n);
+  oy.resize(n);
+  vx.resize(n);
+  vy.resize(n);
+  vz.resize(n);
+}
+
+kern::ParticleArrays Particle::Buffer::view() const {
+  return kern::ParticleArrays{cell.get(), ox.get(), oy.get(), vx.get(), vy.get(), vz.get()};
+}
+
 Particle::Particle(const Init& init, int s, cudaStream_t st) : stream(st), host_cnt_(1) {
   if (s < 0 || s >= int(init.paramForParticle.size())) throw ConfigError("species index out of range");
   const ParamForParticle& pp = init.paramForParticle[s];
@@ -21,6 +34,7 @@ Particle::Particle(const Init& init, int s, cudaStream_t st) : stream(st), host_
   boris = fp.BorisOrder;
   dx_ = fp.dx;
   dy_ = fp.dy;
+  sort_interval = init.paramForComputing.sortInterval;
   if (boris != 2 && boris != 4 && boris != 6) throw ConfigError("BorisOrder must be 2, 4 or 6");
   // src/Particle.mm:459-514 (an unknown BC string is fatal there too)
   auto codes = init.particleBCCodes();
@@ -32,15 +46,19 @@ Particle::Particle(const Init& init, int s, cudaStream_t st) : stream(st), host_
   if (pp.pNum > pNumMax) throw ConfigError("pNum > pNumMax for " + pName);
   if (fp.ngx + 2 * fp.ngb + 2 > 65535 || fp.ngy + 2 * fp.ngb + 2 > 32767)
     throw ConfigError("grid too large for the packed cell index");
+  dims_.ngx = fp.ngx;
+  dims_.ngy = fp.ngy;
+  dims_.ngb = fp.ngb;
+  dims_.nx = fp.ngx + 2 * fp.ngb;
+  dims_.ny = fp.ngy + 2 * fp.ngb;
+  sort_tile_ = kern::sort_tile_size(dims_);
   const size_t cap = pNumMax;
-  cell.resize(cap);
-  ox.resize(cap);
-  oy.resize(cap);
-  vx.resize(cap);
-  vy.resize(cap);
-  vz.resize(cap);
+  buf[0].alloc(cap);
+  buf[1].alloc(cap);
   dead_bits.resize((cap + 31) / 32 + 1, true);
   scratch.resize(kern::compact_scratch_words(uint32_t(cap)), true);
+  sort_bins.resize(size_t(kern::sort_bins(dims_, sort_tile_)) + 1, true);
+  sort_offsets.resize(size_t(kern::sort_bins(dims_, sort_tile_)) + 1, true);
   cnt.resize(1, true);
   n_bound = 0;
   // The reference loads pNum particles on the CPU here (src/Particle.mm:568-597)
@@ -48,9 +66,7 @@ Particle::Particle(const Init& init, int s, cudaStream_t st) : stream(st), host_
   // (src/Collision.mm:315-336); the build loads only through Collision.
 }
 
-kern::ParticleArrays Particle::arrays() const {
-  return kern::ParticleArrays{cell.get(), ox.get(), oy.get(), vx.get(), vy.get(), vz.get()};
-}
+kern::ParticleArrays Particle::arrays() const { return buf[cur].view(); }
 
 kern::SpeciesCounters Particle::counters() {
   GP_CUDA(cudaMemcpyAsync(host_cnt_.get(), cnt.get(), sizeof(kern::SpeciesCounters), cudaMemcpyDeviceToHost,
@@ -83,6 +99,7 @@ void Particle::upload_aos(const kern::ParticleStateAoS* host, uint32_t n) {
     GP_CUDA(cudaStreamSynchronize(stream));
   }
   setPNum(n);
+  needs_sort = true;
 }
 
 void Particle::download_aos(kern::ParticleStateAoS* host, uint32_t n) {
@@ -91,6 +108,14 @@ void Particle::download_aos(kern::ParticleStateAoS* host, uint32_t n) {
   kern::soa_to_aos(arrays(), n, tmp.get(), stream);
   GP_CUDA(cudaMemcpyAsync(host, tmp.get(), size_t(n) * sizeof(*host), cudaMemcpyDeviceToHost, stream));
   GP_CUDA(cudaStreamSynchronize(stream));
+}
+
+void Particle::sort() {
+  kern::sort_by_tile(dims_, sort_tile_, buf[cur].view(), buf[1 - cur].view(), cnt.get(), sort_bins.get(),
+                     sort_offsets.get(), n_bound, stream);
+  cur = 1 - cur;
+  needs_sort = false;
+  cycles_since_sort = 0;
 }
 
 void Particle::update(double dt, EMField& fld, bool fused_deposit) {
@@ -106,11 +131,12 @@ void Particle::update(double dt, EMField& fld, bool fused_deposit) {
   c.ke_half_m = 0.5 * double(m);
   c.ke_w = double(w);
   fld.species_scale[index] = c.scale;
-  if (fused_deposit && fld.det) fld.charge_dirty = true;
+  if (fused_deposit) fld.charge_dirty = true;
   last_dt = dt;
   kern::FieldPtrs f{fld.Ex.get(), fld.Ey.get(), fld.Bz.get()};
   kern::push(order, boris, fused_deposit, fld.det, fld.current, fld.bz_uniform, fld.dims, arrays(), f, c,
              fld.targets(index), cnt.get(), dead_bits.get(), n_bound, stream);
+  ++cycles_since_sort;
 }
 
 FlowStats Particle::reduce(XmlLogger* logger) {
@@ -131,6 +157,13 @@ FlowStats Particle::reduce(XmlLogger* logger) {
   lastKE = c.ke;
   last_pulled = c.n_pulled;
   n_bound = c.n;
+  // Sort policy: a fixed interval, or when more than 2% of the particles
+  // were pushed without a shared-memory window (chunks spread out by drift,
+  // compaction and injection).
+  if (sort_interval > 0)
+    needs_sort = needs_sort || cycles_since_sort >= sort_interval;
+  else
+    needs_sort = needs_sort || double(c.n_slow) > 0.02 * double(c.n);
   if (logger && logger->on()) {
     // src/Particle.mm:990-1001
     std::map<std::string, std::string> data = {
@@ -152,7 +185,7 @@ FlowStats Particle::reduce(XmlLogger* logger) {
 void Particle::integrateChargeDensity(EMField& fld, bool injected_only) {
   const float scale = float(double(q * w) / (dx_ * dy_));  // src/Particle.mm:540
   fld.species_scale[index] = scale;
-  if (fld.det) fld.charge_dirty = true;
+  fld.charge_dirty = true;
   kern::deposit(order, fld.det, fld.current, fld.dims, arrays(), scale, fld.targets(index), cnt.get(), n_bound,
                 injected_only, stream);
 }

@@ -64,6 +64,8 @@ void Simulation::phase_times(double out[PH_COUNT]) {
 
 void Simulation::initialize() {
   // src/main.mm:114-141: the logger is still switched off here.
+  for (auto* p : ptrs)
+    if (p->needs_sort) p->sort();  // tile order for the freshly loaded particles
   field->resetChargeDensity();
   for (auto* p : ptrs) p->integrateChargeDensity(*field);
   last_solve = field->solvePoisson(0.0, logger.get());
@@ -100,6 +102,11 @@ void Simulation::cycle() {
   }
   if (fused) field->resetChargeDensity();
   for (size_t s = 0; s < ptrs.size(); ++s) {
+    if (ptrs[s]->needs_sort) {
+      mark(PH_SORT, true);
+      ptrs[s]->sort();
+      mark(PH_SORT, false);
+    }
     mark(PH_PUSH, true);
     ptrs[s]->update(dt, *field, fused);
     mark(PH_PUSH, false);

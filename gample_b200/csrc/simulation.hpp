@@ -21,7 +21,7 @@
 
 namespace gample {
 
-enum Phase { PH_DEPOSIT = 0, PH_SOLVE, PH_PUSH, PH_REDUCE, PH_SOURCE, PH_COUNT };
+enum Phase { PH_DEPOSIT = 0, PH_SOLVE, PH_PUSH, PH_REDUCE, PH_SOURCE, PH_SORT, PH_COUNT };
 
 class Simulation {
  public:
@@ -56,7 +56,7 @@ class Simulation {
   bool profiling_ = false;
   std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> events_;
   cudaEvent_t open_ = nullptr;
-  double acc_[PH_COUNT] = {0, 0, 0, 0, 0};
+  double acc_[PH_COUNT] = {0, 0, 0, 0, 0, 0};
 };
 
 }  // namespace gample

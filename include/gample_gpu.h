@@ -99,9 +99,9 @@ gp_status gp_sim_synchronize(gp_sim* sim);
 /* Device-side timing of whole cycles on the run's stream (CUDA events). */
 gp_status gp_sim_time_cycles(gp_sim* sim, int ncycles, float* ms);
 /* Per-phase device time accumulated while profiling is on (ms):
- * [0] deposit [1] field solve [2] push [3] reduce [4] sources. */
+ * [0] deposit [1] field solve [2] push [3] reduce [4] sources [5] tile sort. */
 gp_status gp_sim_set_profiling(gp_sim* sim, int on);
-gp_status gp_sim_phase_times(gp_sim* sim, double out[5]);
+gp_status gp_sim_phase_times(gp_sim* sim, double out[6]);
 
 /* ---- EMField ---- */
 gp_status gp_field_dims(const gp_sim* sim, int* ngx, int* ngy, int* ngb, int* nkx, int* nky);

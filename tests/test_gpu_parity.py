@@ -92,6 +92,10 @@ def test_push_matches_oracle(gpu, order, boris, bcs):
         assert not np.any(mism), np.nonzero(mism)
         live = (flag_g == 0) & (flag_r == 0)
         vth = np.sqrt(np.mean(r["vx"][live].astype(np.float64) ** 2)) + 1e-30
+        # thermal displacement per step in cells: the velocity tolerance below
+        # is relative to |v| + v_th, so positions get the same scale
+        cst = ora.species_consts(s)
+        dth_x, dth_y = vth * cst["constX"], vth * cst["constY"]
         for c in ("vx", "vy", "vz"):
             a = g[c][live].astype(np.float64)
             b = r[c][live].astype(np.float64)
@@ -112,8 +116,10 @@ def test_push_matches_oracle(gpu, order, boris, bcs):
         if pbx == "Reflect":
             reflected = np.sign(g["vx"][live]) != np.sign(o["vx"][live])
             dxg = np.where(reflected, dxr, dxg)  # reflection geometry covered by the flag/velocity checks
-        assert np.all(np.abs(dxg - dxr) <= 4 * ulp_x + 1e-5 * np.abs(dxr)), "x"
-        assert np.all(np.abs(dyg - dyr) <= 4 * ulp_y + 1e-5 * np.abs(dyr)), "y"
+        ex = np.abs(dxg - dxr) - (4 * ulp_x + 1e-5 * (np.abs(dxr) + dth_x))
+        ey = np.abs(dyg - dyr) - (4 * ulp_y + 1e-5 * (np.abs(dyr) + dth_y))
+        assert np.all(ex <= 0), ("x", np.max(ex), int(np.argmax(ex)))
+        assert np.all(ey <= 0), ("y", np.max(ey), int(np.argmax(ey)))
 
 
 # ---------------------------------------------------------------- deposit
@@ -190,6 +196,11 @@ def test_deposit_deterministic_bit_exact(gpu, order):
     assert rel_inf(got, ora64.field("rho"), e_only) < 1e-6
 
 
+def as_set(particles):
+    """Particle order is unspecified (tile sorts): compare as a sorted multiset."""
+    return np.sort(particles, order=["x", "y", "vx", "vy", "vz", "piflag"])
+
+
 def test_deterministic_run_is_reproducible(gpu):
     cond = condition(ngx=32, ngy=32, order=3, ppc=16, deposit_mode=1, bz_tesla=0.02, end=6)
     out = []
@@ -200,7 +211,7 @@ def test_deterministic_run_is_reproducible(gpu):
         out.append((sim.field("Ex"), sim.field("Ey"), sim.particles(0)))
     for a, b in zip(out[0][:2], out[1][:2]):
         assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
-    assert np.array_equal(out[0][2].view(np.uint8), out[1][2].view(np.uint8))
+    assert np.array_equal(as_set(out[0][2]).view(np.uint8), as_set(out[1][2]).view(np.uint8))
 
 
 # ---------------------------------------------------------------- Poisson
@@ -218,14 +229,19 @@ def test_poisson_residual_and_fields(gpu, xbc, ybc, ngx, ngy, order):
     st = sim.solve_poisson(0.0)
     assert st.error <= 1e-8
     folded = sim.field("rho")
+    # ghost folding is float arithmetic in the reference: bit-exact against
+    # the oracle's FP32 restatement
+    ora32 = L.OracleSim(ocfg.parse(cond), real64=False)
+    ora32.set_field("rho", rho)
+    ora32.solve_poisson(0.0, tol=1e-6)
+    assert np.array_equal(folded, ora32.field("rho").astype(np.float32))
     ora.set_field("rho", folded)
     sol = sim.field("sol").ravel()
     res = ora.poisson_residual(sol)
     assert res <= 1.05e-8, res
-    # E from the oracle's tight FP64 solve of the same folded charge
+    # E from the oracle's tight FP64 solve of the same charge
     ora.set_field("rho", rho)
     ora.solve_poisson(0.0, tol=1e-13)
-    np.testing.assert_allclose(sim.field("rho"), ora.field("rho").astype(np.float32), rtol=0, atol=1e-12)
     # a 1e-8 residual bounds the error only through the condition number
     for name in ("Ex", "Ey"):
         assert rel_inf(sim.field(name), ora.field(name)) < 1e-4, name
@@ -252,7 +268,8 @@ def test_compaction_reproduces_reference_permutation(gpu):
         sim.update(s, 4e-11, fused_deposit=False)
         before = sim.particles(s)
         nflag = int(np.count_nonzero(before["piflag"]))
-        assert nflag > 0
+        if s == 0:
+            assert nflag > 0  # hot electrons cross the walls; cold ions may not
         ora.set_particles(s, before["x"], before["y"], before["vx"], before["vy"], before["vz"],
                           piflag=before["piflag"], f32=True)
         fo = ora.reduce(s, faithful=False)
@@ -295,7 +312,7 @@ def test_fused_order_equals_reference_order(gpu):
         sim = capi.Sim(cond, reference_order=ref_order)
         sim.initialize()
         sim.run(5)
-        runs.append((sim.field("Ex"), sim.field("Ey"), sim.particles(0), sim.particles(1)))
+        runs.append((sim.field("Ex"), sim.field("Ey"), as_set(sim.particles(0)), as_set(sim.particles(1))))
     for a, b in zip(runs[0], runs[1]):
         assert np.array_equal(a.view(np.uint8), b.view(np.uint8))
 
@@ -303,7 +320,8 @@ def test_fused_order_equals_reference_order(gpu):
 def test_sources_match_oracle(gpu):
     src = [
         {"ParticleName": "ion_Xe1", "GenerateType": "uniformIonization", "SrcSetMethod": "Source[1/cm/s]",
-         "SrcValue": 4e21, "GeneratePosX": [0.02, 0.1], "GenerateTemp": 0.5, "GenTempForElectron": 10},
+         # src / w * dt = 1.5e18 / 1.5625e5 * 1e-11 ~ 96 pairs per cycle
+         "SrcValue": 1.5e18, "GeneratePosX": [0.02, 0.1], "GenerateTemp": 0.5, "GenTempForElectron": 10},
         {"ParticleName": "electron", "GenerateType": "hollow-cathode", "SrcSetMethod": "BoundaryCurrentAtXmax",
          "GeneratePosX": [0.15, 0.15], "GenerateTemp": 5},
     ]
