@@ -9,21 +9,31 @@ namespace gample {
 
 namespace {
 
+constexpr int kSmallPoints = 4096;       // levels at or below run in one CTA
+constexpr int kMaxSmallLevels = 16;
+constexpr int TX = 32, TY = 16, HALO = 4;  // smoother tile and halo (4 half-sweeps)
+constexpr int SW = TX + 2 * HALO, SH = TY + 2 * HALO;
+constexpr int kSmoothThreads = 256;
+constexpr int kSmallThreads = 1024;
+
+// state words (FP64): see multigrid.hpp
+enum { S_SUM = 0, S_SUM2, S_NORMB, S_REL, S_DONE, S_ITER, S_MEAN, S_COUNT };
+
 struct LevelDesc {
   int mx, my;
   int perx, pery;
   float cx, cy, cd;
 };
 
+__device__ __forceinline__ bool wrap(int& i, int n, int per) {
+  if (i >= 0 && i < n) return true;
+  if (!per) return false;
+  i = ((i % n) + n) % n;
+  return true;
+}
+
 __device__ __forceinline__ float ld(const float* u, const LevelDesc& d, int i, int j) {
-  if (i < 0 || i >= d.mx) {
-    if (!d.perx) return 0.0f;
-    i = (i + d.mx) % d.mx;
-  }
-  if (j < 0 || j >= d.my) {
-    if (!d.pery) return 0.0f;
-    j = (j + d.my) % d.my;
-  }
+  if (!wrap(i, d.mx, d.perx) || !wrap(j, d.my, d.pery)) return 0.0f;
   return u[i + j * d.mx];
 }
 
@@ -43,114 +53,8 @@ __device__ __forceinline__ double block_sum(double v, double* sh) {
   return r;
 }
 
-// r = b - A x in FP64 with the CSR row of src/EMField.mm:329-400
-// (diagonal, i-1, i+1, j-1, j+1); stores float(r) and sum(r), sum(r^2).
-__global__ void k_residual64(const double* __restrict__ x, const double* __restrict__ b, kern::PoissonLayout L,
-                             float* __restrict__ r32, double* sums) {
-  __shared__ double sh[32];
-  const int mx = L.nkx + 1, my = L.nky + 1, n = mx * my;
-  double s1 = 0.0, s2 = 0.0;
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-    const int i = k % mx, j = k / mx;
-    double ax = L.Cd * x[k];
-    if (i > 0)
-      ax += L.Cx * x[k - 1];
-    else if (L.periodic_x)
-      ax += L.Cx * x[k + L.nkx];
-    if (i < L.nkx)
-      ax += L.Cx * x[k + 1];
-    else if (L.periodic_x)
-      ax += L.Cx * x[k - L.nkx];
-    if (j > 0)
-      ax += L.Cy * x[k - mx];
-    else if (L.periodic_y)
-      ax += L.Cy * x[k + L.nky * mx];
-    if (j < L.nky)
-      ax += L.Cy * x[k + mx];
-    else if (L.periodic_y)
-      ax += L.Cy * x[k - L.nky * mx];
-    const double r = b[k] - ax;
-    r32[k] = float(r);
-    s1 += r;
-    s2 += r * r;
-  }
-  s1 = block_sum(s1, sh);
-  s2 = block_sum(s2, sh);
-  if (threadIdx.x == 0) {
-    atomicAdd(sums, s1);
-    atomicAdd(sums + 1, s2);
-  }
-}
-
-__global__ void k_sub_mean32(float* f, int n, const double* sums) {
-  const float m = float(sums[0] / double(n));
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) f[k] -= m;
-}
-
-__global__ void k_axpy(double* x, const float* e, int n) {
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) x[k] += double(e[k]);
-}
-
-__global__ void k_sum64(const double* x, int n, double* sums) {
-  __shared__ double sh[32];
-  double s = 0.0;
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) s += x[k];
-  s = block_sum(s, sh);
-  if (threadIdx.x == 0) atomicAdd(sums, s);
-}
-
-__global__ void k_sub_mean64(double* x, int n, const double* sums) {
-  const double m = sums[0] / double(n);
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) x[k] -= m;
-}
-
-// Red-black Gauss-Seidel half sweep: points with (i + j) % 2 == color.
-__global__ void k_smooth(float* __restrict__ u, const float* __restrict__ f, LevelDesc d, int color) {
-  const int hx = (d.mx + 1) / 2;
-  const int n = hx * d.my;
-  const float inv = 1.0f / d.cd;
-  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
-    const int j = t / hx;
-    const int i = 2 * (t % hx) + ((j + color) & 1);
-    if (i >= d.mx) continue;
-    const float s = d.cx * (ld(u, d, i - 1, j) + ld(u, d, i + 1, j)) + d.cy * (ld(u, d, i, j - 1) + ld(u, d, i, j + 1));
-    u[i + j * d.mx] = (f[i + j * d.mx] - s) * inv;
-  }
-}
-
-__global__ void k_residual32(const float* __restrict__ u, const float* __restrict__ f, float* __restrict__ r,
-                             LevelDesc d) {
-  const int n = d.mx * d.my;
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-    const int i = k % d.mx, j = k / d.mx;
-    const float au = d.cd * u[k] + d.cx * (ld(u, d, i - 1, j) + ld(u, d, i + 1, j)) +
-                     d.cy * (ld(u, d, i, j - 1) + ld(u, d, i, j + 1));
-    r[k] = f[k] - au;
-  }
-}
-
-// Full weighting; coarse I sits on fine 2I+1 (Dirichlet) or 2I (periodic).
-__global__ void k_restrict(const float* __restrict__ rf, LevelDesc fd, float* __restrict__ fc, LevelDesc cd) {
-  const int n = cd.mx * cd.my;
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-    const int I = k % cd.mx, J = k / cd.mx;
-    const int fi = fd.perx ? 2 * I : 2 * I + 1;
-    const int fj = fd.pery ? 2 * J : 2 * J + 1;
-    float s = 0.0f;
-#pragma unroll
-    for (int b = -1; b <= 1; ++b) {
-      const float wb = b == 0 ? 0.5f : 0.25f;
-#pragma unroll
-      for (int a = -1; a <= 1; ++a) {
-        const float wa = a == 0 ? 0.5f : 0.25f;
-        s += wa * wb * ld(rf, fd, fi + a, fj + b);
-      }
-    }
-    fc[k] = s;
-  }
-}
-
-// Bilinear interpolation of the coarse correction, added to the fine level.
+// Bilinear interpolation weights of fine index i from a coarse level
+// (coarse I on fine 2I+1 for Dirichlet, 2I for periodic).
 __device__ __forceinline__ void interp1d(int i, int per, int mc, int& i0, float& w0, int& i1, float& w1) {
   if (per) {
     if ((i & 1) == 0) {
@@ -180,25 +84,252 @@ __device__ __forceinline__ void interp1d(int i, int per, int mc, int& i0, float&
   }
 }
 
-__global__ void k_prolong(const float* __restrict__ uc, LevelDesc cd, float* __restrict__ uf, LevelDesc fd) {
-  const int n = fd.mx * fd.my;
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-    const int i = k % fd.mx, j = k / fd.mx;
-    int a0, a1, b0, b1;
-    float wa0, wa1, wb0, wb1;
-    interp1d(i, fd.perx, cd.mx, a0, wa0, a1, wa1);
-    interp1d(j, fd.pery, cd.my, b0, wb0, b1, wb1);
-    const float e = wb0 * (wa0 * uc[a0 + b0 * cd.mx] + wa1 * uc[a1 + b0 * cd.mx]) +
-                    wb1 * (wa0 * uc[a0 + b1 * cd.mx] + wa1 * uc[a1 + b1 * cd.mx]);
-    uf[k] += e;
+__device__ __forceinline__ float prolong_at(const float* uc, const LevelDesc& c, const LevelDesc& f, int i, int j) {
+  int a0, a1, b0, b1;
+  float wa0, wa1, wb0, wb1;
+  interp1d(i, f.perx, c.mx, a0, wa0, a1, wa1);
+  interp1d(j, f.pery, c.my, b0, wb0, b1, wb1);
+  return wb0 * (wa0 * uc[a0 + b0 * c.mx] + wa1 * uc[a1 + b0 * c.mx]) +
+         wb1 * (wa0 * uc[a0 + b1 * c.mx] + wa1 * uc[a1 + b1 * c.mx]);
+}
+
+// Full-weighting restriction of the residual f - A u at coarse (I, J).
+__device__ __forceinline__ float restrict_at(const float* u, const float* f, const LevelDesc& d, int I, int J) {
+  const int fi = d.perx ? 2 * I : 2 * I + 1;
+  const int fj = d.pery ? 2 * J : 2 * J + 1;
+  float s = 0.0f;
+#pragma unroll
+  for (int b = -1; b <= 1; ++b) {
+    const float wb = b == 0 ? 0.5f : 0.25f;
+#pragma unroll
+    for (int a = -1; a <= 1; ++a) {
+      const float wa = a == 0 ? 0.5f : 0.25f;
+      int i = fi + a, j = fj + b;
+      if (!wrap(i, d.mx, d.perx) || !wrap(j, d.my, d.pery)) continue;
+      const float au = d.cd * u[i + j * d.mx] + d.cx * (ld(u, d, i - 1, j) + ld(u, d, i + 1, j)) +
+                       d.cy * (ld(u, d, i, j - 1) + ld(u, d, i, j + 1));
+      s += wa * wb * (f[i + j * d.mx] - au);
+    }
+  }
+  return s;
+}
+
+// ---------------------------------------------------------------- outer loop
+__global__ void k_init(double* st, const double* sums_b) {
+  const double nb = sqrt(sums_b[1] > 0 ? sums_b[1] : 0.0);
+  for (int i = 0; i < S_COUNT; ++i) st[i] = 0.0;
+  st[S_NORMB] = nb;
+  // AMGCL clears x and returns for a zero right-hand side
+  if (nb < DBL_EPSILON) {
+    st[S_DONE] = 2.0;
+    st[S_REL] = nb;
   }
 }
 
-// Coarsest level: CG on (-A) u = -f in one block; work holds 3 vectors.
-__global__ void __launch_bounds__(1024) k_coarse_cg(float* u, const float* f, LevelDesc d, float* work, int maxit,
-                                                    float rtol) {
+__global__ void k_clear_if_zero_rhs(double* x, int n, const double* st) {
+  if (st[S_DONE] != 2.0) return;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) x[k] = 0.0;
+}
+
+// r = b - A x in FP64 with the CSR row of src/EMField.mm:329-400 (diagonal,
+// i-1, i+1, j-1, j+1); stores float(r) and accumulates sum r, sum r^2.
+__global__ void k_residual64(const double* __restrict__ x, const double* __restrict__ b, kern::PoissonLayout L,
+                             float* __restrict__ r32, double* st) {
   __shared__ double sh[32];
-  __shared__ double s_val;
+  if (st[S_DONE] != 0.0) return;
+  const int mx = L.nkx + 1, my = L.nky + 1, n = mx * my;
+  double s1 = 0.0, s2 = 0.0;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+    const int i = k % mx, j = k / mx;
+    double ax = L.Cd * x[k];
+    if (i > 0)
+      ax += L.Cx * x[k - 1];
+    else if (L.periodic_x)
+      ax += L.Cx * x[k + L.nkx];
+    if (i < L.nkx)
+      ax += L.Cx * x[k + 1];
+    else if (L.periodic_x)
+      ax += L.Cx * x[k - L.nkx];
+    if (j > 0)
+      ax += L.Cy * x[k - mx];
+    else if (L.periodic_y)
+      ax += L.Cy * x[k + L.nky * mx];
+    if (j < L.nky)
+      ax += L.Cy * x[k + mx];
+    else if (L.periodic_y)
+      ax += L.Cy * x[k - L.nky * mx];
+    const double r = b[k] - ax;
+    r32[k] = float(r);
+    s1 += r;
+    s2 += r * r;
+  }
+  s1 = block_sum(s1, sh);
+  s2 = block_sum(s2, sh);
+  if (threadIdx.x == 0) {
+    atomicAdd(st + S_SUM, s1);
+    atomicAdd(st + S_SUM2, s2);
+  }
+}
+
+// Convergence test (one thread): AMGCL's ||r|| / ||b|| <= tol or maxiter.
+__global__ void k_check(double* st, double tol, int maxiter, int n) {
+  if (st[S_DONE] != 0.0) return;
+  const double rel = sqrt(st[S_SUM2] > 0 ? st[S_SUM2] : 0.0) / st[S_NORMB];
+  st[S_REL] = rel;
+  if (!(rel > tol) || st[S_ITER] >= double(maxiter)) {
+    st[S_DONE] = 1.0;
+  } else {
+    st[S_ITER] += 1.0;
+    st[S_MEAN] = st[S_SUM] / double(n);
+  }
+  st[S_SUM] = 0.0;
+  st[S_SUM2] = 0.0;
+}
+
+__global__ void k_sub_mean32(float* f, int n, const double* st) {
+  if (st[S_DONE] != 0.0) return;
+  const float m = float(st[S_MEAN]);
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) f[k] -= m;
+}
+
+__global__ void k_sum64(const double* x, int n, double* out) {
+  __shared__ double sh[32];
+  double s = 0.0;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) s += x[k];
+  s = block_sum(s, sh);
+  if (threadIdx.x == 0) atomicAdd(out, s);
+}
+
+__global__ void k_sub_mean64(double* x, int n, const double* sum) {
+  const double m = sum[0] / double(n);
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) x[k] -= m;
+}
+
+// ---------------------------------------------------------------- large levels
+// Two red-black Gauss-Seidel iterations on a TX x TY tile, computed in shared
+// memory with a 4-point halo (each half-sweep invalidates one ring), so the
+// interior equals two global sweeps. PRE: starts from u = 0 (red, black, red,
+// black). Otherwise adds the bilinear prolongation of the coarse correction
+// first and sweeps black, red, black, red.
+// The result goes to u_out: CTAs read their halos from u, so u itself must
+// not change during the launch (u_out == u only when u is not read, PRE).
+template <bool PRE>
+__global__ void __launch_bounds__(kSmoothThreads) k_smooth_tile(const float* u, float* u_out,
+                                                                const float* __restrict__ f, LevelDesc d,
+                                                                const float* __restrict__ uc, LevelDesc c,
+                                                                const double* st) {
+  __shared__ float su[SH][SW + 1];
+  __shared__ float sf[SH][SW + 1];
+  __shared__ unsigned char s_in[SH][SW];
+  if (st[S_DONE] != 0.0) return;
+  const int x0 = blockIdx.x * TX - HALO, y0 = blockIdx.y * TY - HALO;
+  for (int e = threadIdx.x; e < SW * SH; e += kSmoothThreads) {
+    const int li = e % SW, lj = e / SW;
+    int gi = x0 + li, gj = y0 + lj;
+    const bool inside = wrap(gi, d.mx, d.perx) && wrap(gj, d.my, d.pery);
+    float uv = 0.0f, fv = 0.0f;
+    if (inside) {
+      fv = f[gi + gj * d.mx];
+      if (!PRE) uv = u[gi + gj * d.mx] + prolong_at(uc, c, d, gi, gj);
+    }
+    su[lj][li] = uv;
+    sf[lj][li] = fv;
+    s_in[lj][li] = inside ? 1 : 0;
+  }
+  __syncthreads();
+  const float inv = 1.0f / d.cd;
+#pragma unroll
+  for (int hs = 0; hs < 4; ++hs) {
+    const int color = PRE ? (hs & 1) : 1 - (hs & 1);
+    // points of this color in [1, SW-2] x [1, SH-2]
+    for (int e = threadIdx.x; e < (SW - 2) * (SH - 2) / 2 + SH; e += kSmoothThreads) {
+      const int lj = 1 + e / ((SW - 2) / 2);
+      if (lj > SH - 2) break;
+      const int k = e % ((SW - 2) / 2);
+      // global parity (x0 + li + y0 + lj) & 1 == color
+      const int par = (x0 + y0 + lj + 1) & 1;  // parity of li = 1
+      const int li = 1 + 2 * k + ((par ^ color) & 1);
+      if (li > SW - 2 || !s_in[lj][li]) continue;
+      const float s = d.cx * (su[lj][li - 1] + su[lj][li + 1]) + d.cy * (su[lj - 1][li] + su[lj + 1][li]);
+      su[lj][li] = (sf[lj][li] - s) * inv;
+    }
+    __syncthreads();
+  }
+  for (int e = threadIdx.x; e < TX * TY; e += kSmoothThreads) {
+    const int li = HALO + e % TX, lj = HALO + e / TX;
+    const int gi = x0 + li, gj = y0 + lj;
+    if (gi < d.mx && gj < d.my) u_out[gi + gj * d.mx] = su[lj][li];
+  }
+}
+
+__global__ void k_restrict(const float* __restrict__ u, const float* __restrict__ f, LevelDesc d, float* __restrict__ fc,
+                           LevelDesc c, const double* st) {
+  if (st[S_DONE] != 0.0) return;
+  const int n = c.mx * c.my;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
+    fc[k] = restrict_at(u, f, d, k % c.mx, k / c.mx);
+}
+
+// Generic (untiled) red-black half sweep, used for large levels whose shape
+// does not fit the tile kernel.
+__global__ void k_smooth_generic(float* __restrict__ u, const float* __restrict__ f, LevelDesc d, int color,
+                                 const double* st) {
+  if (st[S_DONE] != 0.0) return;
+  const int hx = (d.mx + 1) / 2;
+  const int n = hx * d.my;
+  const float inv = 1.0f / d.cd;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    const int j = t / hx;
+    const int i = 2 * (t % hx) + ((j + color) & 1);
+    if (i >= d.mx) continue;
+    const float s = d.cx * (ld(u, d, i - 1, j) + ld(u, d, i + 1, j)) + d.cy * (ld(u, d, i, j - 1) + ld(u, d, i, j + 1));
+    u[i + j * d.mx] = (f[i + j * d.mx] - s) * inv;
+  }
+}
+
+__global__ void k_prolong_generic(const float* __restrict__ uc, LevelDesc c, float* __restrict__ uf, LevelDesc d,
+                                  const double* st) {
+  if (st[S_DONE] != 0.0) return;
+  const int n = d.mx * d.my;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
+    uf[k] += prolong_at(uc, c, d, k % d.mx, k / d.mx);
+}
+
+__global__ void k_zero32(float* u, int n, const double* st) {
+  if (st[S_DONE] != 0.0) return;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) u[k] = 0.0f;
+}
+
+__global__ void k_add_x(double* x, const float* e, int n, const double* st) {
+  if (st[S_DONE] != 0.0) return;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) x[k] += double(e[k]);
+}
+
+// ---------------------------------------------------------------- small levels
+struct SmallLevels {
+  int count;  // levels ls .. ls+count-1
+  LevelDesc d[kMaxSmallLevels];
+  int off[kMaxSmallLevels];  // float offset of u; f at +n, r at +2n
+  int cg_off;                // 3 CG vectors of the coarsest level
+};
+
+__device__ void sm_smooth(float* u, const float* f, const LevelDesc& d, int color) {
+  const int hx = (d.mx + 1) / 2;
+  const int n = hx * d.my;
+  const float inv = 1.0f / d.cd;
+  for (int t = threadIdx.x; t < n; t += blockDim.x) {
+    const int j = t / hx;
+    const int i = 2 * (t % hx) + ((j + color) & 1);
+    if (i >= d.mx) continue;
+    const float s = d.cx * (ld(u, d, i - 1, j) + ld(u, d, i + 1, j)) + d.cy * (ld(u, d, i, j - 1) + ld(u, d, i, j + 1));
+    u[i + j * d.mx] = (f[i + j * d.mx] - s) * inv;
+  }
+  __syncthreads();
+}
+
+// CG on (-A) u = -f (shared memory); the doubly periodic system is solved in
+// the zero-mean subspace.
+__device__ void sm_coarse_cg(float* u, const float* f, const LevelDesc& d, float* work, double* sh, double* sval) {
   const int n = d.mx * d.my;
   float* r = work;
   float* p = work + n;
@@ -209,9 +340,9 @@ __global__ void __launch_bounds__(1024) k_coarse_cg(float* u, const float* f, Le
     double s = 0.0;
     for (int k = threadIdx.x; k < n; k += blockDim.x) s += f[k];
     s = block_sum(s, sh);
-    if (threadIdx.x == 0) s_val = s / n;
+    if (threadIdx.x == 0) *sval = s / n;
     __syncthreads();
-    mean = s_val;
+    mean = *sval;
   }
   double rr = 0.0;
   for (int k = threadIdx.x; k < n; k += blockDim.x) {
@@ -222,10 +353,11 @@ __global__ void __launch_bounds__(1024) k_coarse_cg(float* u, const float* f, Le
     rr += double(v) * v;
   }
   rr = block_sum(rr, sh);
-  if (threadIdx.x == 0) s_val = rr;
+  if (threadIdx.x == 0) *sval = rr;
   __syncthreads();
-  rr = s_val;
-  const double stop = double(rtol) * double(rtol) * rr;
+  rr = *sval;
+  const double stop = 1e-10 * rr;
+  const int maxit = 2 * n + 10 < 1000 ? 2 * n + 10 : 1000;
   for (int it = 0; it < maxit && rr > stop && rr > 0.0; ++it) {
     double pq = 0.0;
     for (int k = threadIdx.x; k < n; k += blockDim.x) {
@@ -236,9 +368,9 @@ __global__ void __launch_bounds__(1024) k_coarse_cg(float* u, const float* f, Le
       pq += double(p[k]) * double(-ap);
     }
     pq = block_sum(pq, sh);
-    if (threadIdx.x == 0) s_val = pq;
+    if (threadIdx.x == 0) *sval = pq;
     __syncthreads();
-    pq = s_val;
+    pq = *sval;
     if (!(pq > 0.0)) break;
     const float alpha = float(rr / pq);
     double rn = 0.0;
@@ -248,9 +380,9 @@ __global__ void __launch_bounds__(1024) k_coarse_cg(float* u, const float* f, Le
       rn += double(r[k]) * r[k];
     }
     rn = block_sum(rn, sh);
-    if (threadIdx.x == 0) s_val = rn;
+    if (threadIdx.x == 0) *sval = rn;
     __syncthreads();
-    rn = s_val;
+    rn = *sval;
     const float beta = float(rn / rr);
     rr = rn;
     for (int k = threadIdx.x; k < n; k += blockDim.x) p[k] = r[k] + beta * p[k];
@@ -260,15 +392,75 @@ __global__ void __launch_bounds__(1024) k_coarse_cg(float* u, const float* f, Le
     double s = 0.0;
     for (int k = threadIdx.x; k < n; k += blockDim.x) s += u[k];
     s = block_sum(s, sh);
-    if (threadIdx.x == 0) s_val = s / n;
+    if (threadIdx.x == 0) *sval = s / n;
     __syncthreads();
-    const float m = float(s_val);
+    const float m = float(*sval);
     for (int k = threadIdx.x; k < n; k += blockDim.x) u[k] -= m;
+    __syncthreads();
   }
 }
 
-int blocks_for(int n, int per_thread = 1) {
-  long long b = ((long long)n + 256LL * per_thread - 1) / (256LL * per_thread);
+// The V-cycle of every small level in one CTA: f of the first small level is
+// read from global memory, its correction u written back (and added to the
+// FP64 solution when it is the finest level).
+__global__ void __launch_bounds__(kSmallThreads) k_small_vcycle(SmallLevels S, const float* __restrict__ f_in,
+                                                                float* __restrict__ u_out, double* x, int nu_pre,
+                                                                int nu_post, const double* st) {
+  extern __shared__ float sm[];
+  __shared__ double sh[32];
+  __shared__ double sval;
+  if (st[S_DONE] != 0.0) return;
+  const LevelDesc& d0 = S.d[0];
+  const int n0 = d0.mx * d0.my;
+  for (int k = threadIdx.x; k < n0; k += blockDim.x) sm[S.off[0] + n0 + k] = f_in[k];
+  __syncthreads();
+  const int last = S.count - 1;
+  for (int l = 0; l < last; ++l) {
+    const LevelDesc& d = S.d[l];
+    const int n = d.mx * d.my;
+    float* u = sm + S.off[l];
+    float* f = u + n;
+    for (int k = threadIdx.x; k < n; k += blockDim.x) u[k] = 0.0f;
+    __syncthreads();
+    for (int it = 0; it < nu_pre; ++it) {
+      sm_smooth(u, f, d, 0);
+      sm_smooth(u, f, d, 1);
+    }
+    const LevelDesc& c = S.d[l + 1];
+    float* fc = sm + S.off[l + 1] + c.mx * c.my;
+    for (int k = threadIdx.x; k < c.mx * c.my; k += blockDim.x) fc[k] = restrict_at(u, f, d, k % c.mx, k / c.mx);
+    __syncthreads();
+  }
+  {
+    const LevelDesc& d = S.d[last];
+    const int n = d.mx * d.my;
+    float* u = sm + S.off[last];
+    sm_coarse_cg(u, u + n, d, sm + S.cg_off, sh, &sval);
+    __syncthreads();
+  }
+  for (int l = last - 1; l >= 0; --l) {
+    const LevelDesc& d = S.d[l];
+    const LevelDesc& c = S.d[l + 1];
+    const int n = d.mx * d.my;
+    float* u = sm + S.off[l];
+    float* f = u + n;
+    const float* uc = sm + S.off[l + 1];
+    for (int k = threadIdx.x; k < n; k += blockDim.x) u[k] += prolong_at(uc, c, d, k % d.mx, k / d.mx);
+    __syncthreads();
+    for (int it = 0; it < nu_post; ++it) {
+      sm_smooth(u, f, d, 1);
+      sm_smooth(u, f, d, 0);
+    }
+  }
+  for (int k = threadIdx.x; k < n0; k += blockDim.x) {
+    const float v = sm[S.off[0] + k];
+    u_out[k] = v;
+    if (x) x[k] += double(v);
+  }
+}
+
+int blocks_for(int n) {
+  long long b = ((long long)n + 255) / 256;
   if (b < 1) b = 1;
   return int(b < 2368 ? b : 2368);
 }
@@ -276,11 +468,12 @@ int blocks_for(int n, int per_thread = 1) {
 LevelDesc desc(const PoissonMG::Level& l) { return LevelDesc{l.mx, l.my, l.perx, l.pery, l.cx, l.cy, l.cd}; }
 
 bool can_coarsen(int n, bool per) { return per ? (n >= 4 && n % 2 == 0) : (n >= 3 && n % 2 == 1); }
+bool tiled(const PoissonMG::Level& l) { return l.mx >= SW && l.my >= SH && (!l.perx || l.mx % 2 == 0) && (!l.pery || l.my % 2 == 0); }
 
 }  // namespace
 
 PoissonMG::PoissonMG(const kern::PoissonLayout& L, int nu_pre, int nu_post)
-    : L_(L), nu_pre_(nu_pre), nu_post_(nu_post), sums_(2, true), host_(4) {
+    : L_(L), nu_pre_(nu_pre), nu_post_(nu_post), state_(S_COUNT, true), host_(S_COUNT) {
   if (!((L.fbc[0] == kern::FBC_PERIODIC_C) == (L.fbc[1] == kern::FBC_PERIODIC_C)) ||
       !((L.fbc[2] == kern::FBC_PERIODIC_C) == (L.fbc[3] == kern::FBC_PERIODIC_C)))
     throw std::invalid_argument("periodic field boundaries must be set on both walls of a direction");
@@ -302,8 +495,8 @@ PoissonMG::PoissonMG(const kern::PoissonLayout& L, int nu_pre, int nu_post)
     lv.cy = cy;
     lv.cd = -2.0f * (cx + cy);
     lv.u.resize(size_t(mx) * my, true);
+    lv.u2.resize(size_t(mx) * my, true);
     lv.f.resize(size_t(mx) * my, true);
-    lv.r.resize(size_t(mx) * my, true);
     lv_.push_back(std::move(lv));
     if (!(can_coarsen(mx, L.periodic_x) && can_coarsen(my, L.periodic_y))) break;
     if (size_t(mx) * my <= 16) break;
@@ -312,81 +505,144 @@ PoissonMG::PoissonMG(const kern::PoissonLayout& L, int nu_pre, int nu_post)
     cx *= 0.25f;
     cy *= 0.25f;
   }
+  // first level small enough for the single-CTA kernel (all levels below it too)
+  ls_ = int(lv_.size());
+  for (int l = 0; l < int(lv_.size()); ++l)
+    if (size_t(lv_[l].mx) * lv_[l].my <= size_t(kSmallPoints) && int(lv_.size()) - l <= kMaxSmallLevels) {
+      ls_ = l;
+      break;
+    }
+  if (ls_ == int(lv_.size())) ls_ = int(lv_.size()) - 1;  // coarsest larger than kSmallPoints: one-level CG kernel
+  size_t floats = 0;
+  for (int l = ls_; l < int(lv_.size()); ++l) floats += 3 * size_t(lv_[l].mx) * lv_[l].my;
   const Level& c = lv_.back();
-  cg_work_.resize(3 * size_t(c.mx) * c.my, true);
+  floats += 3 * size_t(c.mx) * c.my;
+  small_smem_ = floats * sizeof(float);
+  int dev = 0, maxsm = 0;
+  GP_CUDA(cudaGetDevice(&dev));
+  GP_CUDA(cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  if (small_smem_ + 1024 > size_t(maxsm))
+    throw std::invalid_argument("coarsest multigrid level too large (grid dimensions do not coarsen)");
+  GP_CUDA(cudaFuncSetAttribute(k_small_vcycle, cudaFuncAttributeMaxDynamicSharedMemorySize, int(small_smem_)));
+  x2_.resize(size_t(n_), true);
 }
 
-void PoissonMG::vcycle_level(int l, cudaStream_t s) {
-  Level& a = lv_[l];
-  const LevelDesc d = desc(a);
-  const int n = a.mx * a.my;
-  if (l + 1 == int(lv_.size())) {
-    const int maxit = n * 2 + 10 < 2000 ? n * 2 + 10 : 2000;
-    k_coarse_cg<<<1, 1024, 0, s>>>(a.u.get(), a.f.get(), d, cg_work_.get(), maxit, 1e-5f);
+void PoissonMG::vcycle(cudaStream_t s) {
+  double* st = state_.get();
+  const int nl = int(lv_.size());
+  // descent over the large levels
+  for (int l = 0; l < ls_; ++l) {
+    Level& a = lv_[l];
+    Level& b = lv_[l + 1];
+    const LevelDesc d = desc(a);
+    if (tiled(a) && nu_pre_ == 2) {
+      dim3 grid((a.mx + TX - 1) / TX, (a.my + TY - 1) / TY);
+      k_smooth_tile<true><<<grid, kSmoothThreads, 0, s>>>(a.u.get(), a.u.get(), a.f.get(), d, nullptr, d, st);
+      GP_LAUNCH_CHECK();
+    } else {
+      k_zero32<<<blocks_for(a.mx * a.my), 256, 0, s>>>(a.u.get(), a.mx * a.my, st);
+      GP_LAUNCH_CHECK();
+      for (int it = 0; it < nu_pre_; ++it) {
+        k_smooth_generic<<<blocks_for((a.mx + 1) / 2 * a.my), 256, 0, s>>>(a.u.get(), a.f.get(), d, 0, st);
+        GP_LAUNCH_CHECK();
+        k_smooth_generic<<<blocks_for((a.mx + 1) / 2 * a.my), 256, 0, s>>>(a.u.get(), a.f.get(), d, 1, st);
+        GP_LAUNCH_CHECK();
+      }
+    }
+    k_restrict<<<blocks_for(b.mx * b.my), 256, 0, s>>>(a.u.get(), a.f.get(), d, b.f.get(), desc(b), st);
     GP_LAUNCH_CHECK();
-    return;
   }
-  Level& b = lv_[l + 1];
-  const int hb = blocks_for((a.mx + 1) / 2 * a.my);
-  GP_CUDA(cudaMemsetAsync(a.u.get(), 0, size_t(n) * sizeof(float), s));
-  for (int it = 0; it < nu_pre_; ++it) {
-    k_smooth<<<hb, 256, 0, s>>>(a.u.get(), a.f.get(), d, 0);
+  // all small levels in one CTA
+  {
+    SmallLevels S{};
+    S.count = nl - ls_;
+    size_t off = 0;
+    for (int l = ls_; l < nl; ++l) {
+      S.d[l - ls_] = desc(lv_[l]);
+      S.off[l - ls_] = int(off);
+      off += 3 * size_t(lv_[l].mx) * lv_[l].my;
+    }
+    S.cg_off = int(off);
+    k_small_vcycle<<<1, kSmallThreads, small_smem_, s>>>(S, lv_[ls_].f.get(), lv_[ls_].u.get(), nullptr, nu_pre_,
+                                                        nu_post_, st);
     GP_LAUNCH_CHECK();
-    k_smooth<<<hb, 256, 0, s>>>(a.u.get(), a.f.get(), d, 1);
-    GP_LAUNCH_CHECK();
+    lv_[ls_].result_in_u2 = false;
   }
-  k_residual32<<<blocks_for(n), 256, 0, s>>>(a.u.get(), a.f.get(), a.r.get(), d);
-  GP_LAUNCH_CHECK();
-  k_restrict<<<blocks_for(b.mx * b.my), 256, 0, s>>>(a.r.get(), d, b.f.get(), desc(b));
-  GP_LAUNCH_CHECK();
-  vcycle_level(l + 1, s);
-  k_prolong<<<blocks_for(n), 256, 0, s>>>(b.u.get(), desc(b), a.u.get(), d);
-  GP_LAUNCH_CHECK();
-  for (int it = 0; it < nu_post_; ++it) {
-    k_smooth<<<hb, 256, 0, s>>>(a.u.get(), a.f.get(), d, 1);
-    GP_LAUNCH_CHECK();
-    k_smooth<<<hb, 256, 0, s>>>(a.u.get(), a.f.get(), d, 0);
-    GP_LAUNCH_CHECK();
+  // ascent
+  for (int l = ls_ - 1; l >= 0; --l) {
+    Level& a = lv_[l];
+    Level& b = lv_[l + 1];
+    const LevelDesc d = desc(a);
+    if (tiled(a) && nu_post_ == 2) {
+      dim3 grid((a.mx + TX - 1) / TX, (a.my + TY - 1) / TY);
+      k_smooth_tile<false><<<grid, kSmoothThreads, 0, s>>>(a.u.get(), a.u2.get(), a.f.get(), d, result(l + 1), desc(b),
+                                                            st);
+      GP_LAUNCH_CHECK();
+      a.result_in_u2 = true;
+    } else {
+      a.result_in_u2 = false;
+      k_prolong_generic<<<blocks_for(a.mx * a.my), 256, 0, s>>>(result(l + 1), desc(b), a.u.get(), d, st);
+      GP_LAUNCH_CHECK();
+      for (int it = 0; it < nu_post_; ++it) {
+        k_smooth_generic<<<blocks_for((a.mx + 1) / 2 * a.my), 256, 0, s>>>(a.u.get(), a.f.get(), d, 1, st);
+        GP_LAUNCH_CHECK();
+        k_smooth_generic<<<blocks_for((a.mx + 1) / 2 * a.my), 256, 0, s>>>(a.u.get(), a.f.get(), d, 0, st);
+        GP_LAUNCH_CHECK();
+      }
+    }
   }
 }
-
-void PoissonMG::vcycle(cudaStream_t s) { vcycle_level(0, s); }
 
 MGResult PoissonMG::solve(const double* b, const double* sums_b, double* x, double tol, int maxiter,
                           cudaStream_t s) {
   MGResult res;
-  GP_CUDA(cudaMemcpyAsync(host_.get(), sums_b, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
-  GP_CUDA(cudaStreamSynchronize(s));
-  res.norm_b = std::sqrt(host_[1] > 0 ? host_[1] : 0.0);
-  if (res.norm_b < DBL_EPSILON) {  // AMGCL clears x for a zero right-hand side
-    GP_CUDA(cudaMemsetAsync(x, 0, size_t(n_) * sizeof(double), s));
-    res.rel_residual = res.norm_b;
-    return res;
-  }
+  double* st = state_.get();
   Level& f = lv_[0];
   const bool singular = L_.periodic_x && L_.periodic_y;
-  for (int it = 0;; ++it) {
-    GP_CUDA(cudaMemsetAsync(sums_.get(), 0, 2 * sizeof(double), s));
-    k_residual64<<<blocks_for(n_), 256, 0, s>>>(x, b, L_, f.f.get(), sums_.get());
+  k_init<<<1, 1, 0, s>>>(st, sums_b);
+  GP_LAUNCH_CHECK();
+  k_clear_if_zero_rhs<<<blocks_for(n_), 256, 0, s>>>(x, n_, st);
+  GP_LAUNCH_CHECK();
+  auto residual_and_check = [&]() {
+    k_residual64<<<blocks_for(n_), 256, 0, s>>>(x, b, L_, f.f.get(), st);
     GP_LAUNCH_CHECK();
-    GP_CUDA(cudaMemcpyAsync(host_.get(), sums_.get(), 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
-    GP_CUDA(cudaStreamSynchronize(s));
-    res.rel_residual = std::sqrt(host_[1] > 0 ? host_[1] : 0.0) / res.norm_b;
-    res.iterations = it;
-    if (!(res.rel_residual > tol) || it >= maxiter) break;
-    if (singular) {
-      k_sub_mean32<<<blocks_for(n_), 256, 0, s>>>(f.f.get(), n_, sums_.get());
+    k_check<<<1, 1, 0, s>>>(st, tol, maxiter, n_);
+    GP_LAUNCH_CHECK();
+  };
+  residual_and_check();
+  // Batches of V-cycles without host synchronisation; every kernel returns at
+  // once after convergence. The batch size follows the last solve.
+  int batch = last_iters_ > 0 ? last_iters_ : 1;
+  int launched = 0;
+  for (;;) {
+    for (int i = 0; i < batch && launched < maxiter; ++i, ++launched) {
+      if (singular) {
+        k_sub_mean32<<<blocks_for(n_), 256, 0, s>>>(f.f.get(), n_, st);
+        GP_LAUNCH_CHECK();
+      }
+      vcycle(s);
+      k_add_x<<<blocks_for(n_), 256, 0, s>>>(x, result(0), n_, st);
       GP_LAUNCH_CHECK();
+      residual_and_check();
     }
-    vcycle_level(0, s);
-    k_axpy<<<blocks_for(n_), 256, 0, s>>>(x, f.u.get(), n_);
-    GP_LAUNCH_CHECK();
+    GP_CUDA(cudaMemcpyAsync(host_.get(), st, S_COUNT * sizeof(double), cudaMemcpyDeviceToHost, s));
+    GP_CUDA(cudaStreamSynchronize(s));
+    if (host_[S_DONE] != 0.0 || launched >= maxiter) break;
+    batch = 1;
   }
-  if (singular) {
-    GP_CUDA(cudaMemsetAsync(sums_.get(), 0, sizeof(double), s));
-    k_sum64<<<blocks_for(n_), 256, 0, s>>>(x, n_, sums_.get());
+  res.norm_b = host_[S_NORMB];
+  res.rel_residual = host_[S_REL];
+  res.iterations = int(host_[S_ITER]);
+  if (host_[S_DONE] == 2.0) {
+    res.iterations = 0;
+    return res;
+  }
+  last_iters_ = res.iterations > 0 ? res.iterations : 1;
+  if (singular) {  // gauge: zero-mean solution
+    GP_CUDA(cudaMemsetAsync(st + S_SUM, 0, sizeof(double), s));
+    k_sum64<<<blocks_for(n_), 256, 0, s>>>(x, n_, st + S_SUM);
     GP_LAUNCH_CHECK();
-    k_sub_mean64<<<blocks_for(n_), 256, 0, s>>>(x, n_, sums_.get());
+    k_sub_mean64<<<blocks_for(n_), 256, 0, s>>>(x, n_, st + S_SUM);
     GP_LAUNCH_CHECK();
   }
   return res;

@@ -10,9 +10,17 @@
 //   _phi_sol), r = b - A x in FP64, e = V-cycle(r) in FP32, x += e,
 //   until ||r||_2 / ||b||_2 <= tol (AMGCL's relative-residual criterion).
 // Levels: vertex-centred coarsening (Dirichlet n -> (n-1)/2, periodic
-// n -> n/2) while both directions allow it; red-black Gauss-Seidel
-// smoothing, full-weighting restriction, bilinear prolongation,
-// re-discretised coarse operators, single-block CG on the coarsest level.
+// n -> n/2) while both directions allow it; red-black Gauss-Seidel,
+// full-weighting restriction, bilinear prolongation, re-discretised coarse
+// operators. Kernels per V-cycle:
+//   large levels (> kSmallPoints points): one pre-smoothing launch (two
+//     red-black sweeps in a shared-memory tile with a 4-point halo), one
+//     residual + restriction launch, one prolongation + post-smoothing launch;
+//   all small levels: one single-CTA kernel running the rest of the V-cycle
+//     in shared memory (coarsest level by CG).
+// The FP64 update + residual and the convergence test run on the device;
+// the host synchronises once per solve (it batches as many V-cycles as the
+// previous solve needed and re-checks).
 #pragma once
 
 #include <cuda_runtime.h>
@@ -38,25 +46,29 @@ class PoissonMG {
   // b, x: device FP64 vectors of unknowns(); sums_b[0..1] = sum(b), sum(b^2)
   // already on the device (from kern::build_rhs). x is updated in place.
   MGResult solve(const double* b, const double* sums_b, double* x, double tol, int maxiter, cudaStream_t s);
-  // One V-cycle on the FP32 rhs in level 0's f; result in level 0's u.
-  void vcycle(cudaStream_t s);
 
   struct Level {
     int mx, my;
     bool perx, pery;
     float cx, cy, cd;
-    DeviceArray<float> u, f, r;
+    DeviceArray<float> u, u2, f;  // u2: output of the tiled post-smoother
+    bool result_in_u2 = false;    // where the level's final correction is
   };
   const std::vector<Level>& level_info() const { return lv_; }
+  int first_small_level() const { return ls_; }
 
  private:
-  void vcycle_level(int l, cudaStream_t s);
+  void vcycle(cudaStream_t s);
+  const float* result(int l) const { return lv_[l].result_in_u2 ? lv_[l].u2.get() : lv_[l].u.get(); }
   kern::PoissonLayout L_;
   int n_;
   int nu_pre_, nu_post_;
+  int ls_ = 0;              // first level handled by the single-CTA kernel
+  size_t small_smem_ = 0;   // its shared-memory bytes
+  int last_iters_ = 2;
   std::vector<Level> lv_;
-  DeviceArray<double> sums_;     // [0] sum r, [1] sum r^2
-  DeviceArray<float> cg_work_;   // coarsest-level CG vectors
+  DeviceArray<double> x2_;      // ping-pong buffer of the FP64 update
+  DeviceArray<double> state_;   // [0] sum r [1] sum r^2 [2] ||b|| [3] rel res [4] done [5] iterations [6] mean r
   PinnedArray<double> host_;
 };
 

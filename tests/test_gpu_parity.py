@@ -101,9 +101,12 @@ def test_push_matches_oracle(gpu, order, boris, bcs):
             b = r[c][live].astype(np.float64)
             assert np.all(np.abs(a - b) <= 1e-5 * (np.abs(b) + vth)), c
         # positions: compare displacement (reference FP32 positions carry an
-        # ulp of rounding per step; the build's cell+offset does not)
-        ulp_x = np.spacing(np.abs(xr[live]).astype(np.float32)).astype(np.float64)
-        ulp_y = np.spacing(np.abs(yr[live]).astype(np.float32)).astype(np.float64)
+        # ulp of rounding per step, and its periodic wrap fmod(x + ngx - ngb,
+        # ngx) rounds at ulp(x + ngx); the build's cell+offset wrap is exact)
+        px = 32.0 if xbc == "periodic" else 0.0
+        py = 20.0 if ybc == "periodic" else 0.0
+        ulp_x = np.spacing((np.abs(xr[live]) + px).astype(np.float32)).astype(np.float64)
+        ulp_y = np.spacing((np.abs(yr[live]) + py).astype(np.float32)).astype(np.float64)
         dxg = g["x"][live].astype(np.float64) - x0[live]
         dxr = xr[live] - x0[live]
         dyg = g["y"][live].astype(np.float64) - y0[live]
