@@ -87,7 +87,7 @@ struct FieldPtrs {
 // Each CTA takes a chunk of consecutive particles, stages the field window
 // covering their stencils in shared memory and accumulates the deposit in a
 // shared-memory window flushed with one global atomic per touched node; the
-// chunks are compact in space because the particles are tile-sorted.
+// chunks are compact in space because the particles are cell-sorted.
 void push(int order, int boris_order, bool deposit, bool det, bool current, bool bz_uniform, GridDims g,
           ParticleArrays p, FieldPtrs f, PushConsts c, DepositTargets d, SpeciesCounters* counters,
           uint32_t* dead_bits, uint32_t n_bound, cudaStream_t s);
@@ -98,13 +98,13 @@ void push(int order, int boris_order, bool deposit, bool det, bool current, bool
 void deposit(int order, bool det, bool current, GridDims g, ParticleArrays p, float scale, DepositTargets d,
              const SpeciesCounters* counters, uint32_t n_bound, bool injected_only, cudaStream_t s);
 
-// Counting sort of particles [0, counters->n) by spatial tile (tile x tile
-// cells, row-major over tiles) from src into dst. Order inside a tile is
-// unspecified. bins/offsets hold sort_bins(g, tile) + 1 words each.
-int sort_tile_size(GridDims g);
-int sort_bins(GridDims g, int tile);
-void sort_by_tile(GridDims g, int tile, ParticleArrays src, ParticleArrays dst, const SpeciesCounters* counters,
-                  uint32_t* bins, uint32_t* offsets, uint32_t n_bound, cudaStream_t s);
+// Counting sort of particles [0, counters->n) by cell, in tile-major order
+// (8 x 8-cell tiles), from src into dst. Order inside a cell is unspecified.
+// scratch holds sort_scratch_words(g) words.
+size_t sort_key_count(GridDims g);
+size_t sort_scratch_words(GridDims g);
+void sort_by_cell(GridDims g, ParticleArrays src, ParticleArrays dst, const SpeciesCounters* counters,
+                  uint32_t* scratch, uint32_t n_bound, cudaStream_t s);
 
 // Remove flagged particles, filling each hole (ascending) with the last
 // live particle (descending) -- the permutation of src/Particle.mm:893-966.

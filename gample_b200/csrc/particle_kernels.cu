@@ -6,10 +6,9 @@
 //                     fused with the charge/current deposit of the new
 //                     positions (src/Particle.mm:281-389).
 //  k_pic<PUSH=false>  deposit of the current positions (src/Particle.mm:281-389).
-//  k_sort_*           counting sort of the particles by spatial tile.
 //
 // Work decomposition: one CTA per chunk of kChunk consecutive particles.
-// Because the particles are tile-sorted, a chunk covers a small box of cells;
+// Because the particles are cell-sorted, a chunk covers a small box of cells;
 // the CTA stages the field window of that box (Ex, Ey, Bz) in shared memory
 // and accumulates its deposit in a shared-memory window that is flushed with
 // one global atomic per touched node (FP64 per species, or exact int64 in the
@@ -35,6 +34,8 @@ constexpr int kPer = 8;                      // particles per thread
 constexpr int kChunk = kThreads * kPer;      // particles per CTA
 constexpr int kWin = 1600;                   // entries of a shared-memory window (e.g. 40 x 40)
 constexpr int kMargin = 2;                   // deposit-window margin for the motion of one step (cells)
+constexpr int kReach = 12;                   // window box: cells within kReach of the chunk's middle particle
+constexpr size_t kDepositBudget = 98304;     // shared-memory bytes for the deposit window copies
 
 __device__ __forceinline__ uint32_t warp_sum(uint32_t v) { return __reduce_add_sync(0xffffffffu, v); }
 __device__ __forceinline__ double warp_sum(double v) {
@@ -57,9 +58,16 @@ __device__ __forceinline__ void gadd(double* p, float v) { atomicAdd(p, double(v
 __device__ __forceinline__ void gadd(long long* p, long long v) {
   atomicAdd(reinterpret_cast<unsigned long long*>(p), static_cast<unsigned long long>(v));
 }
-__device__ __forceinline__ void sadd(float* p, float v) { atomicAdd(p, v); }
-__device__ __forceinline__ void sadd(long long* p, long long v) {
-  atomicAdd(reinterpret_cast<unsigned long long*>(p), static_cast<unsigned long long>(v));
+// Shared-memory windows hold exact fixed-point sums (weights quantised to
+// 2^-40) split over two 32-bit words per node: hi = q >> 20 (signed) and
+// lo = q & (2^20 - 1), each added with a native 32-bit integer atomic (the
+// floating-point and 64-bit shared-memory atomics are compare-and-swap
+// loops that retry under contention). A copy of a window receives at most
+// kChunk contributions per node, each with |q| <= 2^40, so neither word can
+// overflow; the flush recombines hi * 2^20 + lo in 64 bits.
+__device__ __forceinline__ void wadd(int* hi, int* lo, long long q) {
+  atomicAdd(hi, int(q >> 20));
+  atomicAdd(lo, int(q & 0xFFFFF));
 }
 
 // Contribution of one stencil node (rho and the two currents).
@@ -87,50 +95,122 @@ struct Window {  // shared-memory windows of one CTA (array-index coordinates)
   int mnx, mny, mxx, mxy;
   int gx0, gy0, gw, gh;  // gather window (origin, size)
   int dx0, dy0, dw, dh;  // deposit window
+  int ds;                // deposit window row stride (>= dw, congruent to ORDER + 1 mod 32)
 };
+
+// r[t] = w[(t + sh) mod N] for a per-lane shift sh in [0, N).
+template <int N>
+__device__ __forceinline__ void rotate(const float (&w)[N], int sh, float (&r)[N]) {
+#pragma unroll
+  for (int t = 0; t < N; ++t) {
+    float v = w[t];
+#pragma unroll
+    for (int q = 1; q < N; ++q)
+      if (sh == q) v = w[(t + q) % N];
+    r[t] = v;
+  }
+}
 
 // Deposit one particle's weights. WIN: into the shared-memory window;
 // otherwise global (CHECKED skips nodes outside the arrays, which carry
 // weight zero for a particle exactly on the far wall, src/Particle.mm:357-373).
+//
+// In the window each lane visits the (ORDER+1)^2 stencil nodes in its own
+// rotated order: lane L starts at node (L mod N, (L / N) mod N). Lanes of a
+// warp mostly share a cell (the particles are cell-sorted), so without the
+// rotation all 32 lanes would add to the same address at every step; with it
+// the first N^2 lanes add to distinct nodes, and the window row stride
+// (congruent to N mod 32) puts those nodes in distinct banks. The summands
+// are the same as in the unrotated loop; only their order of arrival differs.
+// |v / c| < 1 in FP32 for both components (always true without currents).
+template <bool CUR>
+__device__ __forceinline__ bool sublight(float vx, float vy) {
+  if constexpr (CUR) {
+    constexpr float inv_c = float(1.0 / 2.99792458e10);
+    return fabsf(__fmul_rn(vx, inv_c)) < 1.0f && fabsf(__fmul_rn(vy, inv_c)) < 1.0f;
+  } else {
+    return true;
+  }
+}
+
+__device__ __forceinline__ long long wsum(const int* s, int ihi, int ilo) {
+  return (static_cast<long long>(s[ihi]) << 20) + static_cast<long long>(static_cast<unsigned>(s[ilo]));
+}
+
+struct WinPtrs {  // this lane's copy of the window arrays (hi / lo words)
+  int *rho_hi, *rho_lo, *jx_hi, *jx_lo, *jy_hi, *jy_lo;
+};
+
+// The window path accumulates quant40(w) for rho and quant40(w * v / c) for
+// the currents in both deposit modes; the caller sends a particle with
+// |v| >= c (|w v / c| could exceed 1) to the global path instead.
 template <int ORDER, bool DET, bool CUR, bool WIN, bool CHECKED>
-__device__ __forceinline__ void deposit_one(const GridDims& g, const Window& w, const Stagger& sx, const Stagger& sy,
-                                            const float (&wxn)[ORDER + 1], const float (&wxh)[ORDER + 1],
-                                            const float (&wyn)[ORDER + 1], const float (&wyh)[ORDER + 1],
-                                            float scale, float vx, float vy, const DepositTargets& d,
-                                            typename AccT<DET>::type* sRho, typename AccT<DET>::type* sJx,
-                                            typename AccT<DET>::type* sJy) {
+__device__ __forceinline__ void deposit_one(const GridDims& g, const Window& w, int lane, const Stagger& sx,
+                                            const Stagger& sy, const float (&wxn)[ORDER + 1],
+                                            const float (&wxh)[ORDER + 1], const float (&wyn)[ORDER + 1],
+                                            const float (&wyh)[ORDER + 1], float scale, float vx, float vy,
+                                            const DepositTargets& d, const WinPtrs& s) {
   using C = Contrib<DET>;
+  constexpr int N = ORDER + 1;
+  constexpr float inv_c = float(1.0 / 2.99792458e10);
   const int ngb = g.ngb, nx = g.nx, ny = g.ny;
   const int rc = sx.node - ngb, rr = sy.node - ngb;  // rho / jy column base, rho / jx row base
+  const int xc = sx.half - ngb + 1, yr = sy.half - ngb + 1;  // jx column base, jy row base
+  if constexpr (WIN) {
+    const int si = lane % N, sj = (lane / N) % N;
+    float rxn[N], ryn[N];
+    rotate<N>(wxn, si, rxn);
+    rotate<N>(wyn, sj, ryn);
+    int col[N], row[N];
 #pragma unroll
-  for (int i = 0; i <= ORDER; ++i)
+    for (int t = 0; t < N; ++t) {
+      col[t] = t + si >= N ? t + si - N : t + si;
+      row[t] = (t + sj >= N ? t + sj - N : t + sj) * w.ds;
+    }
+    const int orho = (rc - w.dx0) + (rr - w.dy0) * w.ds;
 #pragma unroll
-    for (int j = 0; j <= ORDER; ++j) {
-      const auto v = C::rho(__fmul_rn(wxn[i], wyn[j]), scale);
-      if constexpr (WIN) {
-        sadd(sRho + (rc + i - w.dx0) + (rr + j - w.dy0) * w.dw, v);
-      } else {
+    for (int a = 0; a < N; ++a)
+#pragma unroll
+      for (int b = 0; b < N; ++b) {
+        const int o = orho + col[b] + row[a];
+        wadd(s.rho_hi + o, s.rho_lo + o, quant40(__fmul_rn(rxn[b], ryn[a])));
+      }
+    if constexpr (CUR) {
+      float rxh[N], ryh[N];
+      rotate<N>(wxh, si, rxh);
+      rotate<N>(wyh, sj, ryh);
+      const float ux = __fmul_rn(vx, inv_c), uy = __fmul_rn(vy, inv_c);
+      const int ojx = (xc - w.dx0) + (rr - w.dy0) * w.ds;
+      const int ojy = (rc - w.dx0) + (yr - w.dy0) * w.ds;
+#pragma unroll
+      for (int a = 0; a < N; ++a)
+#pragma unroll
+        for (int b = 0; b < N; ++b) {
+          const int ox = ojx + col[b] + row[a], oy = ojy + col[b] + row[a];
+          wadd(s.jx_hi + ox, s.jx_lo + ox, quant40(__fmul_rn(__fmul_rn(rxh[b], ryn[a]), ux)));
+          wadd(s.jy_hi + oy, s.jy_lo + oy, quant40(__fmul_rn(__fmul_rn(rxn[b], ryh[a]), uy)));
+        }
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i <= ORDER; ++i)
+#pragma unroll
+      for (int j = 0; j <= ORDER; ++j) {
+        const auto v = C::rho(__fmul_rn(wxn[i], wyn[j]), scale);
         if (CHECKED && !in_box(rc + i, rr + j, nx + 1, ny + 1)) continue;
         if constexpr (DET)
           gadd(d.acc_rho + (rc + i) + (rr + j) * (nx + 1), v);
         else
           gadd(d.f64_rho + (rc + i) + (rr + j) * (nx + 1), v);
       }
-    }
-  if constexpr (CUR) {
-    constexpr float inv_c = float(1.0 / 2.99792458e10);
-    const float ux = __fmul_rn(vx, inv_c), uy = __fmul_rn(vy, inv_c);
-    const int xc = sx.half - ngb + 1, yr = sy.half - ngb + 1;  // jx column base, jy row base
+    if constexpr (CUR) {
+      const float ux = __fmul_rn(vx, inv_c), uy = __fmul_rn(vy, inv_c);
 #pragma unroll
-    for (int i = 0; i <= ORDER; ++i)
+      for (int i = 0; i <= ORDER; ++i)
 #pragma unroll
-      for (int j = 0; j <= ORDER; ++j) {
-        const auto a = C::cur(__fmul_rn(wxh[i], wyn[j]), scale, vx, ux);
-        const auto b = C::cur(__fmul_rn(wxn[i], wyh[j]), scale, vy, uy);
-        if constexpr (WIN) {
-          sadd(sJx + (xc + i - w.dx0) + (rr + j - w.dy0) * w.dw, a);
-          sadd(sJy + (rc + i - w.dx0) + (yr + j - w.dy0) * w.dw, b);
-        } else {
+        for (int j = 0; j <= ORDER; ++j) {
+          const auto a = C::cur(__fmul_rn(wxh[i], wyn[j]), scale, vx, ux);
+          const auto b = C::cur(__fmul_rn(wxn[i], wyh[j]), scale, vy, uy);
           const bool oka = !CHECKED || in_box(xc + i, rr + j, nx + 2, ny + 1);
           const bool okb = !CHECKED || in_box(rc + i, yr + j, nx + 1, ny + 2);
           if constexpr (DET) {
@@ -141,7 +221,7 @@ __device__ __forceinline__ void deposit_one(const GridDims& g, const Window& w, 
             if (okb) gadd(d.f64_jy + (rc + i) + (yr + j) * (nx + 1), b);
           }
         }
-      }
+    }
   }
 }
 
@@ -212,26 +292,46 @@ __device__ __forceinline__ bool interior(const GridDims& g, int ix, int iy) {
   return ix >= g.ngb && ix < g.ngb + g.ngx && iy >= g.ngb && iy < g.ngb + g.ngy;
 }
 
-template <int ORDER, bool PUSH, bool DEP, bool DET, bool BZU>
-__host__ __device__ constexpr size_t smem_bytes(bool cur) {
-  return (PUSH ? (BZU ? 2 : 3) * size_t(kWin) * sizeof(float) : 0) +
-         (DEP ? (cur ? 3 : 1) * size_t(kWin) * (DET ? sizeof(long long) : sizeof(float)) : 0);
+// Deposit windows: each array has kCopies private copies, lane L adding into
+// copy (L / N^2) mod kCopies. With the rotated stencil order this gives the
+// 32 lanes of a warp whose particles share a cell 32 distinct addresses: N^2
+// distinct nodes per copy, and the copy stride (congruent to N^2 mod 32)
+// moves each copy onto its own banks. Copies are summed at the flush.
+template <int ORDER, bool CUR>
+struct DepositLayout {
+  static constexpr int kN2 = (ORDER + 1) * (ORDER + 1);
+  static constexpr int kStride = kWin + kN2 % 32;
+  static constexpr int kArrays = CUR ? 6 : 2;  // hi and lo words of rho (jx, jy)
+  static constexpr size_t kCopyBytes = size_t(kStride) * kArrays * sizeof(int);
+  static constexpr int copies() {
+    int c = kN2 >= 32 ? 1 : 32 / kN2;
+    while (c > 1 && size_t(c) * kCopyBytes > kDepositBudget) c >>= 1;
+    return c;
+  }
+  static constexpr int kCopies = copies();
+  static constexpr size_t kBytes = size_t(kCopies) * kCopyBytes;
+};
+
+template <int ORDER, bool PUSH, bool DEP, bool DET, bool CUR, bool BZU>
+__host__ __device__ constexpr size_t smem_bytes() {
+  return (PUSH ? (BZU ? 2 : 3) * size_t(kWin) * sizeof(float) : 0) + (DEP ? DepositLayout<ORDER, CUR>::kBytes : 0);
 }
 
 template <int ORDER, bool PUSH, bool DEP, bool DET, bool CUR, bool BZU>
-__global__ void __launch_bounds__(kThreads) k_pic(GridDims g, ParticleArrays p, FieldPtrs f, PushConsts c,
+__global__ void __launch_bounds__(kThreads, ORDER == 5 ? 2 : 3) k_pic(GridDims g, ParticleArrays p, FieldPtrs f, PushConsts c,
                                                   int boris_order, DepositTargets d, SpeciesCounters* cnt,
                                                   uint32_t* dead_bits, int injected_only) {
-  using Acc = typename AccT<DET>::type;
+  using DL = DepositLayout<ORDER, CUR>;
   extern __shared__ __align__(16) unsigned char smem[];
   float* sEx = reinterpret_cast<float*>(smem);
   float* sEy = sEx + (PUSH ? kWin : 0);
   float* sBz = sEy + (PUSH ? kWin : 0);
-  Acc* sRho = reinterpret_cast<Acc*>(smem + (PUSH ? (BZU ? 2 : 3) * size_t(kWin) * sizeof(float) : 0));
-  Acc* sJx = sRho + kWin;
-  Acc* sJy = sJx + kWin;
+  // copy c of array a starts at (a * kCopies + c) * kStride; arrays: rho hi,
+  // rho lo, jx hi, jx lo, jy hi, jy lo
+  int* sDep = reinterpret_cast<int*>(smem + (PUSH ? (BZU ? 2 : 3) * size_t(kWin) * sizeof(float) : 0));
   __shared__ int s_red[4][kThreads / 32];
   __shared__ Window s_w;
+  __shared__ int32_t s_ref;
 
   const uint32_t n = cnt->n;
   const uint32_t first = (!PUSH && injected_only) ? n - cnt->n_injected : 0u;
@@ -239,8 +339,28 @@ __global__ void __launch_bounds__(kThreads) k_pic(GridDims g, ParticleArrays p, 
   if (base >= n) return;  // uniform over the block
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   const int ngb = g.ngb;
+  const int copy = (lane / DL::kN2) % DL::kCopies;
+  WinPtrs sw;
+  sw.rho_hi = sDep + copy * DL::kStride;
+  sw.rho_lo = sDep + (DL::kCopies + copy) * DL::kStride;
+  sw.jx_hi = sDep + (2 * DL::kCopies + copy) * DL::kStride;
+  sw.jx_lo = sDep + (3 * DL::kCopies + copy) * DL::kStride;
+  sw.jy_hi = sDep + (4 * DL::kCopies + copy) * DL::kStride;
+  sw.jy_lo = sDep + (5 * DL::kCopies + copy) * DL::kStride;
 
-  // ---- phase A: bounding box of the chunk's cells (re-read from L1 below)
+  // ---- phase A: box of the chunk's cells (re-read from L1 below). Only
+  // particles within kReach cells of the chunk's middle particle count, so
+  // that a few strays (holes filled by compaction, injected particles) do not
+  // blow up the box; particles outside it use the global paths.
+  if (tid == 0) {
+    const uint32_t rest = n - base;
+    const int32_t rc = p.cell[base + (rest < uint32_t(kChunk) ? rest / 2 : uint32_t(kChunk / 2))];
+    s_ref = (rc >= 0 && interior(g, cell_ix(rc), cell_iy(rc))) ? rc : -1;
+  }
+  __syncthreads();
+  const int32_t ref = s_ref;
+  const int rx = ref >= 0 ? cell_ix(ref) : 0, ry = ref >= 0 ? cell_iy(ref) : 0;
+  const int reach = ref >= 0 ? kReach : INT_MAX / 2;
   int mnx = INT_MAX, mny = INT_MAX, mxx = INT_MIN, mxy = INT_MIN;
 #pragma unroll
   for (int i = 0; i < kPer; ++i) {
@@ -248,7 +368,7 @@ __global__ void __launch_bounds__(kThreads) k_pic(GridDims g, ParticleArrays p, 
     const int32_t cl = k < n ? p.cell[k] : -1;
     if (cl >= 0) {
       const int ix = cell_ix(cl), iy = cell_iy(cl);
-      if (interior(g, ix, iy)) {
+      if (interior(g, ix, iy) && abs(ix - rx) <= reach && abs(iy - ry) <= reach) {
         mnx = min(mnx, ix);
         mxx = max(mxx, ix);
         mny = min(mny, iy);
@@ -288,7 +408,8 @@ __global__ void __launch_bounds__(kThreads) k_pic(GridDims g, ParticleArrays p, 
       w.dy0 = w.gy0 - m;
       w.dw = w.gw + 2 * m;
       w.dh = w.gh + 2 * m;
-      w.use = (w.dw * w.dh <= kWin) ? 1 : 0;
+      w.ds = w.dw + (((ORDER + 1 - w.dw) % 32) + 32) % 32;
+      w.use = (w.ds * w.dh <= kWin && w.gw * w.gh <= kWin) ? 1 : 0;
     }
     s_w = w;
   }
@@ -307,13 +428,9 @@ __global__ void __launch_bounds__(kThreads) k_pic(GridDims g, ParticleArrays p, 
       }
     }
     if constexpr (DEP) {
-      for (int e = tid; e < w.dw * w.dh; e += kThreads) {
-        sRho[e] = Acc(0);
-        if constexpr (CUR) {
-          sJx[e] = Acc(0);
-          sJy[e] = Acc(0);
-        }
-      }
+      const int used = w.ds * w.dh;
+      for (int e = tid; e < DL::kArrays * DL::kCopies * used; e += kThreads)
+        sDep[(e / used) * DL::kStride + e % used] = 0;
     }
   }
   __syncthreads();
@@ -333,6 +450,7 @@ __global__ void __launch_bounds__(kThreads) k_pic(GridDims g, ParticleArrays p, 
         int ix = cell_ix(cell), iy = cell_iy(cell);
         float ox = p.ox[k], oy = p.oy[k];
         const bool inside = interior(g, ix, iy);
+        const bool in_box_win = w.use && ix >= w.mnx && ix <= w.mxx && iy >= w.mny && iy <= w.mxy;
         if constexpr (!PUSH) {
           const Stagger sx = stagger(ix, ox), sy = stagger(iy, oy);
           float wxn[ORDER + 1], wxh[ORDER + 1], wyn[ORDER + 1], wyh[ORDER + 1];
@@ -345,12 +463,12 @@ __global__ void __launch_bounds__(kThreads) k_pic(GridDims g, ParticleArrays p, 
             vx = p.vx[k];
             vy = p.vy[k];
           }
-          if (inside && w.use)
-            deposit_one<ORDER, DET, CUR, true, false>(g, w, sx, sy, wxn, wxh, wyn, wyh, c.scale, vx, vy, d, sRho, sJx, sJy);
+          if (in_box_win && sublight<CUR>(vx, vy))
+            deposit_one<ORDER, DET, CUR, true, false>(g, w, lane, sx, sy, wxn, wxh, wyn, wyh, c.scale, vx, vy, d, sw);
           else if (inside)
-            deposit_one<ORDER, DET, CUR, false, false>(g, w, sx, sy, wxn, wxh, wyn, wyh, c.scale, vx, vy, d, sRho, sJx, sJy);
+            deposit_one<ORDER, DET, CUR, false, false>(g, w, lane, sx, sy, wxn, wxh, wyn, wyh, c.scale, vx, vy, d, sw);
           else
-            deposit_one<ORDER, DET, CUR, false, true>(g, w, sx, sy, wxn, wxh, wyn, wyh, c.scale, vx, vy, d, sRho, sJx, sJy);
+            deposit_one<ORDER, DET, CUR, false, true>(g, w, lane, sx, sy, wxn, wxh, wyn, wyh, c.scale, vx, vy, d, sw);
         } else {
           float vx = p.vx[k], vy = p.vy[k], vz = p.vz[k];
           const Stagger sx = stagger(ix, ox), sy = stagger(iy, oy);
@@ -360,13 +478,13 @@ __global__ void __launch_bounds__(kThreads) k_pic(GridDims g, ParticleArrays p, 
           shape<ORDER>(sy.hnode, wyn);
           shape<ORDER>(sy.hhalf, wyh);
           float Epx = 0.0f, Epy = 0.0f, Bpz = 0.0f;
-          if (inside && w.use)
+          if (in_box_win)
             gather<ORDER, BZU, true, false>(g, f, w, sx, sy, wxn, wxh, wyn, wyh, sEx, sEy, sBz, Epx, Epy, Bpz);
           else if (inside)
             gather<ORDER, BZU, false, false>(g, f, w, sx, sy, wxn, wxh, wyn, wyh, sEx, sEy, sBz, Epx, Epy, Bpz);
           else
             gather<ORDER, BZU, false, true>(g, f, w, sx, sy, wxn, wxh, wyn, wyh, sEx, sEy, sBz, Epx, Epy, Bpz);
-          if (!w.use) nslow++;
+          if (!in_box_win) nslow++;
           if constexpr (BZU) Bpz = c.bz_uniform;
           // Boris push (src/Particle.mm:157-209); Ez, Bx, By are identically
           // zero in the reference's gather (:134-139).
@@ -446,12 +564,12 @@ __global__ void __launch_bounds__(kThreads) k_pic(GridDims g, ParticleArrays p, 
               }
               const bool in_win = w.use && ix >= w.mnx - kMargin && ix <= w.mxx + kMargin &&
                                   iy >= w.mny - kMargin && iy <= w.mxy + kMargin;
-              if (in_win)
-                deposit_one<ORDER, DET, CUR, true, false>(g, w, nsx, nsy, wxn, wxh, wyn, wyh, c.scale, vx, vy, d,
-                                                          sRho, sJx, sJy);
+              if (in_win && sublight<CUR>(vx, vy))
+                deposit_one<ORDER, DET, CUR, true, false>(g, w, lane, nsx, nsy, wxn, wxh, wyn, wyh, c.scale, vx, vy, d,
+                                                          sw);
               else
-                deposit_one<ORDER, DET, CUR, false, false>(g, w, nsx, nsy, wxn, wxh, wyn, wyh, c.scale, vx, vy, d,
-                                                           sRho, sJx, sJy);
+                deposit_one<ORDER, DET, CUR, false, false>(g, w, lane, nsx, nsy, wxn, wxh, wyn, wyh, c.scale, vx, vy, d,
+                                                           sw);
             }
           } else {
             p.cell[k] = -fl;
@@ -478,28 +596,38 @@ __global__ void __launch_bounds__(kThreads) k_pic(GridDims g, ParticleArrays p, 
     __syncthreads();
     if (w.use) {
       const int nx = g.nx, ny = g.ny;
-      for (int e = tid; e < w.dw * w.dh; e += kThreads) {
-        const int col = w.dx0 + e % w.dw, row = w.dy0 + e / w.dw;
-        const Acc r = sRho[e];
-        if (r != Acc(0) && in_box(col, row, nx + 1, ny + 1)) {
+      for (int e = tid; e < w.ds * w.dh; e += kThreads) {
+        if (e % w.ds >= w.dw) continue;  // stride padding, never written
+        const int col = w.dx0 + e % w.ds, row = w.dy0 + e / w.ds;
+        long long r = 0, a = 0, b = 0;
+#pragma unroll
+        for (int q = 0; q < DL::kCopies; ++q) {
+          r += wsum(sDep, (0 * DL::kCopies + q) * DL::kStride + e, (1 * DL::kCopies + q) * DL::kStride + e);
+          if constexpr (CUR) {
+            a += wsum(sDep, (2 * DL::kCopies + q) * DL::kStride + e, (3 * DL::kCopies + q) * DL::kStride + e);
+            b += wsum(sDep, (4 * DL::kCopies + q) * DL::kStride + e, (5 * DL::kCopies + q) * DL::kStride + e);
+          }
+        }
+        // fast mode: FP64 sums of w * scale (currents w * scale * v)
+        const double fr = double(c.scale) * 0x1p-40, fj = fr * 2.99792458e10;
+        if (r != 0 && in_box(col, row, nx + 1, ny + 1)) {
           if constexpr (DET)
             gadd(d.acc_rho + col + row * (nx + 1), r);
           else
-            gadd(d.f64_rho + col + row * (nx + 1), r);
+            atomicAdd(d.f64_rho + col + row * (nx + 1), double(r) * fr);
         }
         if constexpr (CUR) {
-          const Acc a = sJx[e], b = sJy[e];
-          if (a != Acc(0) && in_box(col, row, nx + 2, ny + 1)) {
+          if (a != 0 && in_box(col, row, nx + 2, ny + 1)) {
             if constexpr (DET)
               gadd(d.acc_jx + col + row * (nx + 2), a);
             else
-              gadd(d.f64_jx + col + row * (nx + 2), a);
+              atomicAdd(d.f64_jx + col + row * (nx + 2), double(a) * fj);
           }
-          if (b != Acc(0) && in_box(col, row, nx + 1, ny + 2)) {
+          if (b != 0 && in_box(col, row, nx + 1, ny + 2)) {
             if constexpr (DET)
               gadd(d.acc_jy + col + row * (nx + 1), b);
             else
-              gadd(d.f64_jy + col + row * (nx + 1), b);
+              atomicAdd(d.f64_jy + col + row * (nx + 1), double(b) * fj);
           }
         }
       }
@@ -529,7 +657,7 @@ template <int ORDER, bool PUSH, bool DEP, bool DET, bool CUR, bool BZU>
 void launch_pic(uint32_t nblocks, cudaStream_t s, GridDims g, ParticleArrays p, FieldPtrs f, PushConsts c, int boris,
                 DepositTargets d, SpeciesCounters* cnt, uint32_t* bits, int injected_only) {
   auto kern = k_pic<ORDER, PUSH, DEP, DET, CUR, BZU>;
-  constexpr size_t bytes = smem_bytes<ORDER, PUSH, DEP, DET, BZU>(CUR);
+  constexpr size_t bytes = smem_bytes<ORDER, PUSH, DEP, DET, CUR, BZU>();
   static bool configured = false;
   if (!configured) {
     GP_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)));
@@ -568,106 +696,6 @@ void dispatch_pic(bool dep, bool det, bool cur, bool bzu, uint32_t nblocks, cuda
 #undef GP_PIC
 }
 
-// ------------------------------------------------------------- tile sort
-constexpr int kSortThreads = 256;
-constexpr int kSortPer = 16;
-constexpr int kSortChunk = kSortThreads * kSortPer;
-
-__device__ __forceinline__ int tile_bin(int32_t cell, int tile, int ntx, int nbins) {
-  if (cell < 0) return nbins;  // flagged particles (none after compaction) go last
-  return (cell_iy(cell) / tile) * ntx + cell_ix(cell) / tile;
-}
-
-__global__ void __launch_bounds__(kSortThreads) k_sort_hist(const int32_t* cell, const SpeciesCounters* cnt, int tile,
-                                                            int ntx, int nbins, uint32_t* bins) {
-  extern __shared__ uint32_t sh[];
-  const uint32_t n = cnt->n;
-  const uint32_t base = blockIdx.x * uint32_t(kSortChunk);
-  if (base >= n) return;
-  for (int b = threadIdx.x; b <= nbins; b += kSortThreads) sh[b] = 0;
-  __syncthreads();
-  for (int i = 0; i < kSortPer; ++i) {
-    const uint32_t k = base + uint32_t(i * kSortThreads) + threadIdx.x;
-    if (k < n) atomicAdd(&sh[tile_bin(cell[k], tile, ntx, nbins)], 1u);
-  }
-  __syncthreads();
-  for (int b = threadIdx.x; b <= nbins; b += kSortThreads)
-    if (sh[b]) atomicAdd(&bins[b], sh[b]);
-}
-
-__global__ void __launch_bounds__(1024) k_sort_scan(const uint32_t* bins, uint32_t* offsets, int nb) {
-  __shared__ uint32_t s_warp[32];
-  __shared__ uint32_t s_base;
-  if (threadIdx.x == 0) s_base = 0;
-  __syncthreads();
-  for (int b0 = 0; b0 < nb; b0 += blockDim.x) {
-    const int b = b0 + threadIdx.x;
-    const uint32_t c = b < nb ? bins[b] : 0u;
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    uint32_t incl = c;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
-      if (lane >= o) incl += t;
-    }
-    if (lane == 31) s_warp[wid] = incl;
-    __syncthreads();
-    if (wid == 0) {
-      uint32_t x = s_warp[lane], xi = x;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        uint32_t t = __shfl_up_sync(0xffffffffu, xi, o);
-        if (lane >= o) xi += t;
-      }
-      s_warp[lane] = xi - x;
-    }
-    __syncthreads();
-    if (b < nb) offsets[b] = s_base + s_warp[wid] + incl - c;
-    __syncthreads();
-    if (threadIdx.x == blockDim.x - 1) s_base += s_warp[wid] + incl;
-    __syncthreads();
-  }
-}
-
-__global__ void __launch_bounds__(kSortThreads) k_sort_scatter(ParticleArrays src, ParticleArrays dst,
-                                                               const SpeciesCounters* cnt, int tile, int ntx, int nbins,
-                                                               uint32_t* offsets) {
-  extern __shared__ uint32_t sh[];
-  uint32_t* cntb = sh;              // nbins + 1
-  uint32_t* baseb = sh + nbins + 1;  // nbins + 1
-  const uint32_t n = cnt->n;
-  const uint32_t base = blockIdx.x * uint32_t(kSortChunk);
-  if (base >= n) return;
-  for (int b = threadIdx.x; b <= nbins; b += kSortThreads) cntb[b] = 0;
-  __syncthreads();
-  int bin[kSortPer];
-#pragma unroll
-  for (int i = 0; i < kSortPer; ++i) {
-    const uint32_t k = base + uint32_t(i * kSortThreads) + threadIdx.x;
-    bin[i] = k < n ? tile_bin(src.cell[k], tile, ntx, nbins) : -1;
-    if (bin[i] >= 0) atomicAdd(&cntb[bin[i]], 1u);
-  }
-  __syncthreads();
-  for (int b = threadIdx.x; b <= nbins; b += kSortThreads) {
-    const uint32_t c = cntb[b];
-    baseb[b] = c ? atomicAdd(&offsets[b], c) : 0u;
-    cntb[b] = 0;
-  }
-  __syncthreads();
-#pragma unroll
-  for (int i = 0; i < kSortPer; ++i) {
-    if (bin[i] < 0) continue;
-    const uint32_t k = base + uint32_t(i * kSortThreads) + threadIdx.x;
-    const uint32_t dpos = baseb[bin[i]] + atomicAdd(&cntb[bin[i]], 1u);
-    dst.cell[dpos] = src.cell[k];
-    dst.ox[dpos] = src.ox[k];
-    dst.oy[dpos] = src.oy[k];
-    dst.vx[dpos] = src.vx[k];
-    dst.vy[dpos] = src.vy[k];
-    dst.vz[dpos] = src.vz[k];
-  }
-}
-
 }  // namespace
 
 void push(int order, int boris_order, bool dep, bool det, bool cur, bool bzu, GridDims g, ParticleArrays p,
@@ -701,38 +729,6 @@ void deposit(int order, bool det, bool cur, GridDims g, ParticleArrays p, float 
     case 5: dispatch_pic<5, false>(true, det, cur, true, nblocks, s, g, p, f, c, 2, d, mc, nullptr, inj); break;
     default: throw std::invalid_argument("WeightingOrder must be 1, 3 or 5");
   }
-  GP_LAUNCH_CHECK();
-}
-
-int sort_bins(GridDims g, int tile) { return ((g.nx + tile) / tile) * ((g.ny + tile) / tile); }
-
-int sort_tile_size(GridDims g) {
-  int t = 8;
-  while (sort_bins(g, t) > 8192) t *= 2;
-  return t;
-}
-
-void sort_by_tile(GridDims g, int tile, ParticleArrays src, ParticleArrays dst, const SpeciesCounters* cnt,
-                  uint32_t* bins, uint32_t* offsets, uint32_t n_bound, cudaStream_t s) {
-  if (n_bound == 0) return;
-  const int ntx = (g.nx + tile) / tile;
-  const int nbins = sort_bins(g, tile);
-  const uint32_t nblocks = (n_bound + kSortChunk - 1) / kSortChunk;
-  static bool configured = false;
-  if (!configured) {  // up to 2 x 8193 bins of shared memory
-    GP_CUDA(cudaFuncSetAttribute(k_sort_hist, cudaFuncAttributeMaxDynamicSharedMemorySize, 8193 * 4));
-    GP_CUDA(cudaFuncSetAttribute(k_sort_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * 8193 * 4));
-    configured = true;
-  }
-  if (nbins > 8192) throw std::invalid_argument("sort tile too small for the grid");
-  GP_CUDA(cudaMemsetAsync(bins, 0, size_t(nbins + 1) * sizeof(uint32_t), s));
-  k_sort_hist<<<nblocks, kSortThreads, size_t(nbins + 1) * sizeof(uint32_t), s>>>(src.cell, cnt, tile, ntx, nbins,
-                                                                                  bins);
-  GP_LAUNCH_CHECK();
-  k_sort_scan<<<1, 1024, 0, s>>>(bins, offsets, nbins + 1);
-  GP_LAUNCH_CHECK();
-  k_sort_scatter<<<nblocks, kSortThreads, 2 * size_t(nbins + 1) * sizeof(uint32_t), s>>>(src, dst, cnt, tile, ntx,
-                                                                                         nbins, offsets);
   GP_LAUNCH_CHECK();
 }
 

@@ -128,12 +128,13 @@ class Particle {
   void download_aos(kern::ParticleStateAoS* host, uint32_t n);
   kern::ParticleArrays arrays() const;  // the current buffer
   kern::SpeciesCounters counters();  // synchronous
-  // Reorder the particles by spatial tile (counting sort into the spare
+  // Reorder the particles by cell (counting sort into the spare
   // buffer, then swap). The order of particles is otherwise unspecified.
   void sort();
   bool needs_sort = true;
   int sort_interval = 0;  // cycles between sorts; 0 = when too many chunks miss their window
   int cycles_since_sort = 0;
+  uint32_t slow_after_sort = 0;  // particles pushed outside their window right after the last sort
 
   std::string pName;
   int index = 0;
@@ -155,7 +156,7 @@ class Particle {
   };
   Buffer buf[2];
   int cur = 0;
-  DeviceArray<uint32_t> dead_bits, scratch, sort_bins, sort_offsets;
+  DeviceArray<uint32_t> dead_bits, scratch, sort_scratch;
   DeviceArray<kern::SpeciesCounters> cnt;
   cudaStream_t stream;
 
@@ -163,7 +164,6 @@ class Particle {
   PinnedArray<kern::SpeciesCounters> host_cnt_;
   double dx_ = 0, dy_ = 0;
   kern::GridDims dims_{};
-  int sort_tile_ = 8;
 };
 
 class Collision {

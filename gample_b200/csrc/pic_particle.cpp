@@ -51,14 +51,12 @@ Particle::Particle(const Init& init, int s, cudaStream_t st) : stream(st), host_
   dims_.ngb = fp.ngb;
   dims_.nx = fp.ngx + 2 * fp.ngb;
   dims_.ny = fp.ngy + 2 * fp.ngb;
-  sort_tile_ = kern::sort_tile_size(dims_);
   const size_t cap = pNumMax;
   buf[0].alloc(cap);
   buf[1].alloc(cap);
   dead_bits.resize((cap + 31) / 32 + 1, true);
   scratch.resize(kern::compact_scratch_words(uint32_t(cap)), true);
-  sort_bins.resize(size_t(kern::sort_bins(dims_, sort_tile_)) + 1, true);
-  sort_offsets.resize(size_t(kern::sort_bins(dims_, sort_tile_)) + 1, true);
+  sort_scratch.resize(kern::sort_scratch_words(dims_), true);
   cnt.resize(1, true);
   n_bound = 0;
   // The reference loads pNum particles on the CPU here (src/Particle.mm:568-597)
@@ -111,8 +109,7 @@ void Particle::download_aos(kern::ParticleStateAoS* host, uint32_t n) {
 }
 
 void Particle::sort() {
-  kern::sort_by_tile(dims_, sort_tile_, buf[cur].view(), buf[1 - cur].view(), cnt.get(), sort_bins.get(),
-                     sort_offsets.get(), n_bound, stream);
+  kern::sort_by_cell(dims_, buf[cur].view(), buf[1 - cur].view(), cnt.get(), sort_scratch.get(), n_bound, stream);
   cur = 1 - cur;
   needs_sort = false;
   cycles_since_sort = 0;
@@ -157,13 +154,15 @@ FlowStats Particle::reduce(XmlLogger* logger) {
   lastKE = c.ke;
   last_pulled = c.n_pulled;
   n_bound = c.n;
-  // Sort policy: a fixed interval, or when more than 2% of the particles
-  // were pushed without a shared-memory window (chunks spread out by drift,
-  // compaction and injection).
+  // Sort policy: a fixed interval, or when the particles pushed outside
+  // their chunk's shared-memory window (spread out by drift, compaction and
+  // injection) exceed those of the first push after the last sort by 2% of
+  // the live count.
+  if (cycles_since_sort == 1) slow_after_sort = c.n_slow;
   if (sort_interval > 0)
     needs_sort = needs_sort || cycles_since_sort >= sort_interval;
   else
-    needs_sort = needs_sort || double(c.n_slow) > 0.02 * double(c.n);
+    needs_sort = needs_sort || double(c.n_slow) > double(slow_after_sort) + 0.02 * double(c.n);
   if (logger && logger->on()) {
     // src/Particle.mm:990-1001
     std::map<std::string, std::string> data = {
