@@ -84,6 +84,8 @@ EXPORTS = {
     "gp_collision_artificial_ionization": (C.c_int, [C.c_void_p, C.c_double, C.POINTER(C.c_int)]),
     "gp_collision_hollow_cathode": (C.c_int, [C.c_void_p, C.c_double, C.POINTER(C.c_int)]),
     "gp_collision_flux_reinjection": (C.c_int, [C.c_void_p, C.c_double, C.POINTER(C.c_int)]),
+    "gp_deposit_charge_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_uint32, C.c_float,
+                                            C.c_void_p, C.c_void_p]),
     "gp_last_error": (C.c_char_p, []),
     "gp_version": (C.c_char_p, []),
     "gp_device_count": (C.c_int, []),

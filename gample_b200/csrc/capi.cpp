@@ -109,6 +109,21 @@ FieldBuf field_buf(gample::EMField& f, int which) {
 
 extern "C" {
 
+gp_status gp_deposit_charge_noalloc(int weighting_order, int ngx, int ngy, const gp_particle_state* particles,
+                                    uint32_t n, float scale, float* rho, void* stream) {
+  return guarded([&] {
+    try {
+      gample::kern::deposit_charge_noalloc(weighting_order, ngx, ngy,
+                                           reinterpret_cast<const gample::kern::ParticleStateAoS*>(particles), n,
+                                           scale, rho, static_cast<cudaStream_t>(stream));
+    } catch (const std::length_error& e) {
+      g_error = e.what();
+      return GP_ERR_CAPACITY;
+    }
+    return GP_OK;
+  });
+}
+
 const char* gp_last_error(void) { return g_error.c_str(); }
 unsigned long long gp_kernel_launches(void) { return gample::kernel_launches(); }
 const char* gp_version(void) { return "gample_b200 0.1 (sm_100a)"; }

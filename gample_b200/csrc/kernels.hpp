@@ -186,6 +186,14 @@ void gradient_energy(const double* phi, GridDims g, float dx, float dy, float* E
 // Probe values for the timeseries CSV (src/EMField.mm:1130-1134).
 void probe(const double* phi, const float* Ex, const float* Ey, GridDims g, double* out3, cudaStream_t s);
 
+// Charge density of one species from the reference's 24-byte records in
+// device memory into rho ((nx+1)(ny+1) floats), with no allocation: the int64
+// accumulator is a file-scope device array of noalloc_max_nodes() entries.
+// Throws std::length_error for a larger grid. Calls must not overlap in time.
+size_t noalloc_max_nodes();
+void deposit_charge_noalloc(int order, int ngx, int ngy, const ParticleStateAoS* particles, uint32_t n, float scale,
+                            float* rho, cudaStream_t s);
+
 // ------------------------------------------------------------- utilities
 void fill_f32(float* p, size_t n, float v, cudaStream_t s);
 void fill_f64(double* p, size_t n, double v, cudaStream_t s);

@@ -142,6 +142,33 @@ gp_status gp_collision_hollow_cathode(gp_sim* sim, double dt, int* addn);
  * build addition, no reference counterpart. */
 gp_status gp_collision_flux_reinjection(gp_sim* sim, double dt, int* addn);
 
+/* ---- allocation-free deposit (no reference counterpart) ----
+ * Charge density of one species, for callers that own all device memory and
+ * cannot let the library allocate (a fixed device-memory budget or their own
+ * pool, or a loop that must not pay cudaMalloc/cudaFree's implicit device
+ * synchronisation). No handle is needed and nothing is allocated.
+ *   particles  device pointer to n reference records (x, y in grid units
+ *              offset by ngb = order / 2, as src/Particle.mm:589-594 stores
+ *              them); records with piflag != 0 are skipped
+ *   scale      q * w / (dx * dy) of the species (src/Particle.mm:540)
+ *   rho        device pointer to (nx+1)(ny+1) floats, nx = ngx + 2 ngb,
+ *              ny = ngy + 2 ngb; overwritten (no ghost folding)
+ *   stream     cudaStream_t to run on (NULL = default stream)
+ * Arithmetic: the deterministic deposit of the handle API (weights quantised
+ * to 2^-40, exact int64 sums, one rounding to float), so the result is
+ * bit-identical to gp_particle_integrate_charge of the same species with
+ * DepositMode 1 in an otherwise empty field.
+ * Limit: (nx+1)(ny+1) <= 1048576 nodes (8 MiB of scratch held in a static
+ * device array); a larger grid returns GP_ERR_CAPACITY. The scratch is
+ * cleared by every call, so nothing needs to start at zero. The scratch is
+ * shared by all calls on a device: calls that overlap in time (other streams
+ * or host threads without ordering) race, so serialise them. The first call
+ * on each device looks up the scratch address (cudaGetSymbolAddress) and
+ * should come before any stream capture on that device. Asynchronous: errors
+ * of the kernels themselves surface at the next synchronisation. */
+gp_status gp_deposit_charge_noalloc(int weighting_order, int ngx, int ngy, const gp_particle_state* particles,
+                                    uint32_t n, float scale, float* rho, void* stream);
+
 /* ---- misc ---- */
 const char* gp_last_error(void);
 const char* gp_version(void);
