@@ -98,12 +98,17 @@ def load_peaks():
 
 
 def load_traffic():
-    """DRAM bytes per pushed particle of the push kernel from the committed ncu summary."""
+    """DRAM bytes per pushed particle of the push kernel, from the committed ncu
+    summary (a 64-ppc capture of the same kernel; traffic scales with the
+    particles processed)."""
     try:
-        with open(os.path.join(ROOT, "profiles", "push_es512_o3_traffic.json")) as f:
-            return json.load(f)
-    except Exception:
-        return None
+        with open(os.path.join(ROOT, "profiles", "push_es512_o3.md")) as f:
+            for line in f:
+                if line.startswith("dram_bytes_per_particle:"):
+                    return {"dram_bytes_per_particle": float(line.split(":", 1)[1])}
+    except OSError:
+        pass
+    return None
 
 
 class ClockSampler:
@@ -365,7 +370,7 @@ def main():
     ap.add_argument("--ppc", type=int, default=256)
     ap.add_argument("--cpu-ppc", type=int, default=256)
     ap.add_argument("--cpu-steps", type=int, default=2)
-    ap.add_argument("--ref-ppc", type=int, default=16)
+    ap.add_argument("--ref-ppc", type=int, default=128)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--quick", action="store_true", help="timed cycles only (for profiler runs)")
     args = ap.parse_args()
