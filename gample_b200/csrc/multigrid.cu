@@ -1,6 +1,7 @@
 // multigrid.cu -- geometric multigrid Poisson solver (sm_100a).
 #include "multigrid.hpp"
 
+#include <algorithm>
 #include <cfloat>
 #include <cmath>
 #include <stdexcept>
@@ -11,6 +12,7 @@ namespace {
 
 constexpr int kSmallPoints = 4096;       // levels at or below run in one CTA
 constexpr int kMaxSmallLevels = 16;
+constexpr int kDenseMax = 64;            // coarsest levels up to this size use a precomputed inverse
 constexpr int TX = 32, TY = 16, HALO = 4;  // smoother tile and halo (4 half-sweeps)
 constexpr int SW = TX + 2 * HALO, SH = TY + 2 * HALO;
 constexpr int kSmoothThreads = 256;
@@ -311,20 +313,119 @@ struct SmallLevels {
   LevelDesc d[kMaxSmallLevels];
   int off[kMaxSmallLevels];  // float offset of u; f at +n, r at +2n
   int cg_off;                // 3 CG vectors of the coarsest level
+  const float* cinv;         // dense inverse of the coarsest operator (nullptr: CG), staged at cg_off
 };
 
-__device__ void sm_smooth(float* u, const float* f, const LevelDesc& d, int color) {
-  const int hx = (d.mx + 1) / 2;
-  const int n = hx * d.my;
+// Small-level helpers for the single CTA of kSmallThreads = 32 x kRows
+// threads: thread (tx, ty) takes columns tx, tx + 32, ... of rows ty, ty + kRows,
+// ... (no integer division), and neighbours are read with explicit wraps.
+constexpr int kRows = kSmallThreads / 32;
+
+__device__ __forceinline__ float nb_sum(const float* u, const LevelDesc& d, int i, int j) {
+  const int k = i + j * d.mx;
+  const float l = i > 0 ? u[k - 1] : (d.perx ? u[k + d.mx - 1] : 0.0f);
+  const float r = i < d.mx - 1 ? u[k + 1] : (d.perx ? u[k - d.mx + 1] : 0.0f);
+  const float b = j > 0 ? u[k - d.mx] : (d.pery ? u[k + (d.my - 1) * d.mx] : 0.0f);
+  const float t = j < d.my - 1 ? u[k + d.mx] : (d.pery ? u[k - (d.my - 1) * d.mx] : 0.0f);
+  return d.cx * (l + r) + d.cy * (b + t);
+}
+
+__device__ void sb_smooth(float* u, const float* f, const LevelDesc& d, int color) {
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  const int hx = (d.mx + 1) >> 1;
   const float inv = 1.0f / d.cd;
-  for (int t = threadIdx.x; t < n; t += blockDim.x) {
-    const int j = t / hx;
-    const int i = 2 * (t % hx) + ((j + color) & 1);
-    if (i >= d.mx) continue;
-    const float s = d.cx * (ld(u, d, i - 1, j) + ld(u, d, i + 1, j)) + d.cy * (ld(u, d, i, j - 1) + ld(u, d, i, j + 1));
-    u[i + j * d.mx] = (f[i + j * d.mx] - s) * inv;
+  for (int j = ty; j < d.my; j += kRows) {
+    const int par = (j + color) & 1;
+    for (int h = tx; h < hx; h += 32) {
+      const int i = 2 * h + par;
+      if (i < d.mx) u[i + j * d.mx] = (f[i + j * d.mx] - nb_sum(u, d, i, j)) * inv;
+    }
   }
   __syncthreads();
+}
+
+__device__ void sb_zero(float* u, const LevelDesc& d) {
+  for (int k = threadIdx.x; k < d.mx * d.my; k += kSmallThreads) u[k] = 0.0f;
+  __syncthreads();
+}
+
+// r = f - A u, then full weighting of r onto the coarse right-hand side.
+__device__ void sb_restrict(const float* u, const float* f, float* r, const LevelDesc& d, float* fc,
+                            const LevelDesc& c) {
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  for (int j = ty; j < d.my; j += kRows)
+    for (int i = tx; i < d.mx; i += 32) {
+      const int k = i + j * d.mx;
+      r[k] = f[k] - (d.cd * u[k] + nb_sum(u, d, i, j));
+    }
+  __syncthreads();
+  for (int J = ty; J < c.my; J += kRows)
+    for (int I = tx; I < c.mx; I += 32) {
+      const int fi = d.perx ? 2 * I : 2 * I + 1;
+      const int fj = d.pery ? 2 * J : 2 * J + 1;
+      float s = 0.0f;
+#pragma unroll
+      for (int b = -1; b <= 1; ++b) {
+        int j = fj + b;
+        if (j < 0 || j >= d.my) {
+          if (!d.pery) continue;
+          j = j < 0 ? j + d.my : j - d.my;
+        }
+        const float wb = b == 0 ? 0.5f : 0.25f;
+#pragma unroll
+        for (int a = -1; a <= 1; ++a) {
+          int i = fi + a;
+          if (i < 0 || i >= d.mx) {
+            if (!d.perx) continue;
+            i = i < 0 ? i + d.mx : i - d.mx;
+          }
+          s += (a == 0 ? 0.5f : 0.25f) * wb * r[i + j * d.mx];
+        }
+      }
+      fc[I + J * c.mx] = s;
+    }
+  __syncthreads();
+}
+
+__device__ void sb_prolong_add(float* u, const LevelDesc& d, const float* uc, const LevelDesc& c) {
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  for (int j = ty; j < d.my; j += kRows)
+    for (int i = tx; i < d.mx; i += 32) u[i + j * d.mx] += prolong_at(uc, c, d, i, j);
+  __syncthreads();
+}
+
+// u = M (f - mean f) with M (in shared memory) the inverse of the coarsest
+// operator (of A + a 11^T for the doubly periodic one, whose zero-mean
+// solutions it returns).
+__device__ void sm_dense_solve(float* u, const float* f, const LevelDesc& d, const float* M, double* sh,
+                               double* sval) {
+  const int n = d.mx * d.my;
+  const bool singular = d.perx && d.pery;
+  float mean = 0.0f;
+  if (singular) {
+    double s = 0.0;
+    for (int k = threadIdx.x; k < n; k += blockDim.x) s += f[k];
+    s = block_sum(s, sh);
+    if (threadIdx.x == 0) *sval = s / n;
+    __syncthreads();
+    mean = float(*sval);
+  }
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    float acc = 0.0f;
+    for (int j = 0; j < n; ++j) acc = fmaf(M[i * n + j], f[j] - mean, acc);
+    u[i] = acc;
+  }
+  __syncthreads();
+  if (singular) {
+    double s = 0.0;
+    for (int k = threadIdx.x; k < n; k += blockDim.x) s += u[k];
+    s = block_sum(s, sh);
+    if (threadIdx.x == 0) *sval = s / n;
+    __syncthreads();
+    const float m = float(*sval);
+    for (int k = threadIdx.x; k < n; k += blockDim.x) u[k] -= m;
+    __syncthreads();
+  }
 }
 
 // CG on (-A) u = -f (shared memory); the doubly periodic system is solved in
@@ -413,43 +514,44 @@ __global__ void __launch_bounds__(kSmallThreads) k_small_vcycle(SmallLevels S, c
   const LevelDesc& d0 = S.d[0];
   const int n0 = d0.mx * d0.my;
   for (int k = threadIdx.x; k < n0; k += blockDim.x) sm[S.off[0] + n0 + k] = f_in[k];
+  if (S.cinv) {
+    const LevelDesc& c = S.d[S.count - 1];
+    const int nn = c.mx * c.my * c.mx * c.my;
+    for (int k = threadIdx.x; k < nn; k += blockDim.x) sm[S.cg_off + k] = __ldg(S.cinv + k);
+  }
   __syncthreads();
   const int last = S.count - 1;
   for (int l = 0; l < last; ++l) {
-    const LevelDesc& d = S.d[l];
+    const LevelDesc d = S.d[l];
+    const LevelDesc c = S.d[l + 1];
     const int n = d.mx * d.my;
     float* u = sm + S.off[l];
-    float* f = u + n;
-    for (int k = threadIdx.x; k < n; k += blockDim.x) u[k] = 0.0f;
-    __syncthreads();
+    sb_zero(u, d);
     for (int it = 0; it < nu_pre; ++it) {
-      sm_smooth(u, f, d, 0);
-      sm_smooth(u, f, d, 1);
+      sb_smooth(u, u + n, d, 0);
+      sb_smooth(u, u + n, d, 1);
     }
-    const LevelDesc& c = S.d[l + 1];
-    float* fc = sm + S.off[l + 1] + c.mx * c.my;
-    for (int k = threadIdx.x; k < c.mx * c.my; k += blockDim.x) fc[k] = restrict_at(u, f, d, k % c.mx, k / c.mx);
-    __syncthreads();
+    sb_restrict(u, u + n, u + 2 * n, d, sm + S.off[l + 1] + c.mx * c.my, c);
   }
   {
-    const LevelDesc& d = S.d[last];
-    const int n = d.mx * d.my;
+    const LevelDesc d = S.d[last];
     float* u = sm + S.off[last];
-    sm_coarse_cg(u, u + n, d, sm + S.cg_off, sh, &sval);
-    __syncthreads();
+    if (S.cinv) {
+      sm_dense_solve(u, u + d.mx * d.my, d, sm + S.cg_off, sh, &sval);
+    } else {
+      sm_coarse_cg(u, u + d.mx * d.my, d, sm + S.cg_off, sh, &sval);
+      __syncthreads();
+    }
   }
   for (int l = last - 1; l >= 0; --l) {
-    const LevelDesc& d = S.d[l];
-    const LevelDesc& c = S.d[l + 1];
+    const LevelDesc d = S.d[l];
+    const LevelDesc c = S.d[l + 1];
     const int n = d.mx * d.my;
     float* u = sm + S.off[l];
-    float* f = u + n;
-    const float* uc = sm + S.off[l + 1];
-    for (int k = threadIdx.x; k < n; k += blockDim.x) u[k] += prolong_at(uc, c, d, k % d.mx, k / d.mx);
-    __syncthreads();
+    sb_prolong_add(u, d, sm + S.off[l + 1], c);
     for (int it = 0; it < nu_post; ++it) {
-      sm_smooth(u, f, d, 1);
-      sm_smooth(u, f, d, 0);
+      sb_smooth(u, u + n, d, 1);
+      sb_smooth(u, u + n, d, 0);
     }
   }
   for (int k = threadIdx.x; k < n0; k += blockDim.x) {
@@ -516,7 +618,8 @@ PoissonMG::PoissonMG(const kern::PoissonLayout& L, int nu_pre, int nu_post)
   size_t floats = 0;
   for (int l = ls_; l < int(lv_.size()); ++l) floats += 3 * size_t(lv_[l].mx) * lv_[l].my;
   const Level& c = lv_.back();
-  floats += 3 * size_t(c.mx) * c.my;
+  const size_t ncoarse = size_t(c.mx) * c.my;
+  floats += ncoarse <= size_t(kDenseMax) ? std::max(3 * ncoarse, ncoarse * ncoarse) : 3 * ncoarse;  // inverse or CG
   small_smem_ = floats * sizeof(float);
   int dev = 0, maxsm = 0;
   GP_CUDA(cudaGetDevice(&dev));
@@ -525,6 +628,54 @@ PoissonMG::PoissonMG(const kern::PoissonLayout& L, int nu_pre, int nu_post)
     throw std::invalid_argument("coarsest multigrid level too large (grid dimensions do not coarsen)");
   GP_CUDA(cudaFuncSetAttribute(k_small_vcycle, cudaFuncAttributeMaxDynamicSharedMemorySize, int(small_smem_)));
   x2_.resize(size_t(n_), true);
+  // Dense inverse of the coarsest operator (FP64 Gauss-Jordan, stored FP32);
+  // the doubly periodic operator is regularised as A + a 11^T, a = |cd| / n.
+  const int nc = c.mx * c.my;
+  if (nc <= kDenseMax) {
+    std::vector<double> A(size_t(nc) * nc, 0.0), I(size_t(nc) * nc, 0.0);
+    auto wrapi = [](int i, int n, bool per) { return per ? ((i % n) + n) % n : i; };
+    for (int j = 0; j < c.my; ++j)
+      for (int i = 0; i < c.mx; ++i) {
+        const int k = i + j * c.mx;
+        A[size_t(k) * nc + k] += c.cd;
+        const int di[4] = {-1, 1, 0, 0}, dj[4] = {0, 0, -1, 1};
+        for (int q = 0; q < 4; ++q) {
+          const int ii = wrapi(i + di[q], c.mx, c.perx), jj = wrapi(j + dj[q], c.my, c.pery);
+          if (ii < 0 || ii >= c.mx || jj < 0 || jj >= c.my) continue;
+          A[size_t(k) * nc + ii + jj * c.mx] += q < 2 ? c.cx : c.cy;
+        }
+      }
+    if (c.perx && c.pery)
+      for (auto& a : A) a += std::fabs(double(c.cd)) / nc;
+    for (int k = 0; k < nc; ++k) I[size_t(k) * nc + k] = 1.0;
+    for (int col = 0; col < nc; ++col) {
+      int piv = col;
+      for (int r = col + 1; r < nc; ++r)
+        if (std::fabs(A[size_t(r) * nc + col]) > std::fabs(A[size_t(piv) * nc + col])) piv = r;
+      if (std::fabs(A[size_t(piv) * nc + col]) < 1e-300) throw std::runtime_error("singular coarsest multigrid level");
+      for (int q = 0; q < nc; ++q) {
+        std::swap(A[size_t(col) * nc + q], A[size_t(piv) * nc + q]);
+        std::swap(I[size_t(col) * nc + q], I[size_t(piv) * nc + q]);
+      }
+      const double inv = 1.0 / A[size_t(col) * nc + col];
+      for (int q = 0; q < nc; ++q) {
+        A[size_t(col) * nc + q] *= inv;
+        I[size_t(col) * nc + q] *= inv;
+      }
+      for (int r = 0; r < nc; ++r) {
+        if (r == col) continue;
+        const double fct = A[size_t(r) * nc + col];
+        if (fct == 0.0) continue;
+        for (int q = 0; q < nc; ++q) {
+          A[size_t(r) * nc + q] -= fct * A[size_t(col) * nc + q];
+          I[size_t(r) * nc + q] -= fct * I[size_t(col) * nc + q];
+        }
+      }
+    }
+    std::vector<float> M(I.begin(), I.end());
+    coarse_inv_.resize(M.size());
+    GP_CUDA(cudaMemcpy(coarse_inv_.get(), M.data(), M.size() * sizeof(float), cudaMemcpyHostToDevice));
+  }
 }
 
 void PoissonMG::vcycle(cudaStream_t s) {
@@ -563,6 +714,7 @@ void PoissonMG::vcycle(cudaStream_t s) {
       off += 3 * size_t(lv_[l].mx) * lv_[l].my;
     }
     S.cg_off = int(off);
+    S.cinv = coarse_inv_.size() ? coarse_inv_.get() : nullptr;
     k_small_vcycle<<<1, kSmallThreads, small_smem_, s>>>(S, lv_[ls_].f.get(), lv_[ls_].u.get(), nullptr, nu_pre_,
                                                         nu_post_, st);
     GP_LAUNCH_CHECK();

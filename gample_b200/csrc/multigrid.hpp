@@ -17,7 +17,8 @@
 //     red-black sweeps in a shared-memory tile with a 4-point halo), one
 //     residual + restriction launch, one prolongation + post-smoothing launch;
 //   all small levels: one single-CTA kernel running the rest of the V-cycle
-//     in shared memory (coarsest level by CG).
+//     in shared memory; the coarsest level is solved by a precomputed dense
+//     inverse (by CG when it has more than 64 points).
 // The FP64 update + residual and the convergence test run on the device;
 // the host synchronises once per solve (it batches as many V-cycles as the
 // previous solve needed and re-checks).
@@ -68,6 +69,7 @@ class PoissonMG {
   int last_iters_ = 2;
   std::vector<Level> lv_;
   DeviceArray<double> x2_;      // ping-pong buffer of the FP64 update
+  DeviceArray<float> coarse_inv_;  // dense inverse of the coarsest operator (small coarsest levels)
   DeviceArray<double> state_;   // [0] sum r [1] sum r^2 [2] ||b|| [3] rel res [4] done [5] iterations [6] mean r
   PinnedArray<double> host_;
 };

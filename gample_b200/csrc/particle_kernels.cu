@@ -318,7 +318,7 @@ __host__ __device__ constexpr size_t smem_bytes() {
 }
 
 template <int ORDER, bool PUSH, bool DEP, bool DET, bool CUR, bool BZU>
-__global__ void __launch_bounds__(kThreads, ORDER == 5 ? 2 : 3) k_pic(GridDims g, ParticleArrays p, FieldPtrs f, PushConsts c,
+__global__ void __launch_bounds__(kThreads, ORDER == 5 ? 2 : 4) k_pic(GridDims g, ParticleArrays p, FieldPtrs f, PushConsts c,
                                                   int boris_order, DepositTargets d, SpeciesCounters* cnt,
                                                   uint32_t* dead_bits, int injected_only) {
   using DL = DepositLayout<ORDER, CUR>;
