@@ -84,6 +84,12 @@ EXPORTS = {
     "gp_collision_artificial_ionization": (C.c_int, [C.c_void_p, C.c_double, C.POINTER(C.c_int)]),
     "gp_collision_hollow_cathode": (C.c_int, [C.c_void_p, C.c_double, C.POINTER(C.c_int)]),
     "gp_collision_flux_reinjection": (C.c_int, [C.c_void_p, C.c_double, C.POINTER(C.c_int)]),
+    "gp_moments_integrate": (C.c_int, [C.c_void_p, C.c_int]),
+    "gp_moments_download": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_size_t]),
+    "gp_sim_output_field": (C.c_int, [C.c_void_p, C.c_int]),
+    "gp_sim_output_moments": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
+    "gp_sim_save_progress": (C.c_int, [C.c_void_p, C.c_int]),
+    "gp_sim_load_progress": (C.c_int, [C.c_void_p, C.c_int]),
     "gp_deposit_charge_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_uint32, C.c_float,
                                             C.c_void_p, C.c_void_p]),
     "gp_last_error": (C.c_char_p, []),
@@ -256,6 +262,18 @@ class Sim:
     def set_particles(self, s, arr):
         a = np.ascontiguousarray(arr, PARTICLE_DTYPE)
         check(lib().gp_particle_upload(self.h, s, a.ctypes.data, len(a)))
+
+    MOMENTS = ("n", "ux", "uy", "uz", "Pxx", "Pxy", "Pxz", "Pyy", "Pyz", "Pzz")
+
+    def moments(self, s):
+        """Velocity moments of species s as a dict of (ny+1, nx+1) arrays."""
+        check(lib().gp_moments_integrate(self.h, s))
+        out = {}
+        for i, name in enumerate(self.MOMENTS):
+            a = np.empty(self.shape("rho"), np.float32)
+            check(lib().gp_moments_download(self.h, i, a.ctypes.data, a.nbytes))
+            out[name] = a
+        return out
 
     def particles_raw(self, s):
         n = self.count(s)

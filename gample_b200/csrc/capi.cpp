@@ -4,6 +4,7 @@
 #include <string>
 
 #include "../../include/gample_gpu.h"
+#include "fileio.hpp"
 #include "simulation.hpp"
 
 #include <atomic>
@@ -386,6 +387,63 @@ gp_status gp_particle_download_raw(gp_sim* sim, int s, int32_t* cell, float* ox,
     cp(vy, a.vy, 4);
     cp(vz, a.vz, 4);
     GP_CUDA(cudaStreamSynchronize(p->stream));
+    return GP_OK;
+  });
+}
+
+gp_status gp_moments_integrate(gp_sim* sim, int s) {
+  return guarded([&] {
+    auto* p = species(sim, s);
+    auto& S_ = S(sim);
+    S_.moment->integrateMoments(*p, *S_.field);
+    GP_CUDA(cudaStreamSynchronize(S_.stream));
+    return GP_OK;
+  });
+}
+
+gp_status gp_moments_download(gp_sim* sim, int which, float* host, size_t bytes) {
+  return guarded([&] {
+    auto& S_ = S(sim);
+    if (which < 0 || which >= gample::Moment::kCount) throw std::invalid_argument("moment index out of range");
+    const size_t n = S_.moment->n_rho();
+    if (!host || bytes < n * sizeof(float)) throw std::invalid_argument("host buffer too small");
+    GP_CUDA(cudaMemcpyAsync(host, S_.moment->out.get() + size_t(which) * n, n * sizeof(float), cudaMemcpyDeviceToHost,
+                            S_.stream));
+    GP_CUDA(cudaStreamSynchronize(S_.stream));
+    return GP_OK;
+  });
+}
+
+gp_status gp_sim_output_field(gp_sim* sim, int cycle) {
+  return guarded([&] {
+    auto& S_ = S(sim);
+    gample::outputField(cycle, *S_.field, S_.init, S_.logger.get());
+    return GP_OK;
+  });
+}
+
+gp_status gp_sim_output_moments(gp_sim* sim, int s, int cycle) {
+  return guarded([&] {
+    auto* p = species(sim, s);
+    auto& S_ = S(sim);
+    S_.moment->integrateMoments(*p, *S_.field);
+    gample::outputMoments(cycle, *S_.moment, p->pName, S_.init, S_.logger.get());
+    return GP_OK;
+  });
+}
+
+gp_status gp_sim_save_progress(gp_sim* sim, int cycle) {
+  return guarded([&] {
+    auto& S_ = S(sim);
+    if (!gample::saveProgress(cycle, S_.ptrs, S_.init)) throw std::runtime_error("output progress failed");
+    return GP_OK;
+  });
+}
+
+gp_status gp_sim_load_progress(gp_sim* sim, int cycle) {
+  return guarded([&] {
+    auto& S_ = S(sim);
+    if (!gample::loadProgress(cycle, S_.ptrs, S_.init)) throw std::runtime_error("restart failed");
     return GP_OK;
   });
 }

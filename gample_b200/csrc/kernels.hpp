@@ -186,6 +186,12 @@ void gradient_energy(const double* phi, GridDims g, float dx, float dy, float* E
 // Probe values for the timeseries CSV (src/EMField.mm:1130-1134).
 void probe(const double* phi, const float* Ex, const float* Ey, GridDims g, double* out3, cudaStream_t s);
 
+// Velocity moments of particles [0, counters->n) (src/Moment.mm:33-135,
+// 287-316): out holds 10 arrays of (nx+1)(ny+1) floats (n, ux, uy, uz, Pxx,
+// Pxy, Pxz, Pyy, Pyz, Pzz); acc is FP64 scratch of the same size.
+void moments(int order, GridDims g, ParticleArrays p, const SpeciesCounters* counters, uint32_t n_bound, float scale,
+             float mass, double* acc, float* out, cudaStream_t s);
+
 // Charge density of one species from the reference's 24-byte records in
 // device memory into rho ((nx+1)(ny+1) floats), with no allocation: the int64
 // accumulator is a file-scope device array of noalloc_max_nodes() entries.

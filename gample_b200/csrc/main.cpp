@@ -41,10 +41,6 @@ int main(int argc, char** argv) {
     const auto& T = init.paramForTimeIntegration;
     const bool fused = !(args.count("--reference-order") && args["--reference-order"] == "1");
     gample::Simulation sim(init, T.ProjectName + "_" + tag, fused);
-    if (T.Start != 0) {
-      std::cerr << "restart (Start != 0) is not supported by this driver\n";
-      return 1;
-    }
     sim.initialize();
     for (int c = T.Start + 1; c <= T.End; ++c) {
       sim.cycle();

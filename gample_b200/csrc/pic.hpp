@@ -90,6 +90,7 @@ class EMField {
   double tol = 1e-7;
 
   DeviceArray<float> rho, jx, jy, Ex, Ey, Ez, Bx, By, Bz;
+  DeviceArray<float> delEx, delEy, delBz;  // Darwin corrections (zero in the electrostatic model)
   DeviceArray<double> phi, sol, b, diag;  // diag: [0..1] rhs sums [2..3] E sums [4] cathode mean [5..7] probe
   // per-species deposit accumulators: int64 fixed point (deterministic mode)
   // or FP64 (fast mode); combined into rho/jx/jy by finalizeCharge()
@@ -164,6 +165,25 @@ class Particle {
   PinnedArray<kern::SpeciesCounters> host_cnt_;
   double dx_ = 0, dy_ = 0;
   kern::GridDims dims_{};
+};
+
+// src/Moment.{h,mm}: velocity moments of one species on the rho nodes.
+class Moment {
+ public:
+  static constexpr int kCount = 10;  // n, ux, uy, uz, Pxx, Pxy, Pxz, Pyy, Pyz, Pzz
+  Moment(const Init& init, cudaStream_t s);
+  // src/Moment.mm:206-316; the result stays in `out` (device)
+  void integrateMoments(Particle& p, const EMField& fld);
+  size_t n_rho() const { return n_rho_; }
+  DeviceArray<float> out;     // kCount x (nx+1)(ny+1)
+  DeviceArray<double> acc;    // FP64 sums, same shape
+  int species = -1;           // species of the last integration
+  cudaStream_t stream;
+
+ private:
+  kern::GridDims dims_{};
+  int order_ = 1;
+  size_t n_rho_ = 0;
 };
 
 class Collision {

@@ -77,6 +77,9 @@ EMField::EMField(const Init& init, cudaStream_t s, int nspecies) : stream(s), ho
   Bx.resize(n_ey(), true);
   By.resize(n_ex(), true);
   Bz.resize(n_bz(), true);
+  delEx.resize(n_ex(), true);
+  delEy.resize(n_ey(), true);
+  delBz.resize(n_bz(), true);
   phi.resize(n_phi(), true);
   diag.resize(8, true);
 

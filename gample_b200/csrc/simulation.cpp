@@ -1,7 +1,11 @@
 // simulation.cpp -- time loop of the reference's main() (src/main.mm).
 #include "simulation.hpp"
 
+#include <sys/stat.h>
+
 #include <stdexcept>
+
+#include "fileio.hpp"
 
 namespace gample {
 
@@ -16,9 +20,12 @@ Simulation::Simulation(const Init& in, const std::string& log_name, bool fused_s
     ptrs.push_back(particles.back().get());
   }
   field = std::make_unique<EMField>(init, stream, ns);               // src/main.mm:108-113
+  moment = std::make_unique<Moment>(init, stream);                   // src/main.mm:114-115
   collision = std::make_unique<Collision>(init, ptrs, stream);        // src/main.mm:117-122
   last_flow.resize(ns);
   cycle_no = init.paramForTimeIntegration.Start;
+  struct stat st {};
+  file_output = logger && stat("bin", &st) == 0 && S_ISDIR(st.st_mode);
   time = cycle_no * init.paramForTimeIntegration.TimeStep;
 }
 
@@ -63,12 +70,21 @@ void Simulation::phase_times(double out[PH_COUNT]) {
 }
 
 void Simulation::initialize() {
-  // src/main.mm:114-141: the logger is still switched off here.
+  // src/main.mm:124-147: the logger is still switched off here.
+  const int start = init.paramForTimeIntegration.Start;
+  if (start != 0 && !loadProgress(start, ptrs, init)) throw std::runtime_error("[Fatal] restart failed.");
   for (auto* p : ptrs)
-    if (p->needs_sort) p->sort();  // tile order for the freshly loaded particles
+    if (p->needs_sort) p->sort();  // cell order for the freshly loaded particles
   field->resetChargeDensity();
   for (auto* p : ptrs) p->integrateChargeDensity(*field);
   last_solve = field->solvePoisson(0.0, logger.get());
+  if (file_output) {  // initial field and moments (src/main.mm:142-147)
+    outputField(start, *field, init, logger.get());
+    for (auto* p : ptrs) {
+      moment->integrateMoments(*p, *field);
+      outputMoments(start, *moment, p->pName, init, logger.get());
+    }
+  }
   if (fused) {
     // The first cycle's charge: same particle positions, fresh accumulators.
     field->resetChargeDensity();
@@ -100,6 +116,8 @@ void Simulation::cycle() {
     last_solve = field->solvePoisson(dt, logger.get());
     mark(PH_SOLVE, false);
   }
+  const bool field_out = file_output && T.FieldOutput != 0 && cycle_no % T.FieldOutput == 0;
+  if (field_out) outputField(cycle_no, *field, init, logger.get());  // src/main.mm:193-195
   if (fused) field->resetChargeDensity();
   for (size_t s = 0; s < ptrs.size(); ++s) {
     if (ptrs[s]->needs_sort) {
@@ -113,6 +131,12 @@ void Simulation::cycle() {
     mark(PH_REDUCE, true);
     last_flow[s] = ptrs[s]->reduce(logger.get());
     mark(PH_REDUCE, false);
+    if (file_output && T.ParticleOutput != 0 && cycle_no % T.ParticleOutput == 0)  // :211-214
+      outputPhaseSpace(cycle_no, *ptrs[s], init);
+    if (field_out) {  // :215-220
+      moment->integrateMoments(*ptrs[s], *field);
+      outputMoments(cycle_no, *moment, ptrs[s]->pName, init, logger.get());
+    }
   }
   mark(PH_SOURCE, true);
   last_ai = collision->artificialIonization(dt, ptrs, logger.get());
@@ -121,6 +145,10 @@ void Simulation::cycle() {
   if (fused)
     for (auto* p : ptrs) p->integrateChargeDensity(*field, true);
   mark(PH_SOURCE, false);
+  // src/main.mm:237-243 (guarded by FieldOutput there; a zero ProgressOutput
+  // would divide by zero and is treated as "never")
+  if (file_output && T.FieldOutput != 0 && T.ProgressOutput != 0 && cycle_no % T.ProgressOutput == 0)
+    if (!saveProgress(cycle_no, ptrs, init)) throw std::runtime_error("output progress failed.");
   if (logger) logger->logCycleEnd();
 }
 

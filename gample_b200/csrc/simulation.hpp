@@ -32,6 +32,9 @@ class Simulation {
   void initialize();  // src/main.mm:114-147 (initial deposit and solve)
   void cycle();       // one cycle of src/main.mm:155-253
   void run(int ncycles);
+  // Binary outputs under bin/ (src/FileIO.mm) are written only when a log
+  // name was given and the bin/ directory exists.
+  bool file_output = false;
 
   Init init;
   cudaStream_t stream = nullptr;
@@ -40,6 +43,7 @@ class Simulation {
   std::vector<Particle*> ptrs;
   std::unique_ptr<EMField> field;
   std::unique_ptr<Collision> collision;
+  std::unique_ptr<Moment> moment;
   bool fused = true;
   int cycle_no = 0;
   double time = 0, comp = 0;

@@ -133,6 +133,26 @@ gp_status gp_particle_upload(gp_sim* sim, int s, const gp_particle_state* host, 
 gp_status gp_particle_download_raw(gp_sim* sim, int s, int32_t* cell, float* ox, float* oy, float* vx, float* vy,
                                    float* vz, uint32_t capacity, uint32_t* n);
 
+/* ---- Moment ---- */
+/* -[Moment integrateMoments:withEMField:withLogger:] (src/Moment.mm:206-316)
+ * for species s; the ten arrays stay on the device. */
+gp_status gp_moments_integrate(gp_sim* sim, int s);
+/* One of the ten moment arrays of the last integration, (nx+1)(ny+1) floats:
+ * 0 n, 1 ux, 2 uy, 3 uz, 4 Pxx, 5 Pxy, 6 Pxz, 7 Pyy, 8 Pyz, 9 Pzz
+ * (src/Moment.h:43-53; CGS units, before the 0.1 Pa scaling of the files). */
+gp_status gp_moments_download(gp_sim* sim, int which, float* host, size_t bytes);
+
+/* ---- binary outputs and restart (src/FileIO.mm), under ./bin ---- */
+/* outputField (src/FileIO.mm:41-136): bin/<Project>_EMField_%08d.bin */
+gp_status gp_sim_output_field(gp_sim* sim, int cycle);
+/* integrateMoments + outputMoments (src/FileIO.mm:138-226) of species s */
+gp_status gp_sim_output_moments(gp_sim* sim, int s, int cycle);
+/* saveProgress (src/FileIO.mm:250-293): bin/<Project>_ProgressData_<name>_%08d.bin */
+gp_status gp_sim_save_progress(gp_sim* sim, int cycle);
+/* loadProgress (src/FileIO.mm:295-352): reads bin/<RestartName>_ProgressData_...,
+ * shifting positions by PtclPosOffset */
+gp_status gp_sim_load_progress(gp_sim* sim, int cycle);
+
 /* ---- Collision ---- */
 /* -[Collision artificialIonization:withParticles:withLogger:] (src/Collision.mm:464-566) */
 gp_status gp_collision_artificial_ionization(gp_sim* sim, double dt, int* addn);

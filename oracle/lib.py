@@ -92,6 +92,7 @@ def lib():
             "or_sim_poisson_size": (i, [vp]),
             "or_sim_poisson_residual": (d, [vp, dp]),
             "or_sim_get_poisson_solution": (None, [vp, dp]),
+            "or_sim_moments": (None, [vp, i, i, C.c_void_p]),
             "or_det_deposit_rho": (None, [i, i, i, i, i, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                           C.c_void_p]),
             "or_det_deposit_j": (None, [i, i, i, i, i] + [C.c_void_p] * 8),
@@ -245,6 +246,16 @@ class OracleSim:
         out = np.empty(self.poisson_size(), np.float64)
         lib().or_sim_get_poisson_solution(self.h, _p(out, C.c_double))
         return out
+
+    MOMENTS = ("n", "ux", "uy", "uz", "Pxx", "Pxy", "Pxz", "Pyy", "Pyz", "Pzz")
+
+    def moments(self, sp, build=True):
+        """Velocity moments of species sp (src/Moment.mm) as (ny+1, nx+1) arrays;
+        build=True uses the GPU build's weights and FP64 sums."""
+        shape = self.shape("rho")
+        out = np.empty((10,) + shape, np.float32)
+        lib().or_sim_moments(self.h, sp, 1 if build else 0, out.ctypes.data)
+        return dict(zip(self.MOMENTS, out))
 
 
 def det_deposit_rho(order, ngx, ngy, ngb, ix, iy, ox, oy):

@@ -105,6 +105,9 @@ int or_sim_poisson_size(void* h);
  * system built from the sim's current rho. */
 double or_sim_poisson_residual(void* h, const double* sol);
 void or_sim_get_poisson_solution(void* h, double* sol);
+/* velocity moments of species sp, 10 x n_rho floats (src/Moment.mm); build != 0:
+   Horner weights and FP64 sums (the GPU build's summation) */
+void or_sim_moments(void* h, int sp, int build, float* out);
 
 /* Deterministic-mode deposit of the build restated on the CPU: positions as
  * integer cell (ix, iy) plus float offsets, weights by the build's Horner

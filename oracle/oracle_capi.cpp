@@ -589,6 +589,18 @@ void or_sim_get_poisson_solution(void* h, double* sol) {
   });
 }
 
+// Moments of species sp (src/Moment.mm): out = 10 arrays of n_rho floats.
+void or_sim_moments(void* h, int sp, int build, float* out) {
+  dispatch(h, [&](auto& s) {
+    std::vector<float> m[10];
+    const float scale = s.wf[sp] / (s.dxf * s.dyf);
+    moments(s.P[sp], s.g, s.cfg.weight_order, scale, s.mf[sp], m, build != 0);
+    const size_t ng = s.g.n_rho();
+    for (int a = 0; a < 10; ++a) std::copy(m[a].begin(), m[a].end(), out + a * ng);
+    return 0;
+  });
+}
+
 static inline int64_t quant40(float w) {
   // w * 2^40 is exact in float (power-of-two scale); round half to even.
   return std::llrint(double(w * 1099511627776.0f));

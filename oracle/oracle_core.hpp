@@ -1053,17 +1053,28 @@ inline void generate_one(uint32_t id, int genType, const GenParams& prm, RNGStat
 // Velocity moments of one species: src/Moment.mm:55-129 (kernel) and
 // :287-316 (normalisation). Outputs 10 arrays of (nx+1)(ny+1):
 // n, ux, uy, uz, Pxx, Pxy, Pxz, Pyy, Pyz, Pzz.
+// build = true: Horner-form weights (shape_build) and FP64 sums, the
+// summation the GPU build performs (for parity checks); false: the
+// reference's pow-form weights and FP32 sums.
 template <typename R>
-void moments(const Particles<R>& P, const Grid& g, int order, float scale, float m, std::vector<float>* out) {
+void moments(const Particles<R>& P, const Grid& g, int order, float scale, float m, std::vector<float>* out,
+             bool build = false) {
   const int nx = g.nx();
   const size_t ng = g.n_rho();
   for (int a = 0; a < 10; ++a) out[a].assign(ng, 0.0f);
+  std::vector<double> sum(build ? 10 * ng : 0, 0.0);
   for (size_t k = 0; k < P.n; ++k) {
+    if (P.piflag[k] != 0) continue;
     float px = float(P.x[k]), py = float(P.y[k]);
     int i1 = int(px + 1e-20f), j1 = int(py + 1e-20f);
     float sx[6], sy[6];
-    shape_ref<float>(order, px - float(i1), sx);
-    shape_ref<float>(order, py - float(j1), sy);
+    if (build) {
+      shape_build(order, px - float(i1), sx);
+      shape_build(order, py - float(j1), sy);
+    } else {
+      shape_ref<float>(order, px - float(i1), sx);
+      shape_ref<float>(order, py - float(j1), sy);
+    }
     float vx = float(P.vx[k]), vy = float(P.vy[k]), vz = float(P.vz[k]);
     for (int i = 0; i < order + 1; i++)
       for (int j = 0; j < order + 1; j++) {
@@ -1071,18 +1082,17 @@ void moments(const Particles<R>& P, const Grid& g, int order, float scale, float
         if (ii < 0 || jj < 0 || ii > nx || jj > g.ny()) continue;
         int idx = ii + jj * (nx + 1);
         float s = sx[i] * sy[j];
-        out[0][idx] += s * scale;
-        out[1][idx] += s * vx;
-        out[2][idx] += s * vy;
-        out[3][idx] += s * vz;
-        out[4][idx] += s * vx * vx;
-        out[5][idx] += s * vx * vy;
-        out[6][idx] += s * vx * vz;
-        out[7][idx] += s * vy * vy;
-        out[8][idx] += s * vy * vz;
-        out[9][idx] += s * vz * vz;
+        const float v[10] = {s * scale,   s * vx,      s * vy,      s * vz,      s * vx * vx,
+                             s * vx * vy, s * vx * vz, s * vy * vy, s * vy * vz, s * vz * vz};
+        if (build)
+          for (int a = 0; a < 10; ++a) sum[a * ng + idx] += double(v[a]);
+        else
+          for (int a = 0; a < 10; ++a) out[a][idx] += v[a];
       }
   }
+  if (build)
+    for (int a = 0; a < 10; ++a)
+      for (size_t i = 0; i < ng; ++i) out[a][i] = float(sum[a * ng + i]);
   for (size_t i = 0; i < ng; i++) {
     float n = out[0][i];
     if (n > 1e-20f) {

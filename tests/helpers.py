@@ -94,3 +94,26 @@ def rel_inf(a, b, scale=None):
     b = np.asarray(b, np.float64)
     s = np.max(np.abs(b)) if scale is None else scale
     return float(np.max(np.abs(a - b)) / s) if s > 0 else float(np.max(np.abs(a - b)))
+
+
+def read_field_file(path):
+    """Records of a field/moment file (src/FileIO.mm:109-136, 228-248):
+    header ngx, ngy, ngb (int32), dx, dy (float32), then per record a 32-byte
+    name, an int32 type id and a float32 array whose shape follows the type
+    (0 node, 1 x-shifted, 2 y-shifted, 3 both, 4 potential)."""
+    with open(path, "rb") as f:
+        buf = f.read()
+    ngx, ngy, ngb = np.frombuffer(buf[:12], np.int32)
+    dx, dy = np.frombuffer(buf[12:20], np.float32)
+    off = 20
+    records = {}
+    while off < len(buf):
+        name = buf[off:off + 32].split(b"\0", 1)[0].decode()
+        tid = int(np.frombuffer(buf[off + 32:off + 36], np.int32)[0])
+        nx, ny = ngx + 2 * ngb, ngy + 2 * ngb
+        ex = {0: (0, 0), 1: (1, 0), 2: (0, 1), 3: (1, 1), 4: (2, 2)}[tid]
+        shape = (ny + 1 + ex[1], nx + 1 + ex[0])
+        n = shape[0] * shape[1]
+        records[name] = (tid, np.frombuffer(buf[off + 36:off + 36 + 4 * n], np.float32).reshape(shape))
+        off += 36 + 4 * n
+    return {"ngx": int(ngx), "ngy": int(ngy), "ngb": int(ngb), "dx": float(dx), "dy": float(dy)}, records
