@@ -17,7 +17,8 @@ LIB_PATH = os.path.join(HERE, "libgample_b200.so")
 
 GP_OK = 0
 GP_ERR = {1: "argument", 2: "config", 3: "cuda", 4: "capacity", 5: "internal"}
-FIELDS = {"rho": 0, "Ex": 1, "Ey": 2, "Bz": 3, "jx": 4, "jy": 5, "phi": 6, "sol": 7}
+FIELDS = {"rho": 0, "Ex": 1, "Ey": 2, "Bz": 3, "jx": 4, "jy": 5, "phi": 6, "sol": 7, "delEx": 8, "delEy": 9,
+          "delBz": 10, "psi": 11, "Ax": 12, "Ay": 13}
 PHASES = ("deposit", "solve", "push", "reduce", "sources", "sort")
 
 
@@ -70,6 +71,7 @@ EXPORTS = {
     "gp_field_dims": (C.c_int, [C.c_void_p] + [C.POINTER(C.c_int)] * 5),
     "gp_field_reset_charge": (C.c_int, [C.c_void_p]),
     "gp_field_solve_poisson": (C.c_int, [C.c_void_p, C.c_double, C.POINTER(GpSolveStats)]),
+    "gp_field_solve_darwin": (C.c_int, [C.c_void_p, C.c_double, C.c_void_p, C.c_void_p]),
     "gp_field_download": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_size_t]),
     "gp_field_upload": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_size_t]),
     "gp_field_set_solver": (C.c_int, [C.c_void_p, C.c_double, C.c_int]),
@@ -211,16 +213,31 @@ class Sim:
         nx, ny = self.nx, self.ny
         return {"rho": (ny + 1, nx + 1), "Ex": (ny + 1, nx + 2), "Ey": (ny + 2, nx + 1), "Bz": (ny + 2, nx + 2),
                 "jx": (ny + 1, nx + 2), "jy": (ny + 2, nx + 1), "phi": (ny + 3, nx + 3),
-                "sol": (self.nky + 1, self.nkx + 1)}[which]
+                "sol": (self.nky + 1, self.nkx + 1), "delEx": (ny + 1, nx + 2), "delEy": (ny + 2, nx + 1),
+                "delBz": (ny + 2, nx + 2), "psi": self.darwin_shape(), "Ax": self.darwin_shape(),
+                "Ay": self.darwin_shape()}[which]
+
+    def darwin_shape(self):
+        """(nky_vec+1, nkx_vec+1): ngx (ngy) nodes plus one, minus one when periodic."""
+        types = {b["position"]: b["type"] for b in self.init.dump().get("fieldBCs", [])}
+        px = types.get("Xmin") == "periodic"
+        py = types.get("Ymin") == "periodic"
+        return (self.ngy - (1 if py else 0) + 1, self.ngx - (1 if px else 0) + 1)
+
+    def solve_darwin(self, dt):
+        it = (C.c_int * 3)()
+        er = (C.c_double * 3)()
+        check(lib().gp_field_solve_darwin(self.h, dt, it, er))
+        return list(it), list(er)
 
     def field(self, which):
-        dt = np.float64 if which in ("phi", "sol") else np.float32
+        dt = np.float64 if which in ("phi", "sol", "psi", "Ax", "Ay") else np.float32
         out = np.empty(self.shape(which), dt)
         check(lib().gp_field_download(self.h, FIELDS[which], out.ctypes.data, out.nbytes))
         return out
 
     def set_field(self, which, arr):
-        dt = np.float64 if which in ("phi", "sol") else np.float32
+        dt = np.float64 if which in ("phi", "sol", "psi", "Ax", "Ay") else np.float32
         a = np.ascontiguousarray(arr, dt).reshape(self.shape(which))
         check(lib().gp_field_upload(self.h, FIELDS[which], a.ctypes.data, a.nbytes))
 

@@ -102,6 +102,16 @@ FieldBuf field_buf(gample::EMField& f, int which) {
     case GP_FIELD_JY: return {f.jy.get(), f.jy.bytes()};
     case GP_FIELD_PHI: return {f.phi.get(), f.phi.bytes()};
     case GP_FIELD_SOL: return {f.sol.get(), f.sol.bytes()};
+    case GP_FIELD_DEL_EX: return {f.delEx.get(), f.delEx.bytes()};
+    case GP_FIELD_DEL_EY: return {f.delEy.get(), f.delEy.bytes()};
+    case GP_FIELD_DEL_BZ: return {f.delBz.get(), f.delBz.bytes()};
+    case GP_FIELD_PSI:
+    case GP_FIELD_AX:
+    case GP_FIELD_AY:
+      if (!f.darwin) throw std::invalid_argument("the Darwin solution needs FlagForEquation.EMField = 2");
+      if (which == GP_FIELD_PSI) return {f.psi.get(), f.psi.bytes()};
+      if (which == GP_FIELD_AX) return {f.Ax.get(), f.Ax.bytes()};
+      return {f.Ay.get(), f.Ay.bytes()};
     default: throw std::invalid_argument("unknown field selector");
   }
 }
@@ -283,6 +293,18 @@ gp_status gp_field_solve_poisson(gp_sim* sim, double dt, gp_solve_stats* out) {
     auto& s = S(sim);
     s.last_solve = s.field->solvePoisson(dt, s.logger.get());
     fill(out, s.last_solve);
+    return GP_OK;
+  });
+}
+gp_status gp_field_solve_darwin(gp_sim* sim, double dt, int iterations[3], double errors[3]) {
+  return guarded([&] {
+    auto& s = S(sim);
+    if (!s.field->darwin) throw std::invalid_argument("the Darwin solve needs FlagForEquation.EMField = 2");
+    const auto st = s.field->solveVectorPotential(dt, s.logger.get());
+    for (int q = 0; q < 3; ++q) {
+      if (iterations) iterations[q] = st.iters[q];
+      if (errors) errors[q] = st.errors[q];
+    }
     return GP_OK;
   });
 }

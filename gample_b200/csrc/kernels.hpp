@@ -186,6 +186,23 @@ void gradient_energy(const double* phi, GridDims g, float dx, float dy, float* E
 // Probe values for the timeseries CSV (src/EMField.mm:1130-1134).
 void probe(const double* phi, const float* Ex, const float* Ey, GridDims g, double* out3, cudaStream_t s);
 
+// ------------------------------------------------------------- Darwin
+// Vector-potential grid of the Darwin solves (src/EMField.mm:484-492).
+struct DarwinGeom {
+  int nkx, nky, ngb, nx, ny;
+  bool perx, pery;  // otherwise Neumann
+  float dx, dy;
+};
+// rhs = div J with the Neumann boundary terms (src/EMField.mm:1150-1184)
+void darwin_div_rhs(const float* jx, const float* jy, DarwinGeom G, double* rhs, cudaStream_t s);
+// rhs = -(4 pi / c)(J_a - d_a psi), dir 0: x, 1: y (src/EMField.mm:1201-1275)
+void darwin_a_rhs(const float* ja, const double* psi, DarwinGeom G, int dir, double* rhs, cudaStream_t s);
+// v -= weighted mean (weights 1/2 at Neumann ends); scratch2: 2 doubles
+void darwin_weighted_project(double* v, DarwinGeom G, double* scratch2, cudaStream_t s);
+// delEx, delEy, delBz from A and the previous A (src/EMField.mm:1277-1297)
+void darwin_fields(const double* Ax, const double* Ay, const double* lastAx, const double* lastAy, DarwinGeom G,
+                   double cdt, float* delEx, float* delEy, float* delBz, cudaStream_t s);
+
 // Velocity moments of particles [0, counters->n) (src/Moment.mm:33-135,
 // 287-316): out holds 10 arrays of (nx+1)(ny+1) floats (n, ux, uy, uz, Pxx,
 // Pxy, Pxz, Pyy, Pyz, Pzz); acc is FP64 scratch of the same size.

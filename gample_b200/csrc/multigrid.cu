@@ -21,21 +21,37 @@ constexpr int kSmallThreads = 1024;
 // state words (FP64): see multigrid.hpp
 enum { S_SUM = 0, S_SUM2, S_NORMB, S_REL, S_DONE, S_ITER, S_MEAN, S_COUNT };
 
+// Boundary treatment of a direction: Dirichlet (values outside are zero),
+// periodic (wrap) or Neumann (mirror about the end node, i.e. the doubled
+// off-diagonal of the Darwin operator, src/EMField.mm:527-560).
+enum { BC_DIR = 0, BC_PER = 1, BC_NEU = 2 };
+
 struct LevelDesc {
   int mx, my;
-  int perx, pery;
+  int bx, by;
   float cx, cy, cd;
 };
 
-__device__ __forceinline__ bool wrap(int& i, int n, int per) {
+__host__ __device__ __forceinline__ bool wrap(int& i, int n, int b) {
   if (i >= 0 && i < n) return true;
-  if (!per) return false;
-  i = ((i % n) + n) % n;
+  if (b == BC_DIR) return false;
+  if (b == BC_PER) {
+    i = ((i % n) + n) % n;
+  } else {
+    i = i < 0 ? -i : 2 * (n - 1) - i;
+    if (i < 0 || i >= n) i = i < 0 ? 0 : n - 1;
+  }
   return true;
 }
 
+// Weight of a node in the solvability condition of a singular level (the
+// left null vector of the operator): 1/2 at each Neumann end, 1 elsewhere.
+__host__ __device__ __forceinline__ float bc_weight(int i, int n, int b) {
+  return (b == BC_NEU && (i == 0 || i == n - 1)) ? 0.5f : 1.0f;
+}
+
 __device__ __forceinline__ float ld(const float* u, const LevelDesc& d, int i, int j) {
-  if (!wrap(i, d.mx, d.perx) || !wrap(j, d.my, d.pery)) return 0.0f;
+  if (!wrap(i, d.mx, d.bx) || !wrap(j, d.my, d.by)) return 0.0f;
   return u[i + j * d.mx];
 }
 
@@ -56,9 +72,9 @@ __device__ __forceinline__ double block_sum(double v, double* sh) {
 }
 
 // Bilinear interpolation weights of fine index i from a coarse level
-// (coarse I on fine 2I+1 for Dirichlet, 2I for periodic).
-__device__ __forceinline__ void interp1d(int i, int per, int mc, int& i0, float& w0, int& i1, float& w1) {
-  if (per) {
+// (coarse I on fine 2I+1 for Dirichlet, 2I for periodic and Neumann).
+__device__ __forceinline__ void interp1d(int i, int b, int mc, int& i0, float& w0, int& i1, float& w1) {
+  if (b != BC_DIR) {
     if ((i & 1) == 0) {
       i0 = i / 2;
       w0 = 1.0f;
@@ -89,16 +105,16 @@ __device__ __forceinline__ void interp1d(int i, int per, int mc, int& i0, float&
 __device__ __forceinline__ float prolong_at(const float* uc, const LevelDesc& c, const LevelDesc& f, int i, int j) {
   int a0, a1, b0, b1;
   float wa0, wa1, wb0, wb1;
-  interp1d(i, f.perx, c.mx, a0, wa0, a1, wa1);
-  interp1d(j, f.pery, c.my, b0, wb0, b1, wb1);
+  interp1d(i, f.bx, c.mx, a0, wa0, a1, wa1);
+  interp1d(j, f.by, c.my, b0, wb0, b1, wb1);
   return wb0 * (wa0 * uc[a0 + b0 * c.mx] + wa1 * uc[a1 + b0 * c.mx]) +
          wb1 * (wa0 * uc[a0 + b1 * c.mx] + wa1 * uc[a1 + b1 * c.mx]);
 }
 
 // Full-weighting restriction of the residual f - A u at coarse (I, J).
 __device__ __forceinline__ float restrict_at(const float* u, const float* f, const LevelDesc& d, int I, int J) {
-  const int fi = d.perx ? 2 * I : 2 * I + 1;
-  const int fj = d.pery ? 2 * J : 2 * J + 1;
+  const int fi = d.bx != BC_DIR ? 2 * I : 2 * I + 1;
+  const int fj = d.by != BC_DIR ? 2 * J : 2 * J + 1;
   float s = 0.0f;
 #pragma unroll
   for (int b = -1; b <= 1; ++b) {
@@ -107,7 +123,7 @@ __device__ __forceinline__ float restrict_at(const float* u, const float* f, con
     for (int a = -1; a <= 1; ++a) {
       const float wa = a == 0 ? 0.5f : 0.25f;
       int i = fi + a, j = fj + b;
-      if (!wrap(i, d.mx, d.perx) || !wrap(j, d.my, d.pery)) continue;
+      if (!wrap(i, d.mx, d.bx) || !wrap(j, d.my, d.by)) continue;
       const float au = d.cd * u[i + j * d.mx] + d.cx * (ld(u, d, i - 1, j) + ld(u, d, i + 1, j)) +
                        d.cy * (ld(u, d, i, j - 1) + ld(u, d, i, j + 1));
       s += wa * wb * (f[i + j * d.mx] - au);
@@ -143,26 +159,36 @@ __global__ void k_residual64(const double* __restrict__ x, const double* __restr
   double s1 = 0.0, s2 = 0.0;
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
     const int i = k % mx, j = k / mx;
+    const bool nx_ = L.fbc[0] == kern::FBC_NEUMANN_C, ny_ = L.fbc[2] == kern::FBC_NEUMANN_C;
     double ax = L.Cd * x[k];
     if (i > 0)
       ax += L.Cx * x[k - 1];
     else if (L.periodic_x)
       ax += L.Cx * x[k + L.nkx];
+    else if (nx_ && L.nkx > 0)
+      ax += L.Cx * x[k + 1];
     if (i < L.nkx)
       ax += L.Cx * x[k + 1];
     else if (L.periodic_x)
       ax += L.Cx * x[k - L.nkx];
+    else if (nx_ && L.nkx > 0)
+      ax += L.Cx * x[k - 1];
     if (j > 0)
       ax += L.Cy * x[k - mx];
     else if (L.periodic_y)
       ax += L.Cy * x[k + L.nky * mx];
+    else if (ny_ && L.nky > 0)
+      ax += L.Cy * x[k + mx];
     if (j < L.nky)
       ax += L.Cy * x[k + mx];
     else if (L.periodic_y)
       ax += L.Cy * x[k - L.nky * mx];
+    else if (ny_ && L.nky > 0)
+      ax += L.Cy * x[k - mx];
     const double r = b[k] - ax;
     r32[k] = float(r);
-    s1 += r;
+    const double w = double(bc_weight(i, mx, nx_ ? BC_NEU : BC_PER)) * bc_weight(j, my, ny_ ? BC_NEU : BC_PER);
+    s1 += w * r;
     s2 += r * r;
   }
   s1 = block_sum(s1, sh);
@@ -174,7 +200,7 @@ __global__ void k_residual64(const double* __restrict__ x, const double* __restr
 }
 
 // Convergence test (one thread): AMGCL's ||r|| / ||b|| <= tol or maxiter.
-__global__ void k_check(double* st, double tol, int maxiter, int n) {
+__global__ void k_check(double* st, double tol, int maxiter, double wsum) {
   if (st[S_DONE] != 0.0) return;
   const double rel = sqrt(st[S_SUM2] > 0 ? st[S_SUM2] : 0.0) / st[S_NORMB];
   st[S_REL] = rel;
@@ -182,7 +208,7 @@ __global__ void k_check(double* st, double tol, int maxiter, int n) {
     st[S_DONE] = 1.0;
   } else {
     st[S_ITER] += 1.0;
-    st[S_MEAN] = st[S_SUM] / double(n);
+    st[S_MEAN] = st[S_SUM] / wsum;
   }
   st[S_SUM] = 0.0;
   st[S_SUM2] = 0.0;
@@ -228,7 +254,7 @@ __global__ void __launch_bounds__(kSmoothThreads) k_smooth_tile(const float* u, 
   for (int e = threadIdx.x; e < SW * SH; e += kSmoothThreads) {
     const int li = e % SW, lj = e / SW;
     int gi = x0 + li, gj = y0 + lj;
-    const bool inside = wrap(gi, d.mx, d.perx) && wrap(gj, d.my, d.pery);
+    const bool inside = wrap(gi, d.mx, d.bx) && wrap(gj, d.my, d.by);
     float uv = 0.0f, fv = 0.0f;
     if (inside) {
       fv = f[gi + gj * d.mx];
@@ -323,10 +349,12 @@ constexpr int kRows = kSmallThreads / 32;
 
 __device__ __forceinline__ float nb_sum(const float* u, const LevelDesc& d, int i, int j) {
   const int k = i + j * d.mx;
-  const float l = i > 0 ? u[k - 1] : (d.perx ? u[k + d.mx - 1] : 0.0f);
-  const float r = i < d.mx - 1 ? u[k + 1] : (d.perx ? u[k - d.mx + 1] : 0.0f);
-  const float b = j > 0 ? u[k - d.mx] : (d.pery ? u[k + (d.my - 1) * d.mx] : 0.0f);
-  const float t = j < d.my - 1 ? u[k + d.mx] : (d.pery ? u[k - (d.my - 1) * d.mx] : 0.0f);
+  const int ox = d.mx > 1 ? 1 : 0, oy = d.my > 1 ? d.mx : 0;  // Neumann mirror neighbours
+  const float l = i > 0 ? u[k - 1] : (d.bx == BC_PER ? u[k + d.mx - 1] : d.bx == BC_NEU ? u[k + ox] : 0.0f);
+  const float r = i < d.mx - 1 ? u[k + 1] : (d.bx == BC_PER ? u[k - d.mx + 1] : d.bx == BC_NEU ? u[k - ox] : 0.0f);
+  const float b = j > 0 ? u[k - d.mx] : (d.by == BC_PER ? u[k + (d.my - 1) * d.mx] : d.by == BC_NEU ? u[k + oy] : 0.0f);
+  const float t = j < d.my - 1 ? u[k + d.mx]
+                               : (d.by == BC_PER ? u[k - (d.my - 1) * d.mx] : d.by == BC_NEU ? u[k - oy] : 0.0f);
   return d.cx * (l + r) + d.cy * (b + t);
 }
 
@@ -361,24 +389,18 @@ __device__ void sb_restrict(const float* u, const float* f, float* r, const Leve
   __syncthreads();
   for (int J = ty; J < c.my; J += kRows)
     for (int I = tx; I < c.mx; I += 32) {
-      const int fi = d.perx ? 2 * I : 2 * I + 1;
-      const int fj = d.pery ? 2 * J : 2 * J + 1;
+      const int fi = d.bx != BC_DIR ? 2 * I : 2 * I + 1;
+      const int fj = d.by != BC_DIR ? 2 * J : 2 * J + 1;
       float s = 0.0f;
 #pragma unroll
       for (int b = -1; b <= 1; ++b) {
         int j = fj + b;
-        if (j < 0 || j >= d.my) {
-          if (!d.pery) continue;
-          j = j < 0 ? j + d.my : j - d.my;
-        }
+        if (!wrap(j, d.my, d.by)) continue;
         const float wb = b == 0 ? 0.5f : 0.25f;
 #pragma unroll
         for (int a = -1; a <= 1; ++a) {
           int i = fi + a;
-          if (i < 0 || i >= d.mx) {
-            if (!d.perx) continue;
-            i = i < 0 ? i + d.mx : i - d.mx;
-          }
+          if (!wrap(i, d.mx, d.bx)) continue;
           s += (a == 0 ? 0.5f : 0.25f) * wb * r[i + j * d.mx];
         }
       }
@@ -400,13 +422,18 @@ __device__ void sb_prolong_add(float* u, const LevelDesc& d, const float* uc, co
 __device__ void sm_dense_solve(float* u, const float* f, const LevelDesc& d, const float* M, double* sh,
                                double* sval) {
   const int n = d.mx * d.my;
-  const bool singular = d.perx && d.pery;
+  const bool singular = d.bx != BC_DIR && d.by != BC_DIR;
   float mean = 0.0f;
-  if (singular) {
-    double s = 0.0;
-    for (int k = threadIdx.x; k < n; k += blockDim.x) s += f[k];
+  if (singular) {  // project f onto the range: subtract its weighted mean
+    double s = 0.0, w = 0.0;
+    for (int k = threadIdx.x; k < n; k += blockDim.x) {
+      const double wk = double(bc_weight(k % d.mx, d.mx, d.bx)) * bc_weight(k / d.mx, d.my, d.by);
+      s += wk * f[k];
+      w += wk;
+    }
     s = block_sum(s, sh);
-    if (threadIdx.x == 0) *sval = s / n;
+    w = block_sum(w, sh);
+    if (threadIdx.x == 0) *sval = s / w;
     __syncthreads();
     mean = float(*sval);
   }
@@ -428,26 +455,33 @@ __device__ void sm_dense_solve(float* u, const float* f, const LevelDesc& d, con
   }
 }
 
-// CG on (-A) u = -f (shared memory); the doubly periodic system is solved in
-// the zero-mean subspace.
+// CG on (-W A) u = -W f (shared memory), W = the solvability weights (1/2 at
+// Neumann ends, making the operator symmetric; 1 otherwise). A singular
+// level (no Dirichlet direction) is solved in its range: f is projected with
+// the weights and u returned with zero mean.
 __device__ void sm_coarse_cg(float* u, const float* f, const LevelDesc& d, float* work, double* sh, double* sval) {
   const int n = d.mx * d.my;
   float* r = work;
   float* p = work + n;
   float* q = work + 2 * n;
-  const bool singular = d.perx && d.pery;
+  const bool singular = d.bx != BC_DIR && d.by != BC_DIR;
+  auto wt = [&](int k) { return bc_weight(k % d.mx, d.mx, d.bx) * bc_weight(k / d.mx, d.my, d.by); };
   double mean = 0.0;
   if (singular) {
-    double s = 0.0;
-    for (int k = threadIdx.x; k < n; k += blockDim.x) s += f[k];
+    double s = 0.0, w = 0.0;
+    for (int k = threadIdx.x; k < n; k += blockDim.x) {
+      s += double(wt(k)) * f[k];
+      w += wt(k);
+    }
     s = block_sum(s, sh);
-    if (threadIdx.x == 0) *sval = s / n;
+    w = block_sum(w, sh);
+    if (threadIdx.x == 0) *sval = s / w;
     __syncthreads();
     mean = *sval;
   }
   double rr = 0.0;
   for (int k = threadIdx.x; k < n; k += blockDim.x) {
-    const float v = -(f[k] - float(mean));
+    const float v = -wt(k) * (f[k] - float(mean));
     u[k] = 0.0f;
     r[k] = v;
     p[k] = v;
@@ -458,15 +492,15 @@ __device__ void sm_coarse_cg(float* u, const float* f, const LevelDesc& d, float
   __syncthreads();
   rr = *sval;
   const double stop = 1e-10 * rr;
-  const int maxit = 2 * n + 10 < 1000 ? 2 * n + 10 : 1000;
+  const int maxit = 2 * n + 10 < 2000 ? 2 * n + 10 : 2000;
   for (int it = 0; it < maxit && rr > stop && rr > 0.0; ++it) {
     double pq = 0.0;
     for (int k = threadIdx.x; k < n; k += blockDim.x) {
       const int i = k % d.mx, j = k / d.mx;
       const float ap = d.cd * p[k] + d.cx * (ld(p, d, i - 1, j) + ld(p, d, i + 1, j)) +
                        d.cy * (ld(p, d, i, j - 1) + ld(p, d, i, j + 1));
-      q[k] = -ap;
-      pq += double(p[k]) * double(-ap);
+      q[k] = -wt(k) * ap;
+      pq += double(p[k]) * double(q[k]);
     }
     pq = block_sum(pq, sh);
     if (threadIdx.x == 0) *sval = pq;
@@ -567,10 +601,17 @@ int blocks_for(int n) {
   return int(b < 2368 ? b : 2368);
 }
 
-LevelDesc desc(const PoissonMG::Level& l) { return LevelDesc{l.mx, l.my, l.perx, l.pery, l.cx, l.cy, l.cd}; }
+LevelDesc desc(const PoissonMG::Level& l) { return LevelDesc{l.mx, l.my, l.bx, l.by, l.cx, l.cy, l.cd}; }
 
-bool can_coarsen(int n, bool per) { return per ? (n >= 4 && n % 2 == 0) : (n >= 3 && n % 2 == 1); }
-bool tiled(const PoissonMG::Level& l) { return l.mx >= SW && l.my >= SH && (!l.perx || l.mx % 2 == 0) && (!l.pery || l.my % 2 == 0); }
+bool can_coarsen(int n, int b) { return b == BC_PER ? (n >= 4 && n % 2 == 0) : (n >= 3 && n % 2 == 1); }
+int coarser(int n, int b) { return b == BC_PER ? n / 2 : b == BC_NEU ? (n + 1) / 2 : (n - 1) / 2; }
+bool tiled(const PoissonMG::Level& l) {
+  return l.mx >= SW && l.my >= SH && (l.bx != BC_PER || l.mx % 2 == 0) && (l.by != BC_PER || l.my % 2 == 0);
+}
+int bc_code(const kern::PoissonLayout& L, bool x) {
+  if (x ? L.periodic_x : L.periodic_y) return BC_PER;
+  return L.fbc[x ? 0 : 2] == kern::FBC_NEUMANN_C ? BC_NEU : BC_DIR;
+}
 
 }  // namespace
 
@@ -579,10 +620,11 @@ PoissonMG::PoissonMG(const kern::PoissonLayout& L, int nu_pre, int nu_post)
   if (!((L.fbc[0] == kern::FBC_PERIODIC_C) == (L.fbc[1] == kern::FBC_PERIODIC_C)) ||
       !((L.fbc[2] == kern::FBC_PERIODIC_C) == (L.fbc[3] == kern::FBC_PERIODIC_C)))
     throw std::invalid_argument("periodic field boundaries must be set on both walls of a direction");
-  for (int w = 0; w < 4; ++w)
-    if (L.fbc[w] != kern::FBC_PERIODIC_C && L.fbc[w] != kern::FBC_DIRICHLET_C)
-      throw std::invalid_argument("field boundary must be Dirichlet or periodic (Neumann is rejected as in "
-                                  "the reference's Poisson set-up)");
+  if (L.fbc[0] != L.fbc[1] || L.fbc[2] != L.fbc[3])
+    throw std::invalid_argument("both walls of a direction must have the same boundary type");
+  const int bx = bc_code(L, true), by = bc_code(L, false);
+  bx_ = bx;
+  by_ = by;
   int mx = L.nkx + 1, my = L.nky + 1;
   if (mx < 1 || my < 1) throw std::invalid_argument("empty Poisson system");
   n_ = mx * my;
@@ -591,8 +633,8 @@ PoissonMG::PoissonMG(const kern::PoissonLayout& L, int nu_pre, int nu_post)
     Level lv;
     lv.mx = mx;
     lv.my = my;
-    lv.perx = L.periodic_x;
-    lv.pery = L.periodic_y;
+    lv.bx = bx;
+    lv.by = by;
     lv.cx = cx;
     lv.cy = cy;
     lv.cd = -2.0f * (cx + cy);
@@ -600,10 +642,10 @@ PoissonMG::PoissonMG(const kern::PoissonLayout& L, int nu_pre, int nu_post)
     lv.u2.resize(size_t(mx) * my, true);
     lv.f.resize(size_t(mx) * my, true);
     lv_.push_back(std::move(lv));
-    if (!(can_coarsen(mx, L.periodic_x) && can_coarsen(my, L.periodic_y))) break;
+    if (!(can_coarsen(mx, bx) && can_coarsen(my, by))) break;
     if (size_t(mx) * my <= 16) break;
-    mx = L.periodic_x ? mx / 2 : (mx - 1) / 2;
-    my = L.periodic_y ? my / 2 : (my - 1) / 2;
+    mx = coarser(mx, bx);
+    my = coarser(my, by);
     cx *= 0.25f;
     cy *= 0.25f;
   }
@@ -629,24 +671,32 @@ PoissonMG::PoissonMG(const kern::PoissonLayout& L, int nu_pre, int nu_post)
   GP_CUDA(cudaFuncSetAttribute(k_small_vcycle, cudaFuncAttributeMaxDynamicSharedMemorySize, int(small_smem_)));
   x2_.resize(size_t(n_), true);
   // Dense inverse of the coarsest operator (FP64 Gauss-Jordan, stored FP32);
-  // the doubly periodic operator is regularised as A + a 11^T, a = |cd| / n.
+  // a singular one (no Dirichlet direction) is regularised as A + a 1 w^T
+  // with w its left null vector and a = |cd| / n, whose inverse returns the
+  // w-orthogonal solution for a right-hand side with w^T f = 0.
   const int nc = c.mx * c.my;
+  singular_ = bx != BC_DIR && by != BC_DIR;
+  wsum_ = 0.0;
+  for (int j = 0; j < my_top(); ++j)
+    for (int i = 0; i < mx_top(); ++i) wsum_ += double(bc_weight(i, mx_top(), bx)) * bc_weight(j, my_top(), by);
   if (nc <= kDenseMax) {
     std::vector<double> A(size_t(nc) * nc, 0.0), I(size_t(nc) * nc, 0.0);
-    auto wrapi = [](int i, int n, bool per) { return per ? ((i % n) + n) % n : i; };
     for (int j = 0; j < c.my; ++j)
       for (int i = 0; i < c.mx; ++i) {
         const int k = i + j * c.mx;
         A[size_t(k) * nc + k] += c.cd;
         const int di[4] = {-1, 1, 0, 0}, dj[4] = {0, 0, -1, 1};
         for (int q = 0; q < 4; ++q) {
-          const int ii = wrapi(i + di[q], c.mx, c.perx), jj = wrapi(j + dj[q], c.my, c.pery);
-          if (ii < 0 || ii >= c.mx || jj < 0 || jj >= c.my) continue;
+          int ii = i + di[q], jj = j + dj[q];
+          if (!wrap(ii, c.mx, c.bx) || !wrap(jj, c.my, c.by)) continue;
           A[size_t(k) * nc + ii + jj * c.mx] += q < 2 ? c.cx : c.cy;
         }
       }
-    if (c.perx && c.pery)
-      for (auto& a : A) a += std::fabs(double(c.cd)) / nc;
+    if (singular_)
+      for (int r = 0; r < nc; ++r)
+        for (int q = 0; q < nc; ++q)
+          A[size_t(r) * nc + q] +=
+              std::fabs(double(c.cd)) / nc * bc_weight(q % c.mx, c.mx, c.bx) * bc_weight(q / c.mx, c.my, c.by);
     for (int k = 0; k < nc; ++k) I[size_t(k) * nc + k] = 1.0;
     for (int col = 0; col < nc; ++col) {
       int piv = col;
@@ -750,7 +800,7 @@ MGResult PoissonMG::solve(const double* b, const double* sums_b, double* x, doub
   MGResult res;
   double* st = state_.get();
   Level& f = lv_[0];
-  const bool singular = L_.periodic_x && L_.periodic_y;
+  const bool singular = singular_;
   k_init<<<1, 1, 0, s>>>(st, sums_b);
   GP_LAUNCH_CHECK();
   k_clear_if_zero_rhs<<<blocks_for(n_), 256, 0, s>>>(x, n_, st);
@@ -758,7 +808,7 @@ MGResult PoissonMG::solve(const double* b, const double* sums_b, double* x, doub
   auto residual_and_check = [&]() {
     k_residual64<<<blocks_for(n_), 256, 0, s>>>(x, b, L_, f.f.get(), st);
     GP_LAUNCH_CHECK();
-    k_check<<<1, 1, 0, s>>>(st, tol, maxiter, n_);
+    k_check<<<1, 1, 0, s>>>(st, tol, maxiter, singular_ ? wsum_ : double(n_));
     GP_LAUNCH_CHECK();
   };
   residual_and_check();

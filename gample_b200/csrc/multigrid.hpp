@@ -3,7 +3,11 @@
 // Replaces AMGCL's SA-AMG + CG (src/EMField.mm:20-28, 412-432, 866) for the
 // 5-point system assembled at src/EMField.mm:236-405:
 //   Cd u_ij + Cx (u_i-1,j + u_i+1,j) + Cy (u_i,j-1 + u_i,j+1) = b_ij
-// with Dirichlet (values folded into b) or periodic directions.
+// with Dirichlet (values folded into b), periodic or Neumann (mirrored: the
+// doubled off-diagonal of the Darwin system, src/EMField.mm:527-560)
+// directions. Without a Dirichlet direction the system is singular: the
+// right-hand side is projected with the left null vector (weight 1/2 at
+// Neumann ends) and the solution is returned with zero mean.
 //
 // Method: defect correction in FP64 around an FP32 V(2,2)-cycle.
 //   x (FP64, warm-started from the previous step like the reference's
@@ -50,7 +54,7 @@ class PoissonMG {
 
   struct Level {
     int mx, my;
-    bool perx, pery;
+    int bx, by;  // 0 Dirichlet, 1 periodic, 2 Neumann (mirror)
     float cx, cy, cd;
     DeviceArray<float> u, u2, f;  // u2: output of the tiled post-smoother
     bool result_in_u2 = false;    // where the level's final correction is
@@ -67,6 +71,11 @@ class PoissonMG {
   int ls_ = 0;              // first level handled by the single-CTA kernel
   size_t small_smem_ = 0;   // its shared-memory bytes
   int last_iters_ = 2;
+  int bx_ = 0, by_ = 0;
+  bool singular_ = false;  // no Dirichlet direction: solved in the range, zero-mean gauge
+  double wsum_ = 0;        // sum of the solvability weights of the finest level
+  int mx_top() const { return L_.nkx + 1; }
+  int my_top() const { return L_.nky + 1; }
   std::vector<Level> lv_;
   DeviceArray<double> x2_;      // ping-pong buffer of the FP64 update
   DeviceArray<float> coarse_inv_;  // dense inverse of the coarsest operator (small coarsest levels)

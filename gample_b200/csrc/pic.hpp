@@ -75,6 +75,20 @@ class EMField {
   SolveStats solvePoisson(double dt, XmlLogger* logger);   // src/EMField.mm:745-1136
   // Combine the fixed-point accumulators (deterministic mode) into rho/jx/jy.
   void finalizeCharge();
+  // src/EMField.mm:1138-1361 (Darwin model, FlagForEquation.EMField == 2):
+  // Helmholtz split of J, vector potential, delEx/delEy/delBz.
+  struct DarwinStats {
+    int iters[3] = {0, 0, 0};       // decompose, Ax, Ay
+    double errors[3] = {0, 0, 0};   // relative residuals
+  };
+  DarwinStats solveVectorPotential(double dt, XmlLogger* logger);
+  bool darwin = false;
+  kern::DarwinGeom dgeom{};
+  kern::PoissonLayout dlayout{};
+  std::unique_ptr<PoissonMG> dmg;
+  DeviceArray<double> psi, Ax, Ay, lastAx, lastAy, drhs, dscr;
+  DarwinStats last_darwin;
+  void setupDarwin();  // src/EMField.mm:447-651
 
   kern::GridDims dims{};
   float dx = 0, dy = 0;

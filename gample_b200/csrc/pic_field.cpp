@@ -157,6 +157,7 @@ EMField::EMField(const Init& init, cudaStream_t s, int nspecies) : stream(s), ho
   mg = std::make_unique<PoissonMG>(L);
   sol.resize(size_t(mg->unknowns()), true);
   b.resize(size_t(mg->unknowns()), true);
+  if (init.flagForEquation.EMField == 2) setupDarwin();
 
   acc_rho.resize(nspecies);
   acc_jx.resize(nspecies);

@@ -114,6 +114,7 @@ void Simulation::cycle() {
   if (em == 1 || em == 2) {
     mark(PH_SOLVE, true);
     last_solve = field->solvePoisson(dt, logger.get());
+    if (em == 2) field->solveVectorPotential(dt, logger.get());  // src/main.mm:187-190
     mark(PH_SOLVE, false);
   }
   const bool field_out = file_output && T.FieldOutput != 0 && cycle_no % T.FieldOutput == 0;

@@ -71,6 +71,12 @@ typedef struct {
 #define GP_FIELD_JY 5  /* float (nx+1)(ny+2) */
 #define GP_FIELD_PHI 6 /* double (nx+3)(ny+3) */
 #define GP_FIELD_SOL 7 /* double (nkx+1)(nky+1): Poisson solution vector (src/EMField.mm:97, 410) */
+#define GP_FIELD_DEL_EX 8  /* float (nx+2)(ny+1): Darwin correction (src/EMField.h, delExBuffer) */
+#define GP_FIELD_DEL_EY 9  /* float (nx+1)(ny+2) */
+#define GP_FIELD_DEL_BZ 10 /* float (nx+2)(ny+2) */
+#define GP_FIELD_PSI 11    /* double (nkx_vec+1)(nky_vec+1): longitudinal potential (src/EMField.mm:1193-1199) */
+#define GP_FIELD_AX 12     /* double, same grid: vector potential Ax (src/EMField.mm:1232-1237) */
+#define GP_FIELD_AY 13     /* double, same grid: Ay (src/EMField.mm:1270-1275) */
 
 /* ---- Init: -[Init parseInputFile:] (src/Init.mm:27-301) ---- */
 gp_status gp_init_parse_file(const char* path, gp_init** out);
@@ -112,6 +118,10 @@ gp_status gp_field_solve_poisson(gp_sim* sim, double dt, gp_solve_stats* out);
 /* Buffer accessors (src/EMField.h:22-37, EMField.mm:1396-1424) */
 gp_status gp_field_download(gp_sim* sim, int which, void* host, size_t bytes);
 gp_status gp_field_upload(gp_sim* sim, int which, const void* host, size_t bytes);
+/* -[EMField solveVectorPotential:withLogger:] (src/EMField.mm:1138-1361):
+ * Darwin model (FlagForEquation.EMField = 2); iterations / relative
+ * residuals of the decomposition, Ax and Ay solves (either may be NULL). */
+gp_status gp_field_solve_darwin(gp_sim* sim, double dt, int iterations[3], double errors[3]);
 /* Set the Poisson tolerance / iteration cap (ToleranceForPoisson, MaxiterForPoisson). */
 gp_status gp_field_set_solver(gp_sim* sim, double tol, int maxiter);
 

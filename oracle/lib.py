@@ -93,6 +93,7 @@ def lib():
             "or_sim_poisson_residual": (d, [vp, dp]),
             "or_sim_get_poisson_solution": (None, [vp, dp]),
             "or_sim_moments": (None, [vp, i, i, C.c_void_p]),
+            "or_darwin": (None, [i, i, i, i, i, C.c_float, C.c_float, d] + [C.c_void_p] * 10),
             "or_det_deposit_rho": (None, [i, i, i, i, i, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                           C.c_void_p]),
             "or_det_deposit_j": (None, [i, i, i, i, i] + [C.c_void_p] * 8),
@@ -256,6 +257,30 @@ class OracleSim:
         out = np.empty((10,) + shape, np.float32)
         lib().or_sim_moments(self.h, sp, 1 if build else 0, out.ctypes.data)
         return dict(zip(self.MOMENTS, out))
+
+
+class Darwin:
+    """The oracle's Darwin solve (src/EMField.mm:1138-1361) with its A_last state."""
+
+    def __init__(self, ngx, ngy, ngb, perx, pery, dx, dy):
+        self.a = (ngx, ngy, ngb, int(perx), int(pery), float(dx), float(dy))
+        self.nx, self.ny = ngx + 2 * ngb, ngy + 2 * ngb
+        self.shape = (ngy - int(pery) + 1, ngx - int(perx) + 1)
+        self.lastAx = np.zeros(self.shape)
+        self.lastAy = np.zeros(self.shape)
+
+    def solve(self, jx, jy, dt):
+        jx = np.ascontiguousarray(jx, np.float32)
+        jy = np.ascontiguousarray(jy, np.float32)
+        psi, ax, ay = (np.zeros(self.shape) for _ in range(3))
+        nx, ny = self.nx, self.ny
+        dex = np.zeros((ny + 1, nx + 2), np.float32)
+        dey = np.zeros((ny + 2, nx + 1), np.float32)
+        dbz = np.zeros((ny + 2, nx + 2), np.float32)
+        lib().or_darwin(*self.a, dt, jx.ctypes.data, jy.ctypes.data, self.lastAx.ctypes.data,
+                        self.lastAy.ctypes.data, psi.ctypes.data, ax.ctypes.data, ay.ctypes.data, dex.ctypes.data,
+                        dey.ctypes.data, dbz.ctypes.data)
+        return {"psi": psi, "Ax": ax, "Ay": ay, "delEx": dex, "delEy": dey, "delBz": dbz}
 
 
 def det_deposit_rho(order, ngx, ngy, ngb, ix, iy, ox, oy):

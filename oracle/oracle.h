@@ -108,6 +108,10 @@ void or_sim_get_poisson_solution(void* h, double* sol);
 /* velocity moments of species sp, 10 x n_rho floats (src/Moment.mm); build != 0:
    Horner weights and FP64 sums (the GPU build's summation) */
 void or_sim_moments(void* h, int sp, int build, float* out);
+/* Darwin model (src/EMField.mm:1138-1361) from given jx, jy (reference extents) */
+void or_darwin(int ngx, int ngy, int ngb, int perx, int pery, float dx, float dy, double dt, const float* jx,
+               const float* jy, double* lastAx, double* lastAy, double* psi, double* Ax, double* Ay, float* delEx,
+               float* delEy, float* delBz);
 
 /* Deterministic-mode deposit of the build restated on the CPU: positions as
  * integer cell (ix, iy) plus float offsets, weights by the build's Horner

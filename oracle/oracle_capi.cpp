@@ -601,6 +601,22 @@ void or_sim_moments(void* h, int sp, int build, float* out) {
   });
 }
 
+// Darwin model from given currents (see darwin_solve); lastAx/lastAy are
+// updated in place; del* must be zero-initialised by the caller.
+void or_darwin(int ngx, int ngy, int ngb, int perx, int pery, float dx, float dy, double dt, const float* jx,
+               const float* jy, double* lastAx, double* lastAy, double* psi, double* Ax, double* Ay, float* delEx,
+               float* delEy, float* delBz) {
+  DarwinIn in{ngx, ngy, ngb, perx != 0, pery != 0, dx, dy, dt};
+  const int n = (ngx - (perx ? 1 : 0) + 1) * (ngy - (pery ? 1 : 0) + 1);
+  std::vector<double> p, ax, ay, lx(lastAx, lastAx + n), ly(lastAy, lastAy + n);
+  darwin_solve<float>(in, jx, jy, p, ax, ay, lx, ly, delEx, delEy, delBz);
+  std::copy(p.begin(), p.end(), psi);
+  std::copy(ax.begin(), ax.end(), Ax);
+  std::copy(ay.begin(), ay.end(), Ay);
+  std::copy(lx.begin(), lx.end(), lastAx);
+  std::copy(ly.begin(), ly.end(), lastAy);
+}
+
 static inline int64_t quant40(float w) {
   // w * 2^40 is exact in float (power-of-two scale); round half to even.
   return std::llrint(double(w * 1099511627776.0f));

@@ -1049,6 +1049,160 @@ inline void generate_one(uint32_t id, int genType, const GenParams& prm, RNGStat
   states[id] = rng;
 }
 
+// -------------------------------------------------------- Darwin model
+// src/EMField.mm:447-651 (operator) and 1138-1361 (solveVectorPotential) on
+// the vector-potential grid (nkx+1)(nky+1), nkx = ngx - [x periodic]. The
+// build's documented choices are restated too: with a Neumann direction the
+// right-hand side is also projected with the solvability weights (1/2 at
+// the ends), solutions have zero mean, the last column (row) of a periodic
+// direction closes through the wrap, and delEy sits at (i+ngb, j+ngb+1).
+// Solves: CG on the symmetrised operator W A (W = the weights) to 1e-13.
+struct DarwinIn {
+  int ngx, ngy, ngb;
+  bool perx, pery;
+  float dx, dy;
+  double dt;
+};
+
+inline double darwin_weight(int i, int n, bool per) { return (!per && (i == 0 || i == n - 1)) ? 0.5 : 1.0; }
+
+inline CSR darwin_csr(int nkx, int nky, bool perx, bool pery, double Cx, double Cy, double Cd, bool symmetrise) {
+  CSR A;
+  const int mx = nkx + 1, my = nky + 1;
+  A.n = mx * my;
+  A.ptr.push_back(0);
+  for (int j = 0; j < my; ++j)
+    for (int i = 0; i < mx; ++i) {
+      const int k = i + j * mx;
+      const double w = symmetrise ? darwin_weight(i, mx, perx) * darwin_weight(j, my, pery) : 1.0;
+      std::vector<std::pair<int, double>> e;
+      e.push_back({k, Cd});
+      auto side = [&](int idx, int n, bool per, int stride, double C) {
+        if (idx == 0) {
+          if (per) {
+            e.push_back({k + (n - 1) * stride, C});
+            e.push_back({k + stride, C});
+          } else if (n > 1) {
+            e.push_back({k + stride, 2 * C});  // Neumann: doubled off-diagonal (src/EMField.mm:531-537)
+          }
+        } else if (idx == n - 1) {
+          if (per) {
+            e.push_back({k - stride, C});
+            e.push_back({k - (n - 1) * stride, C});
+          } else {
+            e.push_back({k - stride, 2 * C});
+          }
+        } else {
+          e.push_back({k - stride, C});
+          e.push_back({k + stride, C});
+        }
+      };
+      side(i, mx, perx, 1, Cx);
+      side(j, my, pery, mx, Cy);
+      for (auto& q : e) {
+        A.col.push_back(q.first);
+        A.val.push_back(w * q.second);
+      }
+      A.ptr.push_back(int(A.col.size()));
+    }
+  return A;
+}
+
+template <typename R>
+void darwin_solve(const DarwinIn& in, const R* jx, const R* jy, std::vector<double>& psi, std::vector<double>& Ax,
+                  std::vector<double>& Ay, std::vector<double>& lastAx, std::vector<double>& lastAy, float* delEx,
+                  float* delEy, float* delBz) {
+  const int nkx = in.ngx - (in.perx ? 1 : 0), nky = in.ngy - (in.pery ? 1 : 0);
+  const int mx = nkx + 1, my = nky + 1, n = mx * my;
+  const int ngb = in.ngb, nx = in.ngx + 2 * ngb;
+  const float dx = in.dx, dy = in.dy;
+  const double Cx = 1.0 / dx / dx, Cy = 1.0 / dy / dy, Cd = -2 * (1.0 / dx / dx + 1.0 / dy / dy);
+  const CSR WA = darwin_csr(nkx, nky, in.perx, in.pery, Cx, Cy, Cd, true);
+  auto solve = [&](std::vector<double> rhs, std::vector<double>& x) {
+    double m = 0;
+    for (double v : rhs) m += v;
+    m /= n;
+    for (double& v : rhs) v -= m;  // src/EMField.mm:1186-1191
+    double sw = 0, ww = 0;
+    for (int k = 0; k < n; ++k) {
+      const double w = darwin_weight(k % mx, mx, in.perx) * darwin_weight(k / mx, my, in.pery);
+      sw += w * rhs[k];
+      ww += w;
+    }
+    for (double& v : rhs) v -= sw / ww;
+    std::vector<double> wb(n);
+    for (int k = 0; k < n; ++k) wb[k] = darwin_weight(k % mx, mx, in.perx) * darwin_weight(k / mx, my, in.pery) * rhs[k];
+    x.assign(n, 0.0);
+    cg_solve(WA, wb, x, 1e-13, 20000, true);
+    double xm = 0;
+    for (double v : x) xm += v;
+    xm /= n;
+    for (double& v : x) v -= xm;
+  };
+  // div J (src/EMField.mm:1150-1184)
+  std::vector<double> rhs(n);
+  for (int j = 0; j <= nky; j++)
+    for (int i = 0; i <= nkx; i++) {
+      double r = 0.0;
+      const int ix = i + ngb, iy = j + ngb;
+      if (!in.perx) {
+        if (i == 0)
+          r += double(-2 * float(jx[ix + iy * (nx + 2)]) / dx);
+        else if (i == nkx)
+          r += double(2 * float(jx[ix + iy * (nx + 2)]) / dx);
+      }
+      if (!in.pery) {
+        if (j == 0)
+          r += double(-2 * float(jy[ix + iy * (nx + 1)]) / dy);
+        else if (j == nky)
+          r += double(2 * float(jy[ix + iy * (nx + 1)]) / dy);
+      }
+      const double djx = double((float(jx[ix + 1 + iy * (nx + 2)]) - float(jx[ix + iy * (nx + 2)])) / dx);
+      const double djy = double((float(jy[ix + (iy + 1) * (nx + 1)]) - float(jy[ix + iy * (nx + 1)])) / dy);
+      rhs[i + j * mx] = r + (djx + djy);
+    }
+  solve(rhs, psi);
+  const double f = -4 * PI / 2.99792458e10;
+  for (int j = 0; j <= nky; j++)  // src/EMField.mm:1201-1229
+    for (int i = 0; i <= nkx; i++) {
+      const int k = i + j * mx;
+      double r = 0.0;
+      if (i < nkx || in.perx) {
+        const int k1 = i < nkx ? k + 1 : k - nkx;
+        const double jl = (psi[k1] - psi[k]) / double(dx);
+        r = f * (double(float(jx[(i + ngb + 1) + (j + ngb) * (nx + 2)])) - jl);
+      }
+      rhs[k] = r;
+    }
+  solve(rhs, Ax);
+  for (int j = 0; j <= nky; j++)  // src/EMField.mm:1239-1267
+    for (int i = 0; i <= nkx; i++) {
+      const int k = i + j * mx;
+      double r = 0.0;
+      if (j < nky || in.pery) {
+        const int k1 = j < nky ? k + mx : k - nky * mx;
+        const double jl = (psi[k1] - psi[k]) / double(dy);
+        r = f * (double(float(jy[(i + ngb) + (j + ngb + 1) * (nx + 1)])) - jl);
+      }
+      rhs[k] = r;
+    }
+  solve(rhs, Ay);
+  const double cdt = 2.99792458e10 * in.dt;  // src/EMField.mm:1277-1297
+  const int ni = in.perx ? nkx + 1 : nkx, nj = in.pery ? nky + 1 : nky;
+  for (int j = 0; j < nj; j++)
+    for (int i = 0; i < ni; i++) {
+      const int kf = i + j * mx;
+      const int kx1 = i < nkx ? kf + 1 : kf - nkx, ky1 = j < nky ? kf + mx : kf - nky * mx;
+      const int kpx = (i + ngb + 1) + (j + ngb) * (nx + 2);
+      const int kpy = (i + ngb) + (j + ngb + 1) * (nx + 1);
+      delEx[kpx] = float(-(Ax[kf] - lastAx[kf]) / cdt);
+      delEy[kpy] = float(-(Ay[kf] - lastAy[kf]) / cdt);
+      delBz[kpx + (nx + 2)] = float((Ay[kx1] - Ay[kf]) / double(dx) - (Ax[ky1] - Ax[kf]) / double(dy));
+    }
+  lastAx = Ax;
+  lastAy = Ay;
+}
+
 // -------------------------------------------------------- moments
 // Velocity moments of one species: src/Moment.mm:55-129 (kernel) and
 // :287-316 (normalisation). Outputs 10 arrays of (nx+1)(ny+1):
