@@ -92,6 +92,13 @@ EXPORTS = {
     "gp_sim_output_moments": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
     "gp_sim_save_progress": (C.c_int, [C.c_void_p, C.c_int]),
     "gp_sim_load_progress": (C.c_int, [C.c_void_p, C.c_int]),
+    "gp_nn_create": (C.c_int, [C.c_int, C.c_int, C.c_uint64, C.POINTER(C.c_void_p)]),
+    "gp_nn_free": (None, [C.c_void_p]),
+    "gp_nn_forward": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "gp_nn_loss_grad": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_float)]),
+    "gp_nn_train_step": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_float, C.POINTER(C.c_float)]),
+    "gp_nn_layer_info": (C.c_int, [C.c_void_p, C.c_int] + [C.POINTER(C.c_int)] * 3),
+    "gp_nn_param": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_size_t, C.c_int]),
     "gp_deposit_charge_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_uint32, C.c_float,
                                             C.c_void_p, C.c_void_p]),
     "gp_last_error": (C.c_char_p, []),
@@ -324,3 +331,57 @@ def device_count():
 
 def kernel_launches():
     return int(lib().gp_kernel_launches())
+
+
+class Net:
+    """The learned warm-start network on the GPU (gp_nn_*)."""
+
+    def __init__(self, h, w, seed=0):
+        self.h, self.w = h, w
+        p = C.c_void_p()
+        check(lib().gp_nn_create(h, w, seed, C.byref(p)))
+        self.p = p
+        self.layers = []
+        for i in range(12):
+            a, b, c = C.c_int(), C.c_int(), C.c_int()
+            check(lib().gp_nn_layer_info(self.p, i, C.byref(a), C.byref(b), C.byref(c)))
+            self.layers.append((a.value, b.value, c.value))
+
+    def close(self):
+        if getattr(self, "p", None):
+            lib().gp_nn_free(self.p)
+            self.p = None
+
+    def __del__(self):
+        self.close()
+
+    def forward(self, x):
+        x = np.ascontiguousarray(x, np.float32)
+        out = np.empty((self.h, self.w), np.float32)
+        check(lib().gp_nn_forward(self.p, x.ctypes.data, out.ctypes.data))
+        return out
+
+    def loss_grad(self, x, t):
+        x = np.ascontiguousarray(x, np.float32)
+        t = np.ascontiguousarray(t, np.float32)
+        loss = C.c_float()
+        check(lib().gp_nn_loss_grad(self.p, x.ctypes.data, t.ctypes.data, C.byref(loss)))
+        return loss.value
+
+    def train_step(self, x, t, lr):
+        x = np.ascontiguousarray(x, np.float32)
+        t = np.ascontiguousarray(t, np.float32)
+        loss = C.c_float()
+        check(lib().gp_nn_train_step(self.p, x.ctypes.data, t.ctypes.data, lr, C.byref(loss)))
+        return loss.value
+
+    def param(self, layer, which):
+        cin, cout, kpad = self.layers[layer]
+        n = cout * kpad if which in (0, 2) else cout
+        a = np.empty(n, np.float32)
+        check(lib().gp_nn_param(self.p, layer, which, a.ctypes.data, n, 0))
+        return a.reshape(cout, kpad) if which in (0, 2) else a
+
+    def set_param(self, layer, which, a):
+        a = np.ascontiguousarray(a, np.float32).ravel()
+        check(lib().gp_nn_param(self.p, layer, which, a.ctypes.data, a.size, 1))

@@ -5,6 +5,7 @@
 
 #include "../../include/gample_gpu.h"
 #include "fileio.hpp"
+#include "learned.hpp"
 #include "simulation.hpp"
 
 #include <atomic>
@@ -22,6 +23,15 @@ struct gp_init {
 };
 struct gp_sim {
   std::unique_ptr<gample::Simulation> sim;
+};
+struct gp_nn {
+  std::unique_ptr<gample::nn::WarmStartNet> net;
+  cudaStream_t stream = nullptr;
+  gample::DeviceArray<float> in, out, target;
+  ~gp_nn() {
+    net.reset();
+    if (stream) cudaStreamDestroy(stream);
+  }
 };
 
 namespace {
@@ -131,6 +141,97 @@ gp_status gp_deposit_charge_noalloc(int weighting_order, int ngx, int ngy, const
       g_error = e.what();
       return GP_ERR_CAPACITY;
     }
+    return GP_OK;
+  });
+}
+
+gp_status gp_nn_create(int h, int w, uint64_t seed, gp_nn** out) {
+  return guarded([&] {
+    if (!out) throw std::invalid_argument("null output handle");
+    auto n = std::make_unique<gp_nn>();
+    GP_CUDA(cudaStreamCreateWithFlags(&n->stream, cudaStreamNonBlocking));
+    n->net = std::make_unique<gample::nn::WarmStartNet>(h, w, seed, n->stream);
+    n->in.resize(size_t(h) * w * 2);
+    n->out.resize(size_t(h) * w);
+    n->target.resize(size_t(h) * w);
+    *out = n.release();
+    return GP_OK;
+  });
+}
+void gp_nn_free(gp_nn* nn) { delete nn; }
+
+namespace {
+gp_nn& NN(gp_nn* nn) {
+  if (!nn || !nn->net) throw std::invalid_argument("null network handle");
+  return *nn;
+}
+void put(gample::DeviceArray<float>& d, const float* h, cudaStream_t s) {
+  if (!h) throw std::invalid_argument("null host buffer");
+  GP_CUDA(cudaMemcpyAsync(d.get(), h, d.bytes(), cudaMemcpyHostToDevice, s));
+}
+}  // namespace
+
+gp_status gp_nn_forward(gp_nn* nn, const float* in, float* out) {
+  return guarded([&] {
+    auto& n = NN(nn);
+    put(n.in, in, n.stream);
+    n.net->forward(n.in.get(), n.out.get());
+    GP_CUDA(cudaMemcpyAsync(out, n.out.get(), n.out.bytes(), cudaMemcpyDeviceToHost, n.stream));
+    GP_CUDA(cudaStreamSynchronize(n.stream));
+    return GP_OK;
+  });
+}
+
+gp_status gp_nn_loss_grad(gp_nn* nn, const float* in, const float* target, float* loss) {
+  return guarded([&] {
+    auto& n = NN(nn);
+    put(n.in, in, n.stream);
+    put(n.target, target, n.stream);
+    const float l = n.net->loss_and_grad(n.in.get(), n.target.get());
+    if (loss) *loss = l;
+    return GP_OK;
+  });
+}
+
+gp_status gp_nn_train_step(gp_nn* nn, const float* in, const float* target, float lr, float* loss) {
+  return guarded([&] {
+    auto& n = NN(nn);
+    put(n.in, in, n.stream);
+    put(n.target, target, n.stream);
+    const float l = n.net->train_step(n.in.get(), n.target.get(), lr);
+    if (loss) *loss = l;
+    return GP_OK;
+  });
+}
+
+gp_status gp_nn_layer_info(gp_nn* nn, int layer, int* cin, int* cout, int* kpad) {
+  return guarded([&] {
+    auto& n = NN(nn);
+    if (layer < 0 || layer >= n.net->num_layers()) throw std::invalid_argument("layer index out of range");
+    const auto& L = n.net->layer(layer);
+    if (cin) *cin = L.cin;
+    if (cout) *cout = L.cout;
+    if (kpad) *kpad = L.kpad;
+    return GP_OK;
+  });
+}
+
+gp_status gp_nn_param(gp_nn* nn, int layer, int which, float* host, size_t count, int set) {
+  return guarded([&] {
+    auto& n = NN(nn);
+    if (layer < 0 || layer >= n.net->num_layers()) throw std::invalid_argument("layer index out of range");
+    auto& L = n.net->layer(layer);
+    gample::DeviceArray<float>* a = which == 0 ? &L.w : which == 1 ? &L.b : which == 2 ? &L.gw : which == 3 ? &L.gb
+                                                                                                           : nullptr;
+    if (!a || (set && which >= 2)) throw std::invalid_argument("parameter selector out of range");
+    if (!host || count != a->size()) throw std::invalid_argument("host buffer size does not match the parameter");
+    if (set) {
+      GP_CUDA(cudaMemcpyAsync(a->get(), host, a->bytes(), cudaMemcpyHostToDevice, n.stream));
+      n.net->sync_weights();
+    } else {
+      GP_CUDA(cudaMemcpyAsync(host, a->get(), a->bytes(), cudaMemcpyDeviceToHost, n.stream));
+    }
+    GP_CUDA(cudaStreamSynchronize(n.stream));
     return GP_OK;
   });
 }

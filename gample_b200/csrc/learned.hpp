@@ -1,0 +1,95 @@
+// learned.hpp -- learned warm start of the Poisson solve.
+//
+// A 4-level convolutional encoder-decoder (3 x 3 kernels, 32/64/128/256
+// channels, skip connections, BF16 weights and activations, FP32
+// accumulation on the tensor cores) maps the normalised right-hand side and
+// the previous solution on the unknown grid to a correction of the previous
+// solution; the multigrid then solves from (previous + correction) to the
+// same relative residual as without it, so the network only changes the
+// starting point, never the answer. Training runs on the GPU with the same
+// kernels (im2col + tcgen05 GEMM forward, GEMM-based input and weight
+// gradients, Adam) on (rhs, previous phi) -> (phi - previous phi) pairs the
+// simulator produces while it runs.
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "device.hpp"
+
+namespace gample {
+namespace nn {
+
+// out[row * ldo + n] = act(alpha * acc + bias[n]) for row < m_valid, n < n_valid
+struct GemmEpilogue {
+  float alpha = 1.0f;
+  const float* bias = nullptr;
+  int relu = 0;
+  int accumulate = 0;  // out_f32 += value
+  float* out_f32 = nullptr;
+  __nv_bfloat16* out_bf16 = nullptr;
+  int ldo = 0;
+  int m_valid = 0, n_valid = 0;
+};
+
+// C = A[M x K] * B[N x K]^T on the tensor cores (both K-major BF16); M a
+// multiple of 128, N of 32, K of 32. err: device int set to 1 if an MMA
+// completion wait timed out.
+void gemm_bf16(const __nv_bfloat16* A, const __nv_bfloat16* B, int M, int N, int K, const GemmEpilogue& ep, int* err,
+               cudaStream_t s);
+
+struct ConvLayer {
+  int cin, cout;           // channels
+  int kpad;                // 9 * cin rounded up to a multiple of 32
+  int cout_p;              // cout rounded up to a multiple of 32
+  bool relu;
+  DeviceArray<float> w, b;           // FP32 master weights [cout][kpad] (zero padding), bias
+  DeviceArray<__nv_bfloat16> wb;     // BF16 copy [cout_p][kpad]
+  DeviceArray<__nv_bfloat16> wt;     // BF16 transpose [kpad][cout_p] (input-gradient GEMM)
+  DeviceArray<float> gw, gb;         // gradients
+  DeviceArray<float> mw, vw, mb, vb; // Adam moments
+};
+
+class WarmStartNet {
+ public:
+  // h, w: grid (multiples of 8); the levels run at h, h/2, h/4, h/8.
+  WarmStartNet(int h, int w, uint64_t seed, cudaStream_t s);
+  // in: NHWC input [h][w][2] FP32 (normalised); out: [h][w] FP32
+  void forward(const float* in, float* out);
+  // One Adam step on the mean-squared error against target [h][w]; returns
+  // the loss of the forward pass (synchronous read of one float).
+  float train_step(const float* in, const float* target, float lr);
+  // Parameter access for the gradient check (FP32 masters, layer by layer).
+  int num_layers() const { return int(layers_.size()); }
+  ConvLayer& layer(int i) { return layers_[i]; }
+  void sync_weights();  // refresh the BF16 copies after the FP32 masters changed
+  // forward + backward without the optimiser step (gradients left in gw/gb)
+  float loss_and_grad(const float* in, const float* target);
+  double flops_forward() const;
+  int h() const { return h_; }
+  int w() const { return w_; }
+  cudaStream_t stream;
+
+ private:
+  struct Act {  // one activation tensor NHWC
+    int h, w, c;
+    DeviceArray<__nv_bfloat16> y;  // BF16 values (post activation)
+    DeviceArray<float> g;          // FP32 gradient
+  };
+  void conv_forward(ConvLayer& L, const Act& x, Act& y, float* out_f32 = nullptr);
+  void conv_backward(ConvLayer& L, const Act& x, Act& y, Act* dx, const float* gy_override = nullptr);
+  int h_, w_;
+  std::vector<ConvLayer> layers_;
+  std::vector<Act> acts_;
+  DeviceArray<__nv_bfloat16> col_, colT_, gyT_, gyb_;
+  DeviceArray<float> gcol_, out_, gout_, loss_;
+  DeviceArray<int> err_;
+  int step_ = 0;
+};
+
+}  // namespace nn
+}  // namespace gample

@@ -1,0 +1,188 @@
+// tc_gemm.cu -- BF16 GEMM on the 5th-generation tensor cores (sm_100a):
+// C[M x N] = A[M x K] * B[N x K]^T, A and B K-major (row-major with K
+// contiguous), FP32 accumulation in tensor memory.
+//
+// One CTA (128 threads) per 128 x BN tile. Per K step of BK elements the
+// threads stage A and B in shared memory in the canonical no-swizzle
+// K-major layout (8-row x 16-byte core matrices; leading byte offset
+// between the two K halves of an MMA, stride byte offset between 8-row
+// groups), one elected thread issues BK/16 tcgen05.mma (M=128, N=BN, K=16)
+// into a BN-column TMEM accumulator and commits to an mbarrier; every wait
+// on it is bounded (on time-out the kernel sets an error flag, skips the
+// epilogue and still frees its TMEM). Epilogue: each warp reads its 32 TMEM
+// lanes (rows) with tcgen05.ld and applies one of the fused epilogues.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <stdexcept>
+
+#include "device.hpp"
+#include "learned.hpp"
+
+namespace gample {
+namespace nn {
+
+namespace {
+
+constexpr int BM = 128;
+constexpr int kThreads = 128;
+
+__device__ __forceinline__ uint32_t su32(const void* p) { return static_cast<uint32_t>(__cvta_generic_to_shared(p)); }
+
+// Shared-memory matrix descriptor (sm100 layout: start >> 4 in [0,14),
+// leading byte offset >> 4 in [16,30), stride byte offset >> 4 in [32,46),
+// version 1 in [46,48), no swizzle).
+__device__ __forceinline__ uint64_t sdesc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  return uint64_t((saddr >> 4) & 0x3FFF) | (uint64_t((lbo >> 4) & 0x3FFF) << 16) |
+         (uint64_t((sbo >> 4) & 0x3FFF) << 32) | (uint64_t(1) << 46);
+}
+
+// Instruction descriptor: F32 accumulator, BF16 A and B, both K-major, M=128.
+template <int BN>
+__host__ __device__ constexpr uint32_t idesc() {
+  return (1u << 4) | (1u << 7) | (1u << 10) | (uint32_t(BN >> 3) << 17) | (uint32_t(BM >> 4) << 24);
+}
+
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase) {
+  const uint32_t addr = su32(bar);
+  for (int i = 0; i < (1 << 20); ++i) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(addr), "r"(phase)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+template <int BN, int BK>
+__global__ void __launch_bounds__(kThreads) k_gemm(const __nv_bfloat16* __restrict__ A,
+                                                   const __nv_bfloat16* __restrict__ B, int M, int N, int K,
+                                                   GemmEpilogue ep, int* err) {
+  static_assert(BN == 32 || BN == 64 || BN == 128, "BN");
+  static_assert(BK == 32 || BK == 64, "BK");
+  __shared__ __align__(128) __nv_bfloat16 sA[BM * BK];
+  __shared__ __align__(128) __nv_bfloat16 sB[BN * BK];
+  __shared__ __align__(8) uint64_t mbar;
+  __shared__ uint32_t tbase;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(su32(&tbase)), "r"(BN)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(su32(&mbar)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = tbase;
+  const uint32_t aaddr = su32(sA), baddr = su32(sB);
+  uint32_t phase = 0;
+  bool ok = true;
+  for (int k0 = 0; k0 < K && ok; k0 += BK) {
+    for (int c = tid; c < BM * (BK / 8); c += kThreads) {
+      const int m = c / (BK / 8), kc = c % (BK / 8);
+      const uint4 v = *reinterpret_cast<const uint4*>(A + size_t(m0 + m) * K + k0 + kc * 8);
+      *reinterpret_cast<uint4*>(reinterpret_cast<char*>(sA) + kc * (BM / 8) * 128 + (m / 8) * 128 + (m % 8) * 16) = v;
+    }
+    for (int c = tid; c < BN * (BK / 8); c += kThreads) {
+      const int n = c / (BK / 8), kc = c % (BK / 8);
+      const uint4 v = *reinterpret_cast<const uint4*>(B + size_t(n0 + n) * K + k0 + kc * 8);
+      *reinterpret_cast<uint4*>(reinterpret_cast<char*>(sB) + kc * (BN / 8) * 128 + (n / 8) * 128 + (n % 8) * 16) = v;
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    if (tid == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+#pragma unroll
+      for (int ks = 0; ks < BK / 16; ++ks) {
+        const uint64_t da = sdesc(aaddr + ks * 2 * (BM / 8) * 128, (BM / 8) * 128, 128);
+        const uint64_t db = sdesc(baddr + ks * 2 * (BN / 8) * 128, (BN / 8) * 128, 128);
+        const uint32_t acc = (k0 > 0 || ks > 0) ? 1u : 0u;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\ttcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(
+                tmem),
+            "l"(da), "l"(db), "r"(idesc<BN>()), "r"(acc)
+            : "memory");
+      }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(su32(&mbar))
+                   : "memory");
+    }
+    ok = mbar_wait(&mbar, phase);
+    phase ^= 1;
+    __syncthreads();
+  }
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (!ok) {
+    if (tid == 0) atomicExch(err, 1);
+  } else {
+    const int row = m0 + warp * 32 + lane;
+#pragma unroll 1
+    for (int c0 = 0; c0 < BN; c0 += 16) {
+      uint32_t r[16];
+      tmem_ld16(tmem + (uint32_t(warp * 32) << 16) + uint32_t(c0), r);
+      if (row >= ep.m_valid) continue;
+#pragma unroll
+      for (int j = 0; j < 16; ++j) {
+        const int n = n0 + c0 + j;
+        if (n >= ep.n_valid) continue;
+        float v = __uint_as_float(r[j]) * ep.alpha;
+        if (ep.bias) v += ep.bias[n];
+        if (ep.relu) v = fmaxf(v, 0.0f);
+        if (ep.out_f32) {
+          const size_t o = size_t(row) * ep.ldo + n;
+          ep.out_f32[o] = ep.accumulate ? ep.out_f32[o] + v : v;
+        }
+        if (ep.out_bf16) ep.out_bf16[size_t(row) * ep.ldo + n] = __float2bfloat16_rn(v);
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(BN) : "memory");
+}
+
+template <int BN>
+void launch_bn(const __nv_bfloat16* A, const __nv_bfloat16* B, int M, int N, int K, const GemmEpilogue& ep, int* err,
+               cudaStream_t s) {
+  dim3 grid(N / BN, M / BM);
+  if (K % 64 == 0)
+    k_gemm<BN, 64><<<grid, kThreads, 0, s>>>(A, B, M, N, K, ep, err);
+  else
+    k_gemm<BN, 32><<<grid, kThreads, 0, s>>>(A, B, M, N, K, ep, err);
+  GP_LAUNCH_CHECK();
+}
+
+}  // namespace
+
+void gemm_bf16(const __nv_bfloat16* A, const __nv_bfloat16* B, int M, int N, int K, const GemmEpilogue& ep, int* err,
+               cudaStream_t s) {
+  if (M <= 0 || N <= 0 || K <= 0 || M % BM != 0 || K % 32 != 0)
+    throw std::invalid_argument("gemm_bf16: M must be a multiple of 128 and K of 32");
+  if (N % 128 == 0)
+    launch_bn<128>(A, B, M, N, K, ep, err, s);
+  else if (N % 64 == 0)
+    launch_bn<64>(A, B, M, N, K, ep, err, s);
+  else if (N % 32 == 0)
+    launch_bn<32>(A, B, M, N, K, ep, err, s);
+  else
+    throw std::invalid_argument("gemm_bf16: N must be a multiple of 32");
+}
+
+}  // namespace nn
+}  // namespace gample

@@ -32,6 +32,7 @@ typedef int gp_status;
 
 typedef struct gp_init gp_init; /* parsed condition (src/Init.h:101-118) */
 typedef struct gp_sim gp_sim;   /* Particle[], EMField, Collision, XmlLogger of one run */
+typedef struct gp_nn gp_nn;     /* learned warm-start network (build addition) */
 
 /* Particle record of the reference (src/Particle.h:14-21): x, y in grid units
  * offset by ngb, velocities in cm/s, piflag 0 = live, 1..4 = left through
@@ -198,6 +199,22 @@ gp_status gp_collision_flux_reinjection(gp_sim* sim, double dt, int* addn);
  * of the kernels themselves surface at the next synchronisation. */
 gp_status gp_deposit_charge_noalloc(int weighting_order, int ngx, int ngy, const gp_particle_state* particles,
                                     uint32_t n, float scale, float* rho, void* stream);
+
+/* ---- learned warm start of the Poisson solve (build addition; no
+ * reference counterpart): a 4-level convolutional encoder-decoder (3x3,
+ * 32/64/128/256 channels, BF16 on the tensor cores). Host buffers: in is
+ * [h][w][2] (normalised rhs, previous phi), out/target [h][w]. ---- */
+gp_status gp_nn_create(int h, int w, uint64_t seed, gp_nn** out);
+void gp_nn_free(gp_nn* nn);
+gp_status gp_nn_forward(gp_nn* nn, const float* in, float* out);
+/* forward + backward (mean-squared error), gradients kept for gp_nn_param */
+gp_status gp_nn_loss_grad(gp_nn* nn, const float* in, const float* target, float* loss);
+/* one Adam step (learning rate lr) */
+gp_status gp_nn_train_step(gp_nn* nn, const float* in, const float* target, float lr, float* loss);
+gp_status gp_nn_layer_info(gp_nn* nn, int layer, int* cin, int* cout, int* kpad);
+/* which: 0 weights [cout][kpad], 1 bias [cout], 2 weight gradient, 3 bias
+ * gradient (FP32); set != 0 writes 0/1 */
+gp_status gp_nn_param(gp_nn* nn, int layer, int which, float* host, size_t count, int set);
 
 /* ---- misc ---- */
 const char* gp_last_error(void);
