@@ -92,6 +92,8 @@ EXPORTS = {
     "gp_sim_output_moments": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
     "gp_sim_save_progress": (C.c_int, [C.c_void_p, C.c_int]),
     "gp_sim_load_progress": (C.c_int, [C.c_void_p, C.c_int]),
+    "gp_field_learned": (C.c_int, [C.c_void_p, C.c_int, C.c_float, C.c_uint64]),
+    "gp_field_learned_stats": (C.c_int, [C.c_void_p, C.c_void_p]),
     "gp_nn_create": (C.c_int, [C.c_int, C.c_int, C.c_uint64, C.POINTER(C.c_void_p)]),
     "gp_nn_free": (None, [C.c_void_p]),
     "gp_nn_forward": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
@@ -230,6 +232,17 @@ class Sim:
         px = types.get("Xmin") == "periodic"
         py = types.get("Ymin") == "periodic"
         return (self.ngy - (1 if py else 0) + 1, self.ngx - (1 if px else 0) + 1)
+
+    LEARNED_KEYS = ("loss", "iters_learned", "iters_plain", "ms_learned", "ms_plain", "ms_net", "rel0_learned",
+                    "rel0_plain", "trained_steps")
+
+    def set_learned(self, mode, lr=1e-3, seed=0):
+        check(lib().gp_field_learned(self.h, mode, lr, seed))
+
+    def learned_stats(self):
+        out = (C.c_double * 9)()
+        check(lib().gp_field_learned_stats(self.h, out))
+        return dict(zip(self.LEARNED_KEYS, list(out)))
 
     def solve_darwin(self, dt):
         it = (C.c_int * 3)()

@@ -409,6 +409,24 @@ gp_status gp_field_solve_darwin(gp_sim* sim, double dt, int iterations[3], doubl
     return GP_OK;
   });
 }
+gp_status gp_field_learned(gp_sim* sim, int mode, float lr, uint64_t seed) {
+  return guarded([&] {
+    if (mode < 0 || mode > 7 || !(lr >= 0)) throw std::invalid_argument("learned mode must be 0..7 and lr >= 0");
+    S(sim).field->setLearned(mode, lr, seed);
+    return GP_OK;
+  });
+}
+gp_status gp_field_learned_stats(gp_sim* sim, double out[9]) {
+  return guarded([&] {
+    if (!out) throw std::invalid_argument("null output");
+    const auto& st = S(sim).field->last_learned;
+    const double v[9] = {st.loss,      double(st.iters_learned), double(st.iters_plain),
+                         st.ms_learned, st.ms_plain,              st.ms_net,
+                         st.rel0_learned, st.rel0_plain,          double(st.trained_steps)};
+    for (int i = 0; i < 9; ++i) out[i] = v[i];
+    return GP_OK;
+  });
+}
 gp_status gp_field_download(gp_sim* sim, int which, void* host, size_t bytes) {
   return guarded([&] {
     auto& s = S(sim);

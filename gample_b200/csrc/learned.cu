@@ -314,6 +314,7 @@ void WarmStartNet::conv_backward(ConvLayer& L, const Act& x, Act& y, Act* dx, co
   ew.ldo = L.kpad;
   ew.m_valid = L.cout;
   ew.n_valid = L.kpad;
+  ew.split_k = 1;
   gemm_bf16(gyT_.get(), colT_.get(), cout_pm, L.kpad, rows, ew, err_.get(), stream);
   if (!dx) return;
   // input gradient: gcol [rows][kpad] = gy [rows x cout_p] * wt [kpad x cout_p]^T, then col2im

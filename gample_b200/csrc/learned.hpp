@@ -34,6 +34,7 @@ struct GemmEpilogue {
   __nv_bfloat16* out_bf16 = nullptr;
   int ldo = 0;
   int m_valid = 0, n_valid = 0;
+  int split_k = 0;  // allow splitting K over CTAs (plain FP32 output, zeroed and accumulated atomically)
 };
 
 // C = A[M x K] * B[N x K]^T on the tensor cores (both K-major BF16); M a
@@ -41,6 +42,15 @@ struct GemmEpilogue {
 // completion wait timed out.
 void gemm_bf16(const __nv_bfloat16* A, const __nv_bfloat16* B, int M, int N, int K, const GemmEpilogue& ep, int* err,
                cudaStream_t s);
+
+// Unknown grid <-> network tensors (inv: device floats 1/RMS of the rhs, of
+// phi and of the correction).
+void pack_input(const double* b, const double* phi, int mx, int my, int h, int w, const float* inv, float* in,
+                cudaStream_t s);
+void apply_correction(const float* out, const double* prev, int mx, int my, int w, const float* inv, double* x,
+                      cudaStream_t s);
+void make_target(const double* x, const double* prev, const double* b, int mx, int my, int h, int w,
+                 const float* inv, float* target, double* sums, cudaStream_t s);
 
 struct ConvLayer {
   int cin, cout;           // channels

@@ -19,7 +19,7 @@ constexpr int kSmoothThreads = 256;
 constexpr int kSmallThreads = 1024;
 
 // state words (FP64): see multigrid.hpp
-enum { S_SUM = 0, S_SUM2, S_NORMB, S_REL, S_DONE, S_ITER, S_MEAN, S_COUNT };
+enum { S_SUM = 0, S_SUM2, S_NORMB, S_REL, S_DONE, S_ITER, S_MEAN, S_REL0, S_COUNT };
 
 // Boundary treatment of a direction: Dirichlet (values outside are zero),
 // periodic (wrap) or Neumann (mirror about the end node, i.e. the doubled
@@ -204,6 +204,7 @@ __global__ void k_check(double* st, double tol, int maxiter, double wsum) {
   if (st[S_DONE] != 0.0) return;
   const double rel = sqrt(st[S_SUM2] > 0 ? st[S_SUM2] : 0.0) / st[S_NORMB];
   st[S_REL] = rel;
+  if (st[S_ITER] == 0.0) st[S_REL0] = rel;
   if (!(rel > tol) || st[S_ITER] >= double(maxiter)) {
     st[S_DONE] = 1.0;
   } else {
@@ -834,6 +835,7 @@ MGResult PoissonMG::solve(const double* b, const double* sums_b, double* x, doub
   }
   res.norm_b = host_[S_NORMB];
   res.rel_residual = host_[S_REL];
+  res.rel0 = host_[S_REL0];
   res.iterations = int(host_[S_ITER]);
   if (host_[S_DONE] == 2.0) {
     res.iterations = 0;

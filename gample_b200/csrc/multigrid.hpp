@@ -40,6 +40,7 @@ namespace gample {
 struct MGResult {
   int iterations = 0;        // V-cycles performed
   double rel_residual = 0;   // ||b - A x|| / ||b|| in FP64
+  double rel0 = 0;           // the same for the starting guess
   double norm_b = 0;
 };
 
@@ -79,7 +80,7 @@ class PoissonMG {
   std::vector<Level> lv_;
   DeviceArray<double> x2_;      // ping-pong buffer of the FP64 update
   DeviceArray<float> coarse_inv_;  // dense inverse of the coarsest operator (small coarsest levels)
-  DeviceArray<double> state_;   // [0] sum r [1] sum r^2 [2] ||b|| [3] rel res [4] done [5] iterations [6] mean r
+  DeviceArray<double> state_;   // [0] sum r [1] sum r^2 [2] ||b|| [3] rel res [4] done [5] iterations [6] mean r [7] initial rel res
   PinnedArray<double> host_;
 };
 

@@ -21,6 +21,7 @@
 #include "device.hpp"
 #include "init.hpp"
 #include "kernels.hpp"
+#include "learned.hpp"
 #include "multigrid.hpp"
 
 namespace gample {
@@ -75,6 +76,22 @@ class EMField {
   SolveStats solvePoisson(double dt, XmlLogger* logger);   // src/EMField.mm:745-1136
   // Combine the fixed-point accumulators (deterministic mode) into rho/jx/jy.
   void finalizeCharge();
+  // Learned warm start of the Poisson solve (build addition). mode bits:
+  // 1 start the multigrid from previous phi + the network's correction,
+  // 2 train the network on (rhs, previous phi) -> (phi - previous phi) after
+  // each solve, 4 also solve from the plain warm start for comparison.
+  struct LearnedStats {
+    double loss = 0;
+    int iters_learned = 0, iters_plain = 0;
+    double ms_learned = 0, ms_plain = 0, ms_net = 0;  // solve + network / plain solve / network alone
+    double rel0_learned = 0, rel0_plain = 0;          // relative residual of the starting guess
+    int trained_steps = 0;
+  };
+  void setLearned(int mode, float lr, uint64_t seed);
+  int learned_mode = 0;
+  float learned_lr = 1e-3f;
+  std::unique_ptr<nn::WarmStartNet> net;
+  LearnedStats last_learned;
   // src/EMField.mm:1138-1361 (Darwin model, FlagForEquation.EMField == 2):
   // Helmholtz split of J, vector potential, delEx/delEy/delBz.
   struct DarwinStats {
@@ -125,6 +142,11 @@ class EMField {
 
  private:
   PinnedArray<double> host_diag_;
+  MGResult poissonSolve(double* d);  // plain or learned warm start
+  DeviceArray<float> nn_in_, nn_out_, nn_target_, nn_inv_;
+  DeviceArray<double> sol_prev_, sol_cmp_, nn_sums_;
+  float h_inv_[3] = {0, 0, 0};
+  int nn_h_ = 0, nn_w_ = 0;
   void load1dField(const std::string& path, std::vector<float>& out, size_t need) const;  // :658-687
 };
 

@@ -277,7 +277,7 @@ SolveStats EMField::solvePoisson(double dt, XmlLogger* logger) {
     kern::subtract_mean(b.get(), n, d, stream);
     kern::vec_sums(b.get(), n, d, stream);
   }
-  last_mg = mg->solve(b.get(), d, sol.get(), tol, maxiter, stream);
+  last_mg = poissonSolve(d);
   kern::phi_fill(sol.get(), dims, layout, dx, cathodePos, d + 4, phi.get(), stream);
   kern::gradient_energy(phi.get(), dims, dx, dy, Ex.get(), Ey.get(), jx.get(), jy.get(), d + 2, stream);
   kern::probe(phi.get(), Ex.get(), Ey.get(), dims, d + 5, stream);

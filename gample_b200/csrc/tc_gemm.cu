@@ -14,6 +14,7 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <stdexcept>
 
 #include "device.hpp"
@@ -78,6 +79,9 @@ __global__ void __launch_bounds__(kThreads) k_gemm(const __nv_bfloat16* __restri
   __shared__ uint32_t tbase;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
+  // split K over blockIdx.z (chunks of whole BK steps)
+  const int ksteps = K / BK, per = (ksteps + gridDim.z - 1) / gridDim.z;
+  const int kbeg = blockIdx.z * per * BK, kend = min(K, (int(blockIdx.z) + 1) * per * BK);
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(su32(&tbase)), "r"(BN)
                  : "memory");
@@ -94,7 +98,7 @@ __global__ void __launch_bounds__(kThreads) k_gemm(const __nv_bfloat16* __restri
   const uint32_t aaddr = su32(sA), baddr = su32(sB);
   uint32_t phase = 0;
   bool ok = true;
-  for (int k0 = 0; k0 < K && ok; k0 += BK) {
+  for (int k0 = kbeg; k0 < kend && ok; k0 += BK) {
     for (int c = tid; c < BM * (BK / 8); c += kThreads) {
       const int m = c / (BK / 8), kc = c % (BK / 8);
       const uint4 v = *reinterpret_cast<const uint4*>(A + size_t(m0 + m) * K + k0 + kc * 8);
@@ -113,7 +117,7 @@ __global__ void __launch_bounds__(kThreads) k_gemm(const __nv_bfloat16* __restri
       for (int ks = 0; ks < BK / 16; ++ks) {
         const uint64_t da = sdesc(aaddr + ks * 2 * (BM / 8) * 128, (BM / 8) * 128, 128);
         const uint64_t db = sdesc(baddr + ks * 2 * (BN / 8) * 128, (BN / 8) * 128, 128);
-        const uint32_t acc = (k0 > 0 || ks > 0) ? 1u : 0u;
+        const uint32_t acc = (k0 > kbeg || ks > 0) ? 1u : 0u;
         asm volatile(
             "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\ttcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(
                 tmem),
@@ -130,7 +134,7 @@ __global__ void __launch_bounds__(kThreads) k_gemm(const __nv_bfloat16* __restri
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   if (!ok) {
     if (tid == 0) atomicExch(err, 1);
-  } else {
+  } else if (kbeg < kend) {
     const int row = m0 + warp * 32 + lane;
 #pragma unroll 1
     for (int c0 = 0; c0 < BN; c0 += 16) {
@@ -142,6 +146,10 @@ __global__ void __launch_bounds__(kThreads) k_gemm(const __nv_bfloat16* __restri
         const int n = n0 + c0 + j;
         if (n >= ep.n_valid) continue;
         float v = __uint_as_float(r[j]) * ep.alpha;
+        if (gridDim.z > 1) {  // split K: partial sums added atomically (output zeroed by the caller)
+          atomicAdd(ep.out_f32 + size_t(row) * ep.ldo + n, v);
+          continue;
+        }
         if (ep.bias) v += ep.bias[n];
         if (ep.relu) v = fmaxf(v, 0.0f);
         if (ep.out_f32) {
@@ -160,7 +168,24 @@ __global__ void __launch_bounds__(kThreads) k_gemm(const __nv_bfloat16* __restri
 template <int BN>
 void launch_bn(const __nv_bfloat16* A, const __nv_bfloat16* B, int M, int N, int K, const GemmEpilogue& ep, int* err,
                cudaStream_t s) {
-  dim3 grid(N / BN, M / BM);
+  // split K when the output has few tiles and K is long (weight gradients)
+  const int tiles = (N / BN) * (M / BM);
+  const int ksteps = K / (K % 64 == 0 ? 64 : 32);
+  int splits = 1;
+  if (ep.split_k && tiles < 296 && ksteps >= 16) {
+    splits = std::min(296 / tiles, ksteps / 8);
+    if (splits < 1) splits = 1;
+  }
+  if (splits > 1) {
+    if (!ep.out_f32 || ep.bias || ep.relu || ep.out_bf16 || ep.accumulate)
+      throw std::invalid_argument("gemm_bf16: split K needs a plain FP32 output");
+    if (ep.ldo == ep.n_valid)
+      GP_CUDA(cudaMemsetAsync(ep.out_f32, 0, size_t(ep.m_valid) * ep.ldo * sizeof(float), s));
+    else
+      for (int r = 0; r < ep.m_valid; ++r)
+        GP_CUDA(cudaMemsetAsync(ep.out_f32 + size_t(r) * ep.ldo, 0, size_t(ep.n_valid) * sizeof(float), s));
+  }
+  dim3 grid(N / BN, M / BM, splits);
   if (K % 64 == 0)
     k_gemm<BN, 64><<<grid, kThreads, 0, s>>>(A, B, M, N, K, ep, err);
   else

@@ -204,6 +204,15 @@ gp_status gp_deposit_charge_noalloc(int weighting_order, int ngx, int ngy, const
  * reference counterpart): a 4-level convolutional encoder-decoder (3x3,
  * 32/64/128/256 channels, BF16 on the tensor cores). Host buffers: in is
  * [h][w][2] (normalised rhs, previous phi), out/target [h][w]. ---- */
+/* Attach the network to a run's Poisson solve. mode bits: 1 start the
+ * multigrid from previous phi + network correction, 2 train after each solve
+ * on (rhs, previous phi) -> (phi - previous phi), 4 also time a solve from the
+ * plain warm start; the multigrid always reaches ToleranceForPoisson. */
+gp_status gp_field_learned(gp_sim* sim, int mode, float lr, uint64_t seed);
+/* last solve: loss, V-cycles (learned, plain), ms (learned incl. network,
+ * plain, network alone), starting relative residual (learned, plain),
+ * training steps so far */
+gp_status gp_field_learned_stats(gp_sim* sim, double out[9]);
 gp_status gp_nn_create(int h, int w, uint64_t seed, gp_nn** out);
 void gp_nn_free(gp_nn* nn);
 gp_status gp_nn_forward(gp_nn* nn, const float* in, float* out);
