@@ -94,6 +94,11 @@ EXPORTS = {
     "gp_sim_load_progress": (C.c_int, [C.c_void_p, C.c_int]),
     "gp_field_learned": (C.c_int, [C.c_void_p, C.c_int, C.c_float, C.c_uint64]),
     "gp_field_learned_stats": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "gp_ensemble_create": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
+    "gp_ensemble_free": (None, [C.c_void_p]),
+    "gp_ensemble_initialize": (C.c_int, [C.c_void_p]),
+    "gp_ensemble_run": (C.c_int, [C.c_void_p, C.c_int]),
+    "gp_ensemble_member": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_void_p)]),
     "gp_nn_create": (C.c_int, [C.c_int, C.c_int, C.c_uint64, C.POINTER(C.c_void_p)]),
     "gp_nn_free": (None, [C.c_void_p]),
     "gp_nn_forward": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
@@ -398,3 +403,51 @@ class Net:
     def set_param(self, layer, which, a):
         a = np.ascontiguousarray(a, np.float32).ravel()
         check(lib().gp_nn_param(self.p, layer, which, a.ctypes.data, a.size, 1))
+
+
+class Ensemble:
+    """Independent runs advanced together (gp_ensemble_*); member(i) gives a Sim view."""
+
+    def __init__(self, conds, threads=8):
+        self.inits = [c if isinstance(c, Init) else Init(c) for c in conds]
+        arr = (C.c_void_p * len(self.inits))(*[i.h.value if isinstance(i.h, C.c_void_p) else i.h
+                                               for i in self.inits])
+        p = C.c_void_p()
+        check(lib().gp_ensemble_create(arr, len(self.inits), threads, C.byref(p)))
+        self.p = p
+        self.members = []
+        for k in range(len(self.inits)):
+            h = C.c_void_p()
+            check(lib().gp_ensemble_member(self.p, k, C.byref(h)))
+            self.members.append(SimView(self.inits[k], h))
+
+    def initialize(self):
+        check(lib().gp_ensemble_initialize(self.p))
+
+    def run(self, n):
+        check(lib().gp_ensemble_run(self.p, n))
+
+    def close(self):
+        if getattr(self, "p", None):
+            for m in self.members:
+                m.h = None
+            lib().gp_ensemble_free(self.p)
+            self.p = None
+
+    def __del__(self):
+        self.close()
+
+
+class SimView(Sim):
+    """A member of an Ensemble (not owned: freeing is the ensemble's)."""
+
+    def __init__(self, init, handle):
+        self.init = init
+        self.h = handle
+        d = [C.c_int() for _ in range(5)]
+        check(lib().gp_field_dims(self.h, *[C.byref(x) for x in d]))
+        self.ngx, self.ngy, self.ngb, self.nkx, self.nky = [x.value for x in d]
+        self.nx, self.ny = self.ngx + 2 * self.ngb, self.ngy + 2 * self.ngb
+
+    def close(self):
+        self.h = None

@@ -4,6 +4,7 @@
 #include <string>
 
 #include "../../include/gample_gpu.h"
+#include "ensemble.hpp"
 #include "fileio.hpp"
 #include "learned.hpp"
 #include "simulation.hpp"
@@ -23,6 +24,12 @@ struct gp_init {
 };
 struct gp_sim {
   std::unique_ptr<gample::Simulation> sim;
+  gample::Simulation* view = nullptr;  // member of an ensemble (not owned)
+  gample::Simulation* get() const { return view ? view : sim.get(); }
+};
+struct gp_ensemble {
+  std::unique_ptr<gample::Ensemble> ens;
+  std::vector<gp_sim> views;
 };
 struct gp_nn {
   std::unique_ptr<gample::nn::WarmStartNet> net;
@@ -64,17 +71,17 @@ gp_status guarded(F&& f) {
 }
 
 gample::Particle* species(gp_sim* sim, int s) {
-  if (!sim || !sim->sim) throw std::invalid_argument("null simulation handle");
-  if (s < 0 || s >= int(sim->sim->ptrs.size())) throw std::invalid_argument("species index out of range");
-  return sim->sim->ptrs[s];
+  if (!sim || !sim->get()) throw std::invalid_argument("null simulation handle");
+  if (s < 0 || s >= int(sim->get()->ptrs.size())) throw std::invalid_argument("species index out of range");
+  return sim->get()->ptrs[s];
 }
 gample::Simulation& S(gp_sim* sim) {
-  if (!sim || !sim->sim) throw std::invalid_argument("null simulation handle");
-  return *sim->sim;
+  if (!sim || !sim->get()) throw std::invalid_argument("null simulation handle");
+  return *sim->get();
 }
 const gample::Simulation& S(const gp_sim* sim) {
-  if (!sim || !sim->sim) throw std::invalid_argument("null simulation handle");
-  return *sim->sim;
+  if (!sim || !sim->get()) throw std::invalid_argument("null simulation handle");
+  return *sim->get();
 }
 
 void fill(gp_solve_stats* out, const gample::SolveStats& st) {
@@ -296,9 +303,56 @@ gp_status gp_sim_create(const gp_init* init, const char* log_name, int flags, gp
 }
 void gp_sim_free(gp_sim* sim) {
   try {
+    if (sim && sim->view) return;  // ensemble members are freed with their ensemble
     delete sim;
   } catch (...) {
   }
+}
+
+gp_status gp_ensemble_create(const gp_init* const* inits, int n, int threads, gp_ensemble** out) {
+  return guarded([&] {
+    if (!inits || n <= 0 || !out) throw std::invalid_argument("null or empty ensemble description");
+    std::vector<gample::Init> v;
+    for (int i = 0; i < n; ++i) {
+      if (!inits[i]) throw std::invalid_argument("null condition in the ensemble");
+      v.push_back(inits[i]->init);
+    }
+    auto e = std::make_unique<gp_ensemble>();
+    e->ens = std::make_unique<gample::Ensemble>(v, threads);
+    e->views.resize(size_t(n));
+    for (int i = 0; i < n; ++i) e->views[i].view = e->ens->members[i].get();
+    *out = e.release();
+    return GP_OK;
+  });
+}
+void gp_ensemble_free(gp_ensemble* e) {
+  try {
+    delete e;
+  } catch (...) {
+  }
+}
+gp_status gp_ensemble_initialize(gp_ensemble* e) {
+  return guarded([&] {
+    if (!e || !e->ens) throw std::invalid_argument("null ensemble handle");
+    e->ens->initialize();
+    return GP_OK;
+  });
+}
+gp_status gp_ensemble_run(gp_ensemble* e, int ncycles) {
+  return guarded([&] {
+    if (!e || !e->ens) throw std::invalid_argument("null ensemble handle");
+    if (ncycles < 0) throw std::invalid_argument("negative cycle count");
+    e->ens->run(ncycles);
+    return GP_OK;
+  });
+}
+gp_status gp_ensemble_member(gp_ensemble* e, int i, gp_sim** out) {
+  return guarded([&] {
+    if (!e || !e->ens || !out) throw std::invalid_argument("null argument");
+    if (i < 0 || i >= int(e->views.size())) throw std::invalid_argument("member index out of range");
+    *out = &e->views[size_t(i)];
+    return GP_OK;
+  });
 }
 gp_status gp_sim_initialize(gp_sim* sim) {
   return guarded([&] {

@@ -1,0 +1,31 @@
+// ensemble.hpp -- many independent runs advanced together on one GPU.
+//
+// Every member is a full Simulation with its own CUDA stream; a pool of host
+// threads drives them concurrently, so the kernels of different members
+// overlap on the GPU and the host synchronisation points of one member
+// (diagnostics, counter reads) do not stall the others. Members share no
+// state: each one's results equal the same run alone.
+#pragma once
+
+#include <memory>
+#include <vector>
+
+#include "simulation.hpp"
+
+namespace gample {
+
+class Ensemble {
+ public:
+  Ensemble(const std::vector<Init>& inits, int threads);
+  void initialize();
+  void run(int ncycles);
+  size_t size() const { return members.size(); }
+  std::vector<std::unique_ptr<Simulation>> members;
+
+ private:
+  template <typename F>
+  void parallel(F&& f);
+  int threads_ = 1;
+};
+
+}  // namespace gample

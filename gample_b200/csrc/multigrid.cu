@@ -3,6 +3,7 @@
 
 #include <algorithm>
 #include <cfloat>
+#include <mutex>
 #include <cmath>
 #include <stdexcept>
 
@@ -667,9 +668,17 @@ PoissonMG::PoissonMG(const kern::PoissonLayout& L, int nu_pre, int nu_post)
   int dev = 0, maxsm = 0;
   GP_CUDA(cudaGetDevice(&dev));
   GP_CUDA(cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-  if (small_smem_ + 1024 > size_t(maxsm))
+  if (small_smem_ + 2048 > size_t(maxsm))
     throw std::invalid_argument("coarsest multigrid level too large (grid dimensions do not coarsen)");
-  GP_CUDA(cudaFuncSetAttribute(k_small_vcycle, cudaFuncAttributeMaxDynamicSharedMemorySize, int(small_smem_)));
+  // The attribute is per function and shared by every solver in the process
+  // (ensemble members run concurrently): allow the device's maximum once.
+  static std::once_flag once;
+  std::call_once(once, [maxsm] {
+    cudaFuncAttributes fa{};
+    GP_CUDA(cudaFuncGetAttributes(&fa, k_small_vcycle));
+    GP_CUDA(cudaFuncSetAttribute(k_small_vcycle, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 maxsm - int(fa.sharedSizeBytes)));
+  });
   x2_.resize(size_t(n_), true);
   // Dense inverse of the coarsest operator (FP64 Gauss-Jordan, stored FP32);
   // a singular one (no Dirichlet direction) is regularised as A + a 1 w^T

@@ -19,6 +19,7 @@
 
 #include <climits>
 #include <cstdio>
+#include <mutex>
 
 #include "device.hpp"
 #include "kernels.hpp"
@@ -658,11 +659,8 @@ void launch_pic(uint32_t nblocks, cudaStream_t s, GridDims g, ParticleArrays p, 
                 DepositTargets d, SpeciesCounters* cnt, uint32_t* bits, int injected_only) {
   auto kern = k_pic<ORDER, PUSH, DEP, DET, CUR, BZU>;
   constexpr size_t bytes = smem_bytes<ORDER, PUSH, DEP, DET, CUR, BZU>();
-  static bool configured = false;
-  if (!configured) {
-    GP_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)));
-    configured = true;
-  }
+  static std::once_flag once;  // shared by concurrent runs (ensembles)
+  std::call_once(once, [&] { GP_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes))); });
   kern<<<nblocks, kThreads, bytes, s>>>(g, p, f, c, boris, d, cnt, bits, injected_only);
 }
 

@@ -33,6 +33,7 @@ typedef int gp_status;
 typedef struct gp_init gp_init; /* parsed condition (src/Init.h:101-118) */
 typedef struct gp_sim gp_sim;   /* Particle[], EMField, Collision, XmlLogger of one run */
 typedef struct gp_nn gp_nn;     /* learned warm-start network (build addition) */
+typedef struct gp_ensemble gp_ensemble; /* independent runs advanced together (build addition) */
 
 /* Particle record of the reference (src/Particle.h:14-21): x, y in grid units
  * offset by ngb, velocities in cm/s, piflag 0 = live, 1..4 = left through
@@ -224,6 +225,18 @@ gp_status gp_nn_layer_info(gp_nn* nn, int layer, int* cin, int* cout, int* kpad)
 /* which: 0 weights [cout][kpad], 1 bias [cout], 2 weight gradient, 3 bias
  * gradient (FP32); set != 0 writes 0/1 */
 gp_status gp_nn_param(gp_nn* nn, int layer, int which, float* host, size_t count, int set);
+
+/* ---- ensemble of independent runs (build addition; no reference
+ * counterpart): each member is a full run with its own CUDA stream, driven by
+ * a pool of host threads so that members overlap on the GPU; results equal
+ * each run alone. ---- */
+gp_status gp_ensemble_create(const gp_init* const* inits, int n, int threads, gp_ensemble** out);
+void gp_ensemble_free(gp_ensemble* e);
+gp_status gp_ensemble_initialize(gp_ensemble* e);
+gp_status gp_ensemble_run(gp_ensemble* e, int ncycles);
+/* a view of member i for the gp_sim_* / gp_particle_* / gp_field_* calls
+ * (owned by the ensemble; gp_sim_free on it does nothing) */
+gp_status gp_ensemble_member(gp_ensemble* e, int i, gp_sim** out);
 
 /* ---- misc ---- */
 const char* gp_last_error(void);
