@@ -213,6 +213,49 @@ def learned_leg(cond, train_steps, eval_steps):
                     "the multigrid always reaches 1e-8 from either start"}
 
 
+def ensemble_leg(members, steps, threads, seed=0):
+    """Config-5 style batch: independent runs with grids from {64..512}^2,
+    orders {1, 3, 5}, Bz in [0, 0.05] T and 16..64 particles per cell per
+    species, advanced together (one stream per member, host thread pool) and,
+    for comparison, one after the other."""
+    import random
+    from gample_b200 import capi
+    rnd = random.Random(seed)
+    conds = []
+    for _ in range(members):
+        n = rnd.choice([64, 128, 256, 512])
+        c = workload(ppc=rnd.randint(16, 64), ngx=n, ngy=n, steps=steps)
+        c["ParamForField"]["WeightingOrder"] = rnd.choice([1, 3, 5])
+        c["ParamForField"]["AmplitudeOfB"] = [0.0, 0.0, rnd.uniform(0.0, 0.05) * 1e4]
+        conds.append(c)
+    ens = capi.Ensemble(conds, threads=threads)
+    ens.initialize()
+    ens.run(2)
+    n0 = sum(m.count(0) + m.count(1) for m in ens.members)
+    t0 = time.perf_counter()
+    ens.run(steps)
+    el = time.perf_counter() - t0
+    n1 = sum(m.count(0) + m.count(1) for m in ens.members)
+    ens.close()
+    del ens
+    batched = 0.5 * (n0 + n1) * steps / el
+    seq_el, seq_n = 0.0, 0.0
+    for c in conds:
+        sim = capi.Sim(c)
+        sim.initialize()
+        sim.run(2)
+        a = sim.count(0) + sim.count(1)
+        t0 = time.perf_counter()
+        sim.run(steps)
+        seq_el += time.perf_counter() - t0
+        seq_n += 0.5 * (a + sim.count(0) + sim.count(1)) * steps
+        sim.close()
+    sequential = seq_n / seq_el
+    return {"members": members, "threads": threads, "steps": steps, "particles": n1,
+            "pushes_per_s": batched, "sequential_pushes_per_s": sequential, "speedup": batched / sequential,
+            "wall_s": el, "timing": "host wall clock around the batched run (all members synchronised)"}
+
+
 def dist_setup():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -312,6 +355,7 @@ def run_b200(args):
         t = torch.tensor([ms], device="cuda", dtype=torch.float64)
         pg.all_reduce(t, op=pg.ReduceOp.MAX)
         ms_max = float(t.item())
+    iters_last = sim.last_solve().iterations
     pushes_rank = 0.5 * (n0 + n1) * args.steps
     value = pushes_rank * world / (ms_max / 1e3)
 
@@ -382,6 +426,9 @@ def run_b200(args):
                "h2d_bytes_per_step": int(h2d / args.steps), "d2h_bytes_per_step": int(d2h / args.steps + diag),
                "wall_s": el, "includes": "sim create + restart upload + initial solve + K logged cycles + "
                                          "final download"}
+    ensemble = None
+    if rank == 0 and args.ensemble > 0:
+        ensemble = ensemble_leg(args.ensemble, args.ensemble_steps, args.ensemble_threads)
     learned = None
     if rank == 0 and args.learned_train > 0:
         learned = learned_leg(cond, args.learned_train, args.learned_eval)
@@ -400,7 +447,8 @@ def run_b200(args):
                 "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
                 "gpu_launches": launches, "gpu_launches_per_step": launches / args.steps,
-                "poisson": {"iterations_last_step": None}, "learned_warm_start": learned}
+                "poisson": {"vcycles_last_step": iters_last, "tolerance": 1e-8}, "learned_warm_start": learned,
+                "ensemble": ensemble}
         print(json.dumps(line), flush=True)
     if pg:
         pg.barrier()
@@ -421,6 +469,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--learned-train", type=int, default=100, help="online training steps of the warm-start network")
     ap.add_argument("--learned-eval", type=int, default=20)
+    ap.add_argument("--ensemble", type=int, default=64, help="members of the batched-ensemble leg (0: skip)")
+    ap.add_argument("--ensemble-steps", type=int, default=10)
+    ap.add_argument("--ensemble-threads", type=int, default=16)
     ap.add_argument("--quick", action="store_true", help="timed cycles only (for profiler runs)")
     args = ap.parse_args()
     if args.impl == "reference":
