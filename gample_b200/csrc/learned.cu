@@ -37,6 +37,23 @@ __global__ void k_im2col(const __nv_bfloat16* x, int h, int w, int c, int kpad, 
   }
 }
 
+// The same with 16-byte chunks of 8 channels (C a multiple of 8).
+__global__ void k_im2col8(const __nv_bfloat16* x, int h, int w, int c, int kpad, int rows, __nv_bfloat16* col) {
+  const int kc = kpad / 8;
+  const size_t n = size_t(rows) * kc;
+  for (size_t e = blockIdx.x * size_t(blockDim.x) + threadIdx.x; e < n; e += size_t(gridDim.x) * blockDim.x) {
+    const int p = int(e / kc), k = int(e % kc) * 8;
+    uint4 v = make_uint4(0, 0, 0, 0);
+    if (p < h * w && k < 9 * c) {
+      const int t = k / c, ch = k - t * c;
+      const int yy = p / w + t / 3 - 1, xx = p % w + t % 3 - 1;
+      if (yy >= 0 && yy < h && xx >= 0 && xx < w)
+        v = *reinterpret_cast<const uint4*>(x + (size_t(yy) * w + xx) * c + ch);
+    }
+    *reinterpret_cast<uint4*>(col + size_t(p) * kpad + k) = v;
+  }
+}
+
 // dX[q][c] += sum over taps t of dXcol[q - offset(t)][t * C + c]
 __global__ void k_col2im_add(const float* gcol, int h, int w, int c, int kpad, float* gx) {
   const size_t n = size_t(h) * w * c;
@@ -273,8 +290,16 @@ double WarmStartNet::flops_forward() const {
 
 void WarmStartNet::conv_forward(ConvLayer& L, const Act& x, Act& y, float* out_f32) {
   const int hw = x.h * x.w, rows = rup(hw, 128);
-  k_im2col<<<grid_for(size_t(rows) * L.kpad), kT, 0, stream>>>(x.y.get(), x.h, x.w, x.c, L.kpad, rows, col_.get());
-  GP_LAUNCH_CHECK();
+  // implicit im2col inside the GEMM when each K step stays in one tap
+  ConvA conv;
+  if (L.kpad == 9 * L.cin && L.cin % 32 == 0) {
+    conv.x = x.y.get();
+    conv.h = x.h;
+    conv.w = x.w;
+    conv.cin = x.c;
+  } else {
+    im2col(x, L.kpad, rows);
+  }
   GemmEpilogue ep;
   ep.bias = L.b.get();
   ep.relu = L.relu ? 1 : 0;
@@ -285,7 +310,17 @@ void WarmStartNet::conv_forward(ConvLayer& L, const Act& x, Act& y, float* out_f
     ep.out_f32 = out_f32;
   else
     ep.out_bf16 = y.y.get();
-  gemm_bf16(col_.get(), L.wb.get(), rows, L.cout_p, L.kpad, ep, err_.get(), stream);
+  gemm_bf16(col_.get(), L.wb.get(), rows, L.cout_p, L.kpad, ep, err_.get(), stream, conv);
+}
+
+void WarmStartNet::im2col(const Act& x, int kpad, int rows) {
+  if (x.c % 8 == 0) {
+    const size_t chunks = size_t(rows) * (kpad / 8);
+    k_im2col8<<<grid_for(chunks), kT, 0, stream>>>(x.y.get(), x.h, x.w, x.c, kpad, rows, col_.get());
+  } else {
+    k_im2col<<<grid_for(size_t(rows) * kpad), kT, 0, stream>>>(x.y.get(), x.h, x.w, x.c, kpad, rows, col_.get());
+  }
+  GP_LAUNCH_CHECK();
 }
 
 void WarmStartNet::conv_backward(ConvLayer& L, const Act& x, Act& y, Act* dx, const float* gy_override) {
@@ -298,8 +333,7 @@ void WarmStartNet::conv_backward(ConvLayer& L, const Act& x, Act& y, Act* dx, co
   GP_LAUNCH_CHECK();
   // weight gradient: gw [cout][kpad] = gy^T [cout_pm x rows] * col^T [kpad x rows]^T
   const int cout_pm = rup(L.cout_p, 128);
-  k_im2col<<<grid_for(size_t(rows) * L.kpad), kT, 0, stream>>>(x.y.get(), x.h, x.w, x.c, L.kpad, rows, col_.get());
-  GP_LAUNCH_CHECK();
+  im2col(x, L.kpad, rows);
   {
     dim3 b(32, 8);
     dim3 g1((L.cout_p + 31) / 32, (rows + 31) / 32);

@@ -37,11 +37,19 @@ struct GemmEpilogue {
   int split_k = 0;  // allow splitting K over CTAs (plain FP32 output, zeroed and accumulated atomically)
 };
 
+// Implicit im2col for A: row m = pixel m of an h x w NHWC tensor x with cin
+// channels, column k = tap * cin + channel of the 3 x 3 neighbourhood (zero
+// outside the grid). Needs K = 9 cin and cin a multiple of the K step.
+struct ConvA {
+  const __nv_bfloat16* x = nullptr;
+  int h = 0, w = 0, cin = 0;
+};
+
 // C = A[M x K] * B[N x K]^T on the tensor cores (both K-major BF16); M a
 // multiple of 128, N of 32, K of 32. err: device int set to 1 if an MMA
 // completion wait timed out.
 void gemm_bf16(const __nv_bfloat16* A, const __nv_bfloat16* B, int M, int N, int K, const GemmEpilogue& ep, int* err,
-               cudaStream_t s);
+               cudaStream_t s, const ConvA& conv = ConvA{});
 
 // Unknown grid <-> network tensors (inv: device floats 1/RMS of the rhs, of
 // phi and of the correction).
@@ -92,6 +100,7 @@ class WarmStartNet {
   };
   void conv_forward(ConvLayer& L, const Act& x, Act& y, float* out_f32 = nullptr);
   void conv_backward(ConvLayer& L, const Act& x, Act& y, Act* dx, const float* gy_override = nullptr);
+  void im2col(const Act& x, int kpad, int rows);  // into col_
   int h_, w_;
   std::vector<ConvLayer> layers_;
   std::vector<Act> acts_;

@@ -3,8 +3,8 @@
 // contiguous), FP32 accumulation in tensor memory.
 //
 // One CTA (128 threads) per 128 x BN tile. Per K step of BK elements the
-// threads stage A and B in shared memory in the canonical no-swizzle
-// K-major layout (8-row x 16-byte core matrices; leading byte offset
+// threads stage A and B in one of two shared-memory stages in the canonical
+// no-swizzle K-major layout (8-row x 16-byte core matrices; leading byte offset
 // between the two K halves of an MMA, stride byte offset between 8-row
 // groups), one elected thread issues BK/16 tcgen05.mma (M=128, N=BN, K=16)
 // into a BN-column TMEM accumulator and commits to an mbarrier; every wait
@@ -15,6 +15,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <mutex>
 #include <stdexcept>
 
 #include "device.hpp"
@@ -67,15 +68,22 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
+// Two shared-memory stages: while the tensor core works on stage s, the
+// threads load the next K step into stage s^1 (after the MMAs that last read
+// it have completed, per-stage mbarrier).
+template <int BN, int BK>
+__host__ __device__ constexpr int stage_bytes() {
+  return (BM + BN) * BK * 2;
+}
+
 template <int BN, int BK>
 __global__ void __launch_bounds__(kThreads) k_gemm(const __nv_bfloat16* __restrict__ A,
                                                    const __nv_bfloat16* __restrict__ B, int M, int N, int K,
-                                                   GemmEpilogue ep, int* err) {
+                                                   GemmEpilogue ep, int* err, ConvA conv) {
   static_assert(BN == 32 || BN == 64 || BN == 128, "BN");
   static_assert(BK == 32 || BK == 64, "BK");
-  __shared__ __align__(128) __nv_bfloat16 sA[BM * BK];
-  __shared__ __align__(128) __nv_bfloat16 sB[BN * BK];
-  __shared__ __align__(8) uint64_t mbar;
+  extern __shared__ __align__(128) unsigned char gsm[];
+  __shared__ __align__(8) uint64_t mbar[2];
   __shared__ uint32_t tbase;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
@@ -88,31 +96,61 @@ __global__ void __launch_bounds__(kThreads) k_gemm(const __nv_bfloat16* __restri
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
   if (tid == 0) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(su32(&mbar)) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(su32(&mbar[0])) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(su32(&mbar[1])) : "memory");
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = tbase;
-  const uint32_t aaddr = su32(sA), baddr = su32(sB);
-  uint32_t phase = 0;
+  const uint32_t base = su32(gsm);
+  uint32_t phase[2] = {0, 0};
+  int used[2] = {0, 0};  // MMA batches committed per stage and not yet waited for
   bool ok = true;
-  for (int k0 = kbeg; k0 < kend && ok; k0 += BK) {
-    for (int c = tid; c < BM * (BK / 8); c += kThreads) {
-      const int m = c / (BK / 8), kc = c % (BK / 8);
-      const uint4 v = *reinterpret_cast<const uint4*>(A + size_t(m0 + m) * K + k0 + kc * 8);
-      *reinterpret_cast<uint4*>(reinterpret_cast<char*>(sA) + kc * (BM / 8) * 128 + (m / 8) * 128 + (m % 8) * 16) = v;
+  int t = 0;
+  for (int k0 = kbeg; k0 < kend && ok; k0 += BK, ++t) {
+    const int st = t & 1;
+    if (used[st]) {  // the MMAs of two steps ago read this stage
+      ok = mbar_wait(&mbar[st], phase[st]);
+      phase[st] ^= 1;
+      used[st] = 0;
+      if (!ok) break;
+    }
+    unsigned char* sA = gsm + st * stage_bytes<BN, BK>();
+    unsigned char* sB = sA + BM * BK * 2;
+    if (conv.x) {  // implicit im2col: this K step lies in one tap of the 3 x 3 stencil
+      const int tap = k0 / conv.cin, c0 = k0 - tap * conv.cin;
+      const int dy = tap / 3 - 1, dx = tap % 3 - 1, hw = conv.h * conv.w;
+      for (int c = tid; c < BM * (BK / 8); c += kThreads) {
+        const int m = c / (BK / 8), kc = c % (BK / 8);
+        const int p = m0 + m;
+        uint4 v = make_uint4(0, 0, 0, 0);
+        if (p < hw) {
+          const int py = p / conv.w, px = p - py * conv.w;
+          const int sy = py + dy, sx = px + dx;
+          if (sy >= 0 && sy < conv.h && sx >= 0 && sx < conv.w)
+            v = *reinterpret_cast<const uint4*>(conv.x + (size_t(sy) * conv.w + sx) * conv.cin + c0 + kc * 8);
+        }
+        *reinterpret_cast<uint4*>(sA + kc * (BM / 8) * 128 + (m / 8) * 128 + (m % 8) * 16) = v;
+      }
+    } else {
+      for (int c = tid; c < BM * (BK / 8); c += kThreads) {
+        const int m = c / (BK / 8), kc = c % (BK / 8);
+        const uint4 v = *reinterpret_cast<const uint4*>(A + size_t(m0 + m) * K + k0 + kc * 8);
+        *reinterpret_cast<uint4*>(sA + kc * (BM / 8) * 128 + (m / 8) * 128 + (m % 8) * 16) = v;
+      }
     }
     for (int c = tid; c < BN * (BK / 8); c += kThreads) {
       const int n = c / (BK / 8), kc = c % (BK / 8);
       const uint4 v = *reinterpret_cast<const uint4*>(B + size_t(n0 + n) * K + k0 + kc * 8);
-      *reinterpret_cast<uint4*>(reinterpret_cast<char*>(sB) + kc * (BN / 8) * 128 + (n / 8) * 128 + (n % 8) * 16) = v;
+      *reinterpret_cast<uint4*>(sB + kc * (BN / 8) * 128 + (n / 8) * 128 + (n % 8) * 16) = v;
     }
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncthreads();
     if (tid == 0) {
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const uint32_t aaddr = base + st * stage_bytes<BN, BK>(), baddr = aaddr + BM * BK * 2;
 #pragma unroll
       for (int ks = 0; ks < BK / 16; ++ks) {
         const uint64_t da = sdesc(aaddr + ks * 2 * (BM / 8) * 128, (BM / 8) * 128, 128);
@@ -124,13 +162,18 @@ __global__ void __launch_bounds__(kThreads) k_gemm(const __nv_bfloat16* __restri
             "l"(da), "l"(db), "r"(idesc<BN>()), "r"(acc)
             : "memory");
       }
-      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(su32(&mbar))
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                       su32(&mbar[st]))
                    : "memory");
     }
-    ok = mbar_wait(&mbar, phase);
-    phase ^= 1;
-    __syncthreads();
+    used[st] = 1;
   }
+  // drain: MMAs complete in order, so waiting for both stages' last batches suffices
+  for (int st = 0; st < 2; ++st)
+    if (used[st]) {
+      const bool w = mbar_wait(&mbar[st], phase[st]);
+      ok = ok && w;
+    }
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   if (!ok) {
     if (tid == 0) atomicExch(err, 1);
@@ -165,9 +208,22 @@ __global__ void __launch_bounds__(kThreads) k_gemm(const __nv_bfloat16* __restri
   if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(BN) : "memory");
 }
 
+template <int BN, int BK>
+void launch_k(dim3 grid, const __nv_bfloat16* A, const __nv_bfloat16* B, int M, int N, int K, const GemmEpilogue& ep,
+              int* err, cudaStream_t s, const ConvA& conv) {
+  constexpr int bytes = 2 * stage_bytes<BN, BK>();
+  static std::once_flag once;  // per instantiation; shared by concurrent callers
+  std::call_once(once, [] {
+    GP_CUDA(cudaFuncSetAttribute(k_gemm<BN, BK>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  });
+  if (conv.x && (conv.cin % BK != 0 || K != 9 * conv.cin))
+    throw std::invalid_argument("gemm_bf16: implicit im2col needs K = 9 cin and cin a multiple of the K step");
+  k_gemm<BN, BK><<<grid, kThreads, bytes, s>>>(A, B, M, N, K, ep, err, conv);
+}
+
 template <int BN>
 void launch_bn(const __nv_bfloat16* A, const __nv_bfloat16* B, int M, int N, int K, const GemmEpilogue& ep, int* err,
-               cudaStream_t s) {
+               cudaStream_t s, const ConvA& conv) {
   // split K when the output has few tiles and K is long (weight gradients)
   const int tiles = (N / BN) * (M / BM);
   const int ksteps = K / (K % 64 == 0 ? 64 : 32);
@@ -186,25 +242,25 @@ void launch_bn(const __nv_bfloat16* A, const __nv_bfloat16* B, int M, int N, int
         GP_CUDA(cudaMemsetAsync(ep.out_f32 + size_t(r) * ep.ldo, 0, size_t(ep.n_valid) * sizeof(float), s));
   }
   dim3 grid(N / BN, M / BM, splits);
-  if (K % 64 == 0)
-    k_gemm<BN, 64><<<grid, kThreads, 0, s>>>(A, B, M, N, K, ep, err);
+  if (K % 64 == 0 && (!conv.x || conv.cin % 64 == 0))
+    launch_k<BN, 64>(grid, A, B, M, N, K, ep, err, s, conv);
   else
-    k_gemm<BN, 32><<<grid, kThreads, 0, s>>>(A, B, M, N, K, ep, err);
+    launch_k<BN, 32>(grid, A, B, M, N, K, ep, err, s, conv);
   GP_LAUNCH_CHECK();
 }
 
 }  // namespace
 
 void gemm_bf16(const __nv_bfloat16* A, const __nv_bfloat16* B, int M, int N, int K, const GemmEpilogue& ep, int* err,
-               cudaStream_t s) {
+               cudaStream_t s, const ConvA& conv) {
   if (M <= 0 || N <= 0 || K <= 0 || M % BM != 0 || K % 32 != 0)
     throw std::invalid_argument("gemm_bf16: M must be a multiple of 128 and K of 32");
   if (N % 128 == 0)
-    launch_bn<128>(A, B, M, N, K, ep, err, s);
+    launch_bn<128>(A, B, M, N, K, ep, err, s, conv);
   else if (N % 64 == 0)
-    launch_bn<64>(A, B, M, N, K, ep, err, s);
+    launch_bn<64>(A, B, M, N, K, ep, err, s, conv);
   else if (N % 32 == 0)
-    launch_bn<32>(A, B, M, N, K, ep, err, s);
+    launch_bn<32>(A, B, M, N, K, ep, err, s, conv);
   else
     throw std::invalid_argument("gemm_bf16: N must be a multiple of 32");
 }
