@@ -243,18 +243,27 @@ __global__ void k_sub_mean64(double* x, int n, const double* sum) {
 // first and sweeps black, red, black, red.
 // The result goes to u_out: CTAs read their halos from u, so u itself must
 // not change during the launch (u_out == u only when u is not read, PRE).
+// Halo of the tile kernels: 4 points for the four half-sweeps; the
+// pre-smoother keeps 2 more so that the residual on the tile's interior plus
+// one ring (for the full-weighting restriction) is still exact.
+template <bool PRE>
+constexpr int tile_halo() {
+  return PRE ? HALO + 2 : HALO;
+}
+
 template <bool PRE>
 __global__ void __launch_bounds__(kSmoothThreads) k_smooth_tile(const float* u, float* u_out,
                                                                 const float* __restrict__ f, LevelDesc d,
                                                                 const float* __restrict__ uc, LevelDesc c,
-                                                                const double* st) {
-  __shared__ float su[SH][SW + 1];
-  __shared__ float sf[SH][SW + 1];
-  __shared__ unsigned char s_in[SH][SW];
+                                                                const double* st, float* __restrict__ fc_out) {
+  constexpr int HL = tile_halo<PRE>(), W = TX + 2 * HL, H = TY + 2 * HL;
+  __shared__ float su[H][W + 1];
+  __shared__ float sf[H][W + 1];
+  __shared__ unsigned char s_in[H][W];
   if (st[S_DONE] != 0.0) return;
-  const int x0 = blockIdx.x * TX - HALO, y0 = blockIdx.y * TY - HALO;
-  for (int e = threadIdx.x; e < SW * SH; e += kSmoothThreads) {
-    const int li = e % SW, lj = e / SW;
+  const int x0 = blockIdx.x * TX - HL, y0 = blockIdx.y * TY - HL;
+  for (int e = threadIdx.x; e < W * H; e += kSmoothThreads) {
+    const int li = e % W, lj = e / W;
     int gi = x0 + li, gj = y0 + lj;
     const bool inside = wrap(gi, d.mx, d.bx) && wrap(gj, d.my, d.by);
     float uv = 0.0f, fv = 0.0f;
@@ -271,24 +280,53 @@ __global__ void __launch_bounds__(kSmoothThreads) k_smooth_tile(const float* u, 
 #pragma unroll
   for (int hs = 0; hs < 4; ++hs) {
     const int color = PRE ? (hs & 1) : 1 - (hs & 1);
-    // points of this color in [1, SW-2] x [1, SH-2]
-    for (int e = threadIdx.x; e < (SW - 2) * (SH - 2) / 2 + SH; e += kSmoothThreads) {
-      const int lj = 1 + e / ((SW - 2) / 2);
-      if (lj > SH - 2) break;
-      const int k = e % ((SW - 2) / 2);
+    // points of this color in [1, W-2] x [1, H-2]
+    for (int e = threadIdx.x; e < (W - 2) * (H - 2) / 2 + H; e += kSmoothThreads) {
+      const int lj = 1 + e / ((W - 2) / 2);
+      if (lj > H - 2) break;
+      const int k = e % ((W - 2) / 2);
       // global parity (x0 + li + y0 + lj) & 1 == color
       const int par = (x0 + y0 + lj + 1) & 1;  // parity of li = 1
       const int li = 1 + 2 * k + ((par ^ color) & 1);
-      if (li > SW - 2 || !s_in[lj][li]) continue;
+      if (li > W - 2 || !s_in[lj][li]) continue;
       const float s = d.cx * (su[lj][li - 1] + su[lj][li + 1]) + d.cy * (su[lj - 1][li] + su[lj + 1][li]);
       su[lj][li] = (sf[lj][li] - s) * inv;
     }
     __syncthreads();
   }
   for (int e = threadIdx.x; e < TX * TY; e += kSmoothThreads) {
-    const int li = HALO + e % TX, lj = HALO + e / TX;
+    const int li = HL + e % TX, lj = HL + e / TX;
     const int gi = x0 + li, gj = y0 + lj;
     if (gi < d.mx && gj < d.my) u_out[gi + gj * d.mx] = su[lj][li];
+  }
+  if constexpr (PRE) {
+    if (!fc_out) return;
+    // residual r = f - A u on the interior plus one ring (into sr), then the
+    // full-weighting restriction of the coarse points whose centre this tile owns
+    __shared__ float sr[TY + 2][TX + 2];
+    for (int e = threadIdx.x; e < (TX + 2) * (TY + 2); e += kSmoothThreads) {
+      const int li = HL - 1 + e % (TX + 2), lj = HL - 1 + e / (TX + 2);
+      float r = 0.0f;
+      if (s_in[lj][li])
+        r = sf[lj][li] - (d.cd * su[lj][li] + d.cx * (su[lj][li - 1] + su[lj][li + 1]) +
+                          d.cy * (su[lj - 1][li] + su[lj + 1][li]));
+      sr[lj - (HL - 1)][li - (HL - 1)] = r;
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < (TX / 2) * (TY / 2); e += kSmoothThreads) {
+      const int I = blockIdx.x * (TX / 2) + e % (TX / 2), J = blockIdx.y * (TY / 2) + e / (TX / 2);
+      if (I >= c.mx || J >= c.my) continue;
+      const int fi = d.bx != BC_DIR ? 2 * I : 2 * I + 1, fj = d.by != BC_DIR ? 2 * J : 2 * J + 1;
+      const int li = fi - x0 - (HL - 1), lj = fj - y0 - (HL - 1);  // in sr
+      float v = 0.0f;
+#pragma unroll
+      for (int b = -1; b <= 1; ++b) {
+        const float wb = b == 0 ? 0.5f : 0.25f;
+#pragma unroll
+        for (int a = -1; a <= 1; ++a) v += (a == 0 ? 0.5f : 0.25f) * wb * sr[lj + b][li + a];
+      }
+      fc_out[I + J * c.mx] = v;
+    }
   }
 }
 
@@ -610,6 +648,10 @@ int coarser(int n, int b) { return b == BC_PER ? n / 2 : b == BC_NEU ? (n + 1) /
 bool tiled(const PoissonMG::Level& l) {
   return l.mx >= SW && l.my >= SH && (l.bx != BC_PER || l.mx % 2 == 0) && (l.by != BC_PER || l.my % 2 == 0);
 }
+// the pre-smoother with the fused residual + restriction (wider halo)
+bool tiled_pre(const PoissonMG::Level& l) {
+  return tiled(l) && l.mx >= SW + 4 && l.my >= SH + 4;
+}
 int bc_code(const kern::PoissonLayout& L, bool x) {
   if (x ? L.periodic_x : L.periodic_y) return BC_PER;
   return L.fbc[x ? 0 : 2] == kern::FBC_NEUMANN_C ? BC_NEU : BC_DIR;
@@ -746,9 +788,16 @@ void PoissonMG::vcycle(cudaStream_t s) {
     Level& a = lv_[l];
     Level& b = lv_[l + 1];
     const LevelDesc d = desc(a);
-    if (tiled(a) && nu_pre_ == 2) {
+    if (tiled_pre(a) && nu_pre_ == 2) {  // smoothing, residual and restriction in one launch
       dim3 grid((a.mx + TX - 1) / TX, (a.my + TY - 1) / TY);
-      k_smooth_tile<true><<<grid, kSmoothThreads, 0, s>>>(a.u.get(), a.u.get(), a.f.get(), d, nullptr, d, st);
+      k_smooth_tile<true><<<grid, kSmoothThreads, 0, s>>>(a.u.get(), a.u.get(), a.f.get(), d, nullptr, desc(b), st,
+                                                           b.f.get());
+      GP_LAUNCH_CHECK();
+      continue;
+    } else if (tiled(a) && nu_pre_ == 2) {
+      dim3 grid((a.mx + TX - 1) / TX, (a.my + TY - 1) / TY);
+      k_smooth_tile<true><<<grid, kSmoothThreads, 0, s>>>(a.u.get(), a.u.get(), a.f.get(), d, nullptr, d, st,
+                                                           nullptr);
       GP_LAUNCH_CHECK();
     } else {
       k_zero32<<<blocks_for(a.mx * a.my), 256, 0, s>>>(a.u.get(), a.mx * a.my, st);
@@ -788,7 +837,7 @@ void PoissonMG::vcycle(cudaStream_t s) {
     if (tiled(a) && nu_post_ == 2) {
       dim3 grid((a.mx + TX - 1) / TX, (a.my + TY - 1) / TY);
       k_smooth_tile<false><<<grid, kSmoothThreads, 0, s>>>(a.u.get(), a.u2.get(), a.f.get(), d, result(l + 1), desc(b),
-                                                            st);
+                                                            st, nullptr);
       GP_LAUNCH_CHECK();
       a.result_in_u2 = true;
     } else {
