@@ -227,7 +227,11 @@ __device__ __forceinline__ void deposit_one(const GridDims& g, const Window& w, 
 }
 
 // Gather Ex, Ey (and Bz) for one particle (src/Particle.mm:142-154).
-// WIN: from the staged windows; CHECKED: global with bounds checks.
+// WIN: from the staged windows; CHECKED: global with bounds checks (a tap
+// outside the arrays contributes zero). Every path evaluates the same
+// separable sum -- each stencil row reduced with the x weights, then the row
+// sums with the y weights (20 instead of 32 multiply-adds per component) --
+// so a particle's result does not depend on which path its chunk takes.
 template <int ORDER, bool BZU, bool WIN, bool CHECKED>
 __device__ __forceinline__ void gather(const GridDims& g, const FieldPtrs& f, const Window& w, const Stagger& sx,
                                        const Stagger& sy, const float (&wxn)[ORDER + 1],
@@ -237,24 +241,35 @@ __device__ __forceinline__ void gather(const GridDims& g, const FieldPtrs& f, co
   const int ngb = g.ngb, nx = g.nx, ny = g.ny;
   const int hc = sx.half - ngb + 1, nc = sx.node - ngb;   // Ex/Bz and Ey column bases
   const int nr = sy.node - ngb, hr = sy.half - ngb + 1;   // Ex and Ey/Bz row bases
+  // tap (i, j) of each component
+  auto ex = [&](int i, int j) -> float {
+    if constexpr (WIN) return sEx[(hc + i - w.gx0) + (nr + j - w.gy0) * w.gw];
+    if (CHECKED && !in_box(hc + i, nr + j, nx + 2, ny + 1)) return 0.0f;
+    return __ldg(f.Ex + (hc + i) + (nr + j) * (nx + 2));
+  };
+  auto ey = [&](int i, int j) -> float {
+    if constexpr (WIN) return sEy[(nc + i - w.gx0) + (hr + j - w.gy0) * w.gw];
+    if (CHECKED && !in_box(nc + i, hr + j, nx + 1, ny + 2)) return 0.0f;
+    return __ldg(f.Ey + (nc + i) + (hr + j) * (nx + 1));
+  };
+  auto bz = [&](int i, int j) -> float {
+    if constexpr (WIN) return sBz[(hc + i - w.gx0) + (hr + j - w.gy0) * w.gw];
+    if (CHECKED && !in_box(hc + i, hr + j, nx + 2, ny + 2)) return 0.0f;
+    return __ldg(f.Bz + (hc + i) + (hr + j) * (nx + 2));
+  };
 #pragma unroll
-  for (int i = 0; i <= ORDER; ++i)
+  for (int j = 0; j <= ORDER; ++j) {
+    float rx = 0.0f, ry = 0.0f, rz = 0.0f;
 #pragma unroll
-    for (int j = 0; j <= ORDER; ++j) {
-      if constexpr (WIN) {
-        Epx += (wxh[i] * wyn[j]) * sEx[(hc + i - w.gx0) + (nr + j - w.gy0) * w.gw];
-        Epy += (wxn[i] * wyh[j]) * sEy[(nc + i - w.gx0) + (hr + j - w.gy0) * w.gw];
-        if constexpr (!BZU) Bpz += (wxh[i] * wyh[j]) * sBz[(hc + i - w.gx0) + (hr + j - w.gy0) * w.gw];
-      } else {
-        if (!CHECKED || in_box(hc + i, nr + j, nx + 2, ny + 1))
-          Epx += (wxh[i] * wyn[j]) * __ldg(f.Ex + (hc + i) + (nr + j) * (nx + 2));
-        if (!CHECKED || in_box(nc + i, hr + j, nx + 1, ny + 2))
-          Epy += (wxn[i] * wyh[j]) * __ldg(f.Ey + (nc + i) + (hr + j) * (nx + 1));
-        if constexpr (!BZU)
-          if (!CHECKED || in_box(hc + i, hr + j, nx + 2, ny + 2))
-            Bpz += (wxh[i] * wyh[j]) * __ldg(f.Bz + (hc + i) + (hr + j) * (nx + 2));
-      }
+    for (int i = 0; i <= ORDER; ++i) {
+      rx += wxh[i] * ex(i, j);
+      ry += wxn[i] * ey(i, j);
+      if constexpr (!BZU) rz += wxh[i] * bz(i, j);
     }
+    Epx += wyn[j] * rx;
+    Epy += wyh[j] * ry;
+    if constexpr (!BZU) Bpz += wyh[j] * rz;
+  }
 }
 
 // Reflection of a coordinate (cell, offset) about the integer plane B:
@@ -319,7 +334,7 @@ __host__ __device__ constexpr size_t smem_bytes() {
 }
 
 template <int ORDER, bool PUSH, bool DEP, bool DET, bool CUR, bool BZU>
-__global__ void __launch_bounds__(kThreads, ORDER == 5 ? 2 : 4) k_pic(GridDims g, ParticleArrays p, FieldPtrs f, PushConsts c,
+__global__ void __launch_bounds__(kThreads, ORDER == 5 ? 2 : (PUSH && (!BZU || !DEP) ? 3 : 4)) k_pic(GridDims g, ParticleArrays p, FieldPtrs f, PushConsts c,
                                                   int boris_order, DepositTargets d, SpeciesCounters* cnt,
                                                   uint32_t* dead_bits, int injected_only) {
   using DL = DepositLayout<ORDER, CUR>;
@@ -436,20 +451,40 @@ __global__ void __launch_bounds__(kThreads, ORDER == 5 ? 2 : 4) k_pic(GridDims g
   }
   __syncthreads();
 
-  // ---- phase C: particles
+  // ---- phase C: particles. The loads of a thread's next particle are issued
+  // before the current one is processed, so that their latency overlaps the
+  // arithmetic (the kernel is otherwise bound by the load round trip).
   uint32_t wcount[4] = {0, 0, 0, 0}, ninvalid = 0, ndead = 0, nslow = 0;
   double ke = 0.0;
+  constexpr bool kVel = PUSH || CUR;
+  int32_t q_cell = -1;
+  float q_ox = 0.0f, q_oy = 0.0f, q_vx = 0.0f, q_vy = 0.0f, q_vz = 0.0f;
+  auto fetch = [&](uint32_t k) {
+    if (k < n) {
+      q_cell = p.cell[k];
+      q_ox = p.ox[k];
+      q_oy = p.oy[k];
+      if constexpr (kVel) {
+        q_vx = p.vx[k];
+        q_vy = p.vy[k];
+      }
+      if constexpr (PUSH) q_vz = p.vz[k];
+    }
+  };
+  fetch(base + uint32_t(tid));
 #pragma unroll 1
   for (int i = 0; i < kPer; ++i) {
     const uint32_t k = base + uint32_t(i * kThreads + tid);
+    const int32_t cell = q_cell;
+    const float l_ox = q_ox, l_oy = q_oy, l_vx = q_vx, l_vy = q_vy, l_vz = q_vz;
+    if (i + 1 < kPer) fetch(k + uint32_t(kThreads));
     int fl = 0;
     if (k < n) {
-      const int32_t cell = p.cell[k];
       if (cell < 0) {
         fl = -cell;  // flagged before this push and not yet compacted: keep the flag
       } else {
         int ix = cell_ix(cell), iy = cell_iy(cell);
-        float ox = p.ox[k], oy = p.oy[k];
+        float ox = l_ox, oy = l_oy;
         const bool inside = interior(g, ix, iy);
         const bool in_box_win = w.use && ix >= w.mnx && ix <= w.mxx && iy >= w.mny && iy <= w.mxy;
         if constexpr (!PUSH) {
@@ -461,8 +496,8 @@ __global__ void __launch_bounds__(kThreads, ORDER == 5 ? 2 : 4) k_pic(GridDims g
           if constexpr (CUR) {
             shape<ORDER>(sx.hhalf, wxh);
             shape<ORDER>(sy.hhalf, wyh);
-            vx = p.vx[k];
-            vy = p.vy[k];
+            vx = l_vx;
+            vy = l_vy;
           }
           if (in_box_win && sublight<CUR>(vx, vy))
             deposit_one<ORDER, DET, CUR, true, false>(g, w, lane, sx, sy, wxn, wxh, wyn, wyh, c.scale, vx, vy, d, sw);
@@ -471,7 +506,7 @@ __global__ void __launch_bounds__(kThreads, ORDER == 5 ? 2 : 4) k_pic(GridDims g
           else
             deposit_one<ORDER, DET, CUR, false, true>(g, w, lane, sx, sy, wxn, wxh, wyn, wyh, c.scale, vx, vy, d, sw);
         } else {
-          float vx = p.vx[k], vy = p.vy[k], vz = p.vz[k];
+          float vx = l_vx, vy = l_vy, vz = l_vz;
           const Stagger sx = stagger(ix, ox), sy = stagger(iy, oy);
           float wxn[ORDER + 1], wxh[ORDER + 1], wyn[ORDER + 1], wyh[ORDER + 1];
           shape<ORDER>(sx.hnode, wxn);
