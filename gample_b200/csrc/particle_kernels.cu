@@ -59,17 +59,6 @@ __device__ __forceinline__ void gadd(double* p, float v) { atomicAdd(p, double(v
 __device__ __forceinline__ void gadd(long long* p, long long v) {
   atomicAdd(reinterpret_cast<unsigned long long*>(p), static_cast<unsigned long long>(v));
 }
-// Shared-memory windows hold exact fixed-point sums (weights quantised to
-// 2^-40) split over two 32-bit words per node: hi = q >> 20 (signed) and
-// lo = q & (2^20 - 1), each added with a native 32-bit integer atomic (the
-// floating-point and 64-bit shared-memory atomics are compare-and-swap
-// loops that retry under contention). A copy of a window receives at most
-// kChunk contributions per node, each with |q| <= 2^40, so neither word can
-// overflow; the flush recombines hi * 2^20 + lo in 64 bits.
-__device__ __forceinline__ void wadd(int* hi, int* lo, long long q) {
-  atomicAdd(hi, int(q >> 20));
-  atomicAdd(lo, int(q & 0xFFFFF));
-}
 
 // Contribution of one stencil node (rho and the two currents).
 template <bool DET>
@@ -138,9 +127,48 @@ __device__ __forceinline__ long long wsum(const int* s, int ihi, int ilo) {
   return (static_cast<long long>(s[ihi]) << 20) + static_cast<long long>(static_cast<unsigned>(s[ilo]));
 }
 
-struct WinPtrs {  // this lane's copy of the window arrays (hi / lo words)
-  int *rho_hi, *rho_lo, *jx_hi, *jx_lo, *jy_hi, *jy_lo;
+// Deposit windows: each array has kCopies private copies, lane L adding into
+// copy (L / N^2) mod kCopies. With the rotated stencil order this gives the
+// 32 lanes of a warp whose particles share a cell 32 distinct addresses: N^2
+// distinct nodes per copy, and the copy stride (congruent to N^2 mod 32)
+// moves each copy onto its own banks. Copies are summed at the flush.
+template <int ORDER, bool CUR>
+struct DepositLayout {
+  static constexpr int kN2 = (ORDER + 1) * (ORDER + 1);
+  static constexpr int kStride = kWin + kN2 % 32;
+  static constexpr int kArrays = CUR ? 6 : 2;  // hi and lo words of rho (jx, jy)
+  static constexpr size_t kCopyBytes = size_t(kStride) * kArrays * sizeof(int);
+  static constexpr int copies() {
+    int c = kN2 >= 32 ? 1 : 32 / kN2;
+    while (c > 1 && size_t(c) * kCopyBytes > kDepositBudget) c >>= 1;
+    return c;
+  }
+  static constexpr int kCopies = copies();
+  static constexpr int kArrayBytes = kCopies * kStride * int(sizeof(int));  // one array, all copies
+  static constexpr size_t kBytes = size_t(kCopies) * kCopyBytes;
 };
+
+// This lane's copy of the window arrays: shared-memory byte address of its rho
+// hi-word copy; array a (rho hi, rho lo, jx hi, jx lo, jy hi, jy lo) lies
+// a * kArrayBytes further.
+struct WinPtrs {
+  uint32_t rho;
+};
+
+// Shared-memory windows hold exact fixed-point sums (weights quantised to
+// 2^-40) split over two 32-bit words per node: hi = q >> 20 (signed) and
+// lo = q & (2^20 - 1), each added with a native 32-bit integer reduction (the
+// floating-point and 64-bit shared-memory atomics are compare-and-swap
+// loops that retry under contention). A copy of a window receives at most
+// kChunk contributions per node, each with |q| <= 2^40, so neither word can
+// overflow; the flush recombines hi * 2^20 + lo in 64 bits.
+// One contribution: hi word at addr + HI, lo word at addr + LO (byte offsets
+// known at compile time, folded into the instructions).
+template <int HI, int LO>
+__device__ __forceinline__ void wadd_s(uint32_t addr, long long q) {
+  asm volatile("red.shared.add.s32 [%0+%1], %2;" ::"r"(addr), "n"(HI), "r"(int(q >> 20)) : "memory");
+  asm volatile("red.shared.add.s32 [%0+%1], %2;" ::"r"(addr), "n"(LO), "r"(int(q & 0xFFFFF)) : "memory");
+}
 
 // The window path accumulates quant40(w) for rho and quant40(w * v / c) for
 // the currents in both deposit modes; the caller sends a particle with
@@ -158,38 +186,41 @@ __device__ __forceinline__ void deposit_one(const GridDims& g, const Window& w, 
   const int rc = sx.node - ngb, rr = sy.node - ngb;  // rho / jy column base, rho / jx row base
   const int xc = sx.half - ngb + 1, yr = sy.half - ngb + 1;  // jx column base, jy row base
   if constexpr (WIN) {
+    constexpr int kA = DepositLayout<ORDER, CUR>::kArrayBytes;
     const int si = lane % N, sj = (lane / N) % N;
+    // x weights pre-scaled by 2^40 (exact): quant40(wx * wy) == rn(wx' * wy)
     float rxn[N], ryn[N];
     rotate<N>(wxn, si, rxn);
     rotate<N>(wyn, sj, ryn);
-    int col[N], row[N];
+#pragma unroll
+    for (int t = 0; t < N; ++t) rxn[t] = __fmul_rn(rxn[t], kQuant);
+    uint32_t col[N], row[N];  // byte offsets of the rotated stencil columns / rows
 #pragma unroll
     for (int t = 0; t < N; ++t) {
-      col[t] = t + si >= N ? t + si - N : t + si;
-      row[t] = (t + sj >= N ? t + sj - N : t + sj) * w.ds;
+      col[t] = 4u * uint32_t(t + si >= N ? t + si - N : t + si);
+      row[t] = 4u * uint32_t((t + sj >= N ? t + sj - N : t + sj) * w.ds);
     }
-    const int orho = (rc - w.dx0) + (rr - w.dy0) * w.ds;
+    const uint32_t arho = s.rho + 4u * uint32_t((rc - w.dx0) + (rr - w.dy0) * w.ds);
 #pragma unroll
     for (int a = 0; a < N; ++a)
 #pragma unroll
-      for (int b = 0; b < N; ++b) {
-        const int o = orho + col[b] + row[a];
-        wadd(s.rho_hi + o, s.rho_lo + o, quant40(__fmul_rn(rxn[b], ryn[a])));
-      }
+      for (int b = 0; b < N; ++b)
+        wadd_s<0, kA>(arho + col[b] + row[a], __float2ll_rn(__fmul_rn(rxn[b], ryn[a])));
     if constexpr (CUR) {
       float rxh[N], ryh[N];
       rotate<N>(wxh, si, rxh);
       rotate<N>(wyh, sj, ryh);
+#pragma unroll
+      for (int t = 0; t < N; ++t) rxh[t] = __fmul_rn(rxh[t], kQuant);
       const float ux = __fmul_rn(vx, inv_c), uy = __fmul_rn(vy, inv_c);
-      const int ojx = (xc - w.dx0) + (rr - w.dy0) * w.ds;
-      const int ojy = (rc - w.dx0) + (yr - w.dy0) * w.ds;
+      const uint32_t ajx = s.rho + 4u * uint32_t((xc - w.dx0) + (rr - w.dy0) * w.ds);
+      const uint32_t ajy = s.rho + 4u * uint32_t((rc - w.dx0) + (yr - w.dy0) * w.ds);
 #pragma unroll
       for (int a = 0; a < N; ++a)
 #pragma unroll
         for (int b = 0; b < N; ++b) {
-          const int ox = ojx + col[b] + row[a], oy = ojy + col[b] + row[a];
-          wadd(s.jx_hi + ox, s.jx_lo + ox, quant40(__fmul_rn(__fmul_rn(rxh[b], ryn[a]), ux)));
-          wadd(s.jy_hi + oy, s.jy_lo + oy, quant40(__fmul_rn(__fmul_rn(rxn[b], ryh[a]), uy)));
+          wadd_s<2 * kA, 3 * kA>(ajx + col[b] + row[a], __float2ll_rn(__fmul_rn(__fmul_rn(rxh[b], ryn[a]), ux)));
+          wadd_s<4 * kA, 5 * kA>(ajy + col[b] + row[a], __float2ll_rn(__fmul_rn(__fmul_rn(rxn[b], ryh[a]), uy)));
         }
     }
   } else {
@@ -304,29 +335,21 @@ __device__ __forceinline__ bool advance(int& i, float& o, float v, float cst) {
   return true;
 }
 
+// Periodic wrap of a cell index into [ngb, ngb + n): one conditional add or
+// subtract for a move of less than a period, the remainder otherwise.
+__device__ __forceinline__ int wrap_periodic(int i, int ngb, int n) {
+  int d = i - ngb;
+  if (d < 0)
+    d += n;
+  else if (d >= n)
+    d -= n;
+  if (d < 0 || d >= n) d = ((d % n) + n) % n;
+  return ngb + d;
+}
+
 __device__ __forceinline__ bool interior(const GridDims& g, int ix, int iy) {
   return ix >= g.ngb && ix < g.ngb + g.ngx && iy >= g.ngb && iy < g.ngb + g.ngy;
 }
-
-// Deposit windows: each array has kCopies private copies, lane L adding into
-// copy (L / N^2) mod kCopies. With the rotated stencil order this gives the
-// 32 lanes of a warp whose particles share a cell 32 distinct addresses: N^2
-// distinct nodes per copy, and the copy stride (congruent to N^2 mod 32)
-// moves each copy onto its own banks. Copies are summed at the flush.
-template <int ORDER, bool CUR>
-struct DepositLayout {
-  static constexpr int kN2 = (ORDER + 1) * (ORDER + 1);
-  static constexpr int kStride = kWin + kN2 % 32;
-  static constexpr int kArrays = CUR ? 6 : 2;  // hi and lo words of rho (jx, jy)
-  static constexpr size_t kCopyBytes = size_t(kStride) * kArrays * sizeof(int);
-  static constexpr int copies() {
-    int c = kN2 >= 32 ? 1 : 32 / kN2;
-    while (c > 1 && size_t(c) * kCopyBytes > kDepositBudget) c >>= 1;
-    return c;
-  }
-  static constexpr int kCopies = copies();
-  static constexpr size_t kBytes = size_t(kCopies) * kCopyBytes;
-};
 
 template <int ORDER, bool PUSH, bool DEP, bool DET, bool CUR, bool BZU>
 __host__ __device__ constexpr size_t smem_bytes() {
@@ -357,12 +380,7 @@ __global__ void __launch_bounds__(kThreads, ORDER == 5 ? 2 : (PUSH && (!BZU || !
   const int ngb = g.ngb;
   const int copy = (lane / DL::kN2) % DL::kCopies;
   WinPtrs sw;
-  sw.rho_hi = sDep + copy * DL::kStride;
-  sw.rho_lo = sDep + (DL::kCopies + copy) * DL::kStride;
-  sw.jx_hi = sDep + (2 * DL::kCopies + copy) * DL::kStride;
-  sw.jx_lo = sDep + (3 * DL::kCopies + copy) * DL::kStride;
-  sw.jy_hi = sDep + (4 * DL::kCopies + copy) * DL::kStride;
-  sw.jy_lo = sDep + (5 * DL::kCopies + copy) * DL::kStride;
+  sw.rho = static_cast<uint32_t>(__cvta_generic_to_shared(sDep + copy * DL::kStride));
 
   // ---- phase A: box of the chunk's cells (re-read from L1 below). Only
   // particles within kReach cells of the chunk's middle particle count, so
@@ -553,8 +571,8 @@ __global__ void __launch_bounds__(kThreads, ORDER == 5 ? 2 : (PUSH && (!BZU || !
           if (!(okx && oky) || !isfinite(vz)) {
             fl = 5;
           } else {
-            if (c.bc[0] == 0) ix = ngb + (((ix - ngb) % g.ngx) + g.ngx) % g.ngx;
-            if (c.bc[2] == 0) iy = ngb + (((iy - ngb) % g.ngy) + g.ngy) % g.ngy;
+            if (c.bc[0] == 0) ix = wrap_periodic(ix, ngb, g.ngx);
+            if (c.bc[2] == 0) iy = wrap_periodic(iy, ngb, g.ngy);
             if (c.bc[0] == 1 && ix < ngb) fl = 1;
             if (c.bc[1] == 1 && ix >= ngb + g.ngx) fl = 2;
             if (c.bc[2] == 1 && iy < ngb) fl = 3;
