@@ -472,8 +472,11 @@ __global__ void __launch_bounds__(kThreads, ORDER == 5 ? 2 : (PUSH && (!BZU || !
   // ---- phase C: particles. The loads of a thread's next particle are issued
   // before the current one is processed, so that their latency overlaps the
   // arithmetic (the kernel is otherwise bound by the load round trip).
-  uint32_t wcount[4] = {0, 0, 0, 0}, ninvalid = 0, ndead = 0, nslow = 0;
-  double ke = 0.0;
+  // per-thread tallies in 4-bit fields of one register (at most kPer each):
+  // dead [0,4), wall w [4(w+1), 4(w+2)), invalid [20,24), slow [24,28)
+  static_assert(kPer < 16, "tally fields are 4 bits wide");
+  uint32_t tally = 0;
+  double ke = 0.0;  // sum of |v|^2 (FP64) over this thread's pushed particles
   constexpr bool kVel = PUSH || CUR;
   int32_t q_cell = -1;
   float q_ox = 0.0f, q_oy = 0.0f, q_vx = 0.0f, q_vy = 0.0f, q_vz = 0.0f;
@@ -538,7 +541,7 @@ __global__ void __launch_bounds__(kThreads, ORDER == 5 ? 2 : (PUSH && (!BZU || !
             gather<ORDER, BZU, false, false>(g, f, w, sx, sy, wxn, wxh, wyn, wyh, sEx, sEy, sBz, Epx, Epy, Bpz);
           else
             gather<ORDER, BZU, false, true>(g, f, w, sx, sy, wxn, wxh, wyn, wyh, sEx, sEy, sBz, Epx, Epy, Bpz);
-          if (!in_box_win) nslow++;
+          if (!in_box_win) tally += 1u << 24;
           if constexpr (BZU) Bpz = c.bz_uniform;
           // Boris push (src/Particle.mm:157-209); Ez, Bx, By are identically
           // zero in the reference's gather (:134-139).
@@ -570,7 +573,7 @@ __global__ void __launch_bounds__(kThreads, ORDER == 5 ? 2 : (PUSH && (!BZU || !
           const bool oky = advance(iy, oy, vy, c.constY);
           if (!(okx && oky) || !isfinite(vz)) {
             fl = 5;
-          } else {
+          } else if (!interior(g, ix, iy)) {  // boundary conditions act only on a particle that left the grid
             if (c.bc[0] == 0) ix = wrap_periodic(ix, ngb, g.ngx);
             if (c.bc[2] == 0) iy = wrap_periodic(iy, ngb, g.ngy);
             if (c.bc[0] == 1 && ix < ngb) fl = 1;
@@ -605,9 +608,8 @@ __global__ void __launch_bounds__(kThreads, ORDER == 5 ? 2 : (PUSH && (!BZU || !
             p.cell[k] = pack_cell(ix, iy);
             p.ox[k] = ox;
             p.oy[k] = oy;
-            // kinetic energy, src/Particle.mm:980-982
             const float vv = __fadd_rn(__fadd_rn(__fmul_rn(vx, vx), __fmul_rn(vy, vy)), __fmul_rn(vz, vz));
-            ke += (c.ke_half_m * double(vv)) * c.ke_w;
+            ke += double(vv);
             if constexpr (DEP) {
               const Stagger nsx = stagger(ix, ox), nsy = stagger(iy, oy);
               shape<ORDER>(nsx.hnode, wxn);
@@ -630,13 +632,8 @@ __global__ void __launch_bounds__(kThreads, ORDER == 5 ? 2 : (PUSH && (!BZU || !
           }
         }
       }
-      if (fl) {  // includes particles flagged before this push and not yet compacted
-        ndead++;
-        if (fl <= 4)
-          wcount[fl - 1]++;
-        else
-          ninvalid++;
-      }
+      if (fl)  // includes particles flagged before this push and not yet compacted
+        tally += 1u + (fl <= 4 ? 1u << (4 * fl) : 1u << 20);
     }
     if constexpr (PUSH) {
       const uint32_t wbase = base + uint32_t(i * kThreads + wid * 32);
@@ -689,11 +686,12 @@ __global__ void __launch_bounds__(kThreads, ORDER == 5 ? 2 : (PUSH && (!BZU || !
   }
 
   if constexpr (PUSH) {
-    const uint32_t s_dead = warp_sum(ndead);
-    const uint32_t s_w0 = warp_sum(wcount[0]), s_w1 = warp_sum(wcount[1]);
-    const uint32_t s_w2 = warp_sum(wcount[2]), s_w3 = warp_sum(wcount[3]);
-    const uint32_t s_inv = warp_sum(ninvalid), s_slow = warp_sum(nslow);
-    const double s_ke = warp_sum(ke);
+    auto field = [&](int f) { return warp_sum((tally >> (4 * f)) & 0xFu); };
+    const uint32_t s_dead = field(0);
+    const uint32_t s_w0 = field(1), s_w1 = field(2);
+    const uint32_t s_w2 = field(3), s_w3 = field(4);
+    const uint32_t s_inv = field(5), s_slow = field(6);
+    const double s_ke = warp_sum(ke) * c.ke_half_m * c.ke_w;  // kinetic energy, src/Particle.mm:980-982
     if (lane == 0) {
       if (s_dead) atomicAdd(&cnt->n_dead, s_dead);
       if (s_w0) atomicAdd(&cnt->wall[0], s_w0);
