@@ -132,11 +132,22 @@ __device__ __forceinline__ long long wsum(const int* s, int ihi, int ilo) {
 // 32 lanes of a warp whose particles share a cell 32 distinct addresses: N^2
 // distinct nodes per copy, and the copy stride (congruent to N^2 mod 32)
 // moves each copy onto its own banks. Copies are summed at the flush.
-template <int ORDER, bool CUR>
+//
+// Two number formats. The deterministic mode, and any deposit with currents,
+// holds exact 2^-40 fixed-point sums in two words per node (below). The atomic
+// mode without currents holds one 32-bit word per node with the weight
+// quantised to 2^-kQBits (2^-22 for orders 1 and 3, 2^-21 for order 5): the
+// rounding of a contribution is at most 2^-(kQBits+1) in weight units, finer
+// than the FP32 atomic additions of the reference's deposit (each rounds the
+// running node sum to 24 bits, src/Particle.mm:362), and the window sums stay
+// exact integers, so only the FP64 flush order varies between runs.
+template <int ORDER, bool CUR, bool DET>
 struct DepositLayout {
   static constexpr int kN2 = (ORDER + 1) * (ORDER + 1);
   static constexpr int kStride = kWin + kN2 % 32;
-  static constexpr int kArrays = CUR ? 6 : 2;  // hi and lo words of rho (jx, jy)
+  static constexpr bool kSingle = !DET && !CUR;
+  static constexpr int kQBits = ORDER == 5 ? 21 : 22;
+  static constexpr int kArrays = kSingle ? 1 : (CUR ? 6 : 2);  // words of rho (jx, jy)
   static constexpr size_t kCopyBytes = size_t(kStride) * kArrays * sizeof(int);
   static constexpr int copies() {
     int c = kN2 >= 32 ? 1 : 32 / kN2;
@@ -146,6 +157,11 @@ struct DepositLayout {
   static constexpr int kCopies = copies();
   static constexpr int kArrayBytes = kCopies * kStride * int(sizeof(int));  // one array, all copies
   static constexpr size_t kBytes = size_t(kCopies) * kCopyBytes;
+  // single word: a copy receives at most kChunk / kCopies contributions per
+  // node, each at most the largest stencil weight (1, (2/3)^2, (11/20)^2)
+  static constexpr double kMaxW = ORDER == 1 ? 1.0 : (ORDER == 3 ? 0.4445 : 0.3026);
+  static_assert(!kSingle || double(kChunk / kCopies) * kMaxW * double(1 << kQBits) < 2147483647.0,
+                "single-word deposit window could overflow");
 };
 
 // This lane's copy of the window arrays: shared-memory byte address of its rho
@@ -171,8 +187,9 @@ __device__ __forceinline__ void wadd_s(uint32_t addr, long long q) {
 }
 
 // The window path accumulates quant40(w) for rho and quant40(w * v / c) for
-// the currents in both deposit modes; the caller sends a particle with
-// |v| >= c (|w v / c| could exceed 1) to the global path instead.
+// the currents (rn(w * 2^kQBits) for rho in the single-word layout); the
+// caller sends a particle with |v| >= c (|w v / c| could exceed 1) to the
+// global path instead.
 template <int ORDER, bool DET, bool CUR, bool WIN, bool CHECKED>
 __device__ __forceinline__ void deposit_one(const GridDims& g, const Window& w, int lane, const Stagger& sx,
                                             const Stagger& sy, const float (&wxn)[ORDER + 1],
@@ -186,14 +203,16 @@ __device__ __forceinline__ void deposit_one(const GridDims& g, const Window& w, 
   const int rc = sx.node - ngb, rr = sy.node - ngb;  // rho / jy column base, rho / jx row base
   const int xc = sx.half - ngb + 1, yr = sy.half - ngb + 1;  // jx column base, jy row base
   if constexpr (WIN) {
-    constexpr int kA = DepositLayout<ORDER, CUR>::kArrayBytes;
+    using DL = DepositLayout<ORDER, CUR, DET>;
+    constexpr int kA = DL::kArrayBytes;
+    // x weights pre-scaled by the fixed-point unit (exact): quant(wx * wy) == rn(wx' * wy)
+    constexpr float kUnit = DL::kSingle ? float(1 << DL::kQBits) : kQuant;
     const int si = lane % N, sj = (lane / N) % N;
-    // x weights pre-scaled by 2^40 (exact): quant40(wx * wy) == rn(wx' * wy)
     float rxn[N], ryn[N];
     rotate<N>(wxn, si, rxn);
     rotate<N>(wyn, sj, ryn);
 #pragma unroll
-    for (int t = 0; t < N; ++t) rxn[t] = __fmul_rn(rxn[t], kQuant);
+    for (int t = 0; t < N; ++t) rxn[t] = __fmul_rn(rxn[t], kUnit);
     uint32_t col[N], row[N];  // byte offsets of the rotated stencil columns / rows
 #pragma unroll
     for (int t = 0; t < N; ++t) {
@@ -204,8 +223,14 @@ __device__ __forceinline__ void deposit_one(const GridDims& g, const Window& w, 
 #pragma unroll
     for (int a = 0; a < N; ++a)
 #pragma unroll
-      for (int b = 0; b < N; ++b)
-        wadd_s<0, kA>(arho + col[b] + row[a], __float2ll_rn(__fmul_rn(rxn[b], ryn[a])));
+      for (int b = 0; b < N; ++b) {
+        if constexpr (DL::kSingle)
+          asm volatile("red.shared.add.s32 [%0], %1;" ::"r"(arho + col[b] + row[a]),
+                       "r"(__float2int_rn(__fmul_rn(rxn[b], ryn[a])))
+                       : "memory");
+        else
+          wadd_s<0, kA>(arho + col[b] + row[a], __float2ll_rn(__fmul_rn(rxn[b], ryn[a])));
+      }
     if constexpr (CUR) {
       float rxh[N], ryh[N];
       rotate<N>(wxh, si, rxh);
@@ -353,14 +378,15 @@ __device__ __forceinline__ bool interior(const GridDims& g, int ix, int iy) {
 
 template <int ORDER, bool PUSH, bool DEP, bool DET, bool CUR, bool BZU>
 __host__ __device__ constexpr size_t smem_bytes() {
-  return (PUSH ? (BZU ? 2 : 3) * size_t(kWin) * sizeof(float) : 0) + (DEP ? DepositLayout<ORDER, CUR>::kBytes : 0);
+  return (PUSH ? (BZU ? 2 : 3) * size_t(kWin) * sizeof(float) : 0) +
+         (DEP ? DepositLayout<ORDER, CUR, DET>::kBytes : 0);
 }
 
 template <int ORDER, bool PUSH, bool DEP, bool DET, bool CUR, bool BZU>
 __global__ void __launch_bounds__(kThreads, ORDER == 5 ? 2 : (PUSH && (!BZU || !DEP) ? 3 : 4)) k_pic(GridDims g, ParticleArrays p, FieldPtrs f, PushConsts c,
                                                   int boris_order, DepositTargets d, SpeciesCounters* cnt,
                                                   uint32_t* dead_bits, int injected_only) {
-  using DL = DepositLayout<ORDER, CUR>;
+  using DL = DepositLayout<ORDER, CUR, DET>;
   extern __shared__ __align__(16) unsigned char smem[];
   float* sEx = reinterpret_cast<float*>(smem);
   float* sEy = sEx + (PUSH ? kWin : 0);
@@ -653,14 +679,18 @@ __global__ void __launch_bounds__(kThreads, ORDER == 5 ? 2 : (PUSH && (!BZU || !
         long long r = 0, a = 0, b = 0;
 #pragma unroll
         for (int q = 0; q < DL::kCopies; ++q) {
-          r += wsum(sDep, (0 * DL::kCopies + q) * DL::kStride + e, (1 * DL::kCopies + q) * DL::kStride + e);
+          if constexpr (DL::kSingle)
+            r += static_cast<long long>(sDep[q * DL::kStride + e]);
+          else
+            r += wsum(sDep, (0 * DL::kCopies + q) * DL::kStride + e, (1 * DL::kCopies + q) * DL::kStride + e);
           if constexpr (CUR) {
             a += wsum(sDep, (2 * DL::kCopies + q) * DL::kStride + e, (3 * DL::kCopies + q) * DL::kStride + e);
             b += wsum(sDep, (4 * DL::kCopies + q) * DL::kStride + e, (5 * DL::kCopies + q) * DL::kStride + e);
           }
         }
         // fast mode: FP64 sums of w * scale (currents w * scale * v)
-        const double fr = double(c.scale) * 0x1p-40, fj = fr * 2.99792458e10;
+        const double unit = DL::kSingle ? 1.0 / double(1 << DL::kQBits) : 0x1p-40;
+        const double fr = double(c.scale) * unit, fj = fr * 2.99792458e10;
         if (r != 0 && in_box(col, row, nx + 1, ny + 1)) {
           if constexpr (DET)
             gadd(d.acc_rho + col + row * (nx + 1), r);

@@ -157,6 +157,27 @@ def test_deposit_atomic_matches_fp64(gpu, order, current):
         assert rel_inf(sim.field("jy"), ora.field("jy"), jscale) < 1e-6
 
 
+@pytest.mark.gpu
+def test_deposit_atomic_dense_cells_error_bound(gpu):
+    """The atomic mode without currents sums 2^-22 fixed-point weights in one
+    word per node: with 256 particles per cell per species (thousands of
+    contributions per node) the error stays far below the FP32 atomic
+    accumulation of the reference's deposit."""
+    cond = condition(ngx=16, ngy=16, order=3, ppc=256, xbc="Dirichlet", ybc="periodic", te=10.0)
+    sim, ora = pair(cond, real64=True)
+    for s in range(2):
+        g = sim.particles(s)
+        ora.set_particles(s, g["x"], g["y"], g["vx"], g["vy"], g["vz"])
+    sim.reset_charge()
+    ora.reset_charge()
+    sim.integrate_charge(0)
+    ora.deposit(0)
+    got, ref = sim.field("rho"), ora.field("rho")
+    # per node at most ~16 * 256 contributions, each rounded by <= 2^-23 of a
+    # unit weight: a random walk gives ~1e-8 of the peak density
+    assert rel_inf(got, ref) < 2e-7
+
+
 def combine_fixed(accs, scales, extra=1.0):
     v = np.zeros(accs[0].shape, np.float64)
     for a, s in zip(accs, scales):
