@@ -214,10 +214,14 @@ __device__ __forceinline__ void deposit_one(const GridDims& g, const Window& w, 
 #pragma unroll
     for (int t = 0; t < N; ++t) rxn[t] = __fmul_rn(rxn[t], kUnit);
     uint32_t col[N], row[N];  // byte offsets of the rotated stencil columns / rows
+    const uint32_t ds4 = 4u * uint32_t(w.ds);
 #pragma unroll
     for (int t = 0; t < N; ++t) {
-      col[t] = 4u * uint32_t(t + si >= N ? t + si - N : t + si);
-      row[t] = 4u * uint32_t((t + sj >= N ? t + sj - N : t + sj) * w.ds);
+      constexpr bool kPow2 = (N & (N - 1)) == 0;
+      const int cs = kPow2 ? ((t + si) & (N - 1)) : (t + si >= N ? t + si - N : t + si);
+      const int rs = kPow2 ? ((t + sj) & (N - 1)) : (t + sj >= N ? t + sj - N : t + sj);
+      col[t] = 4u * uint32_t(cs);
+      row[t] = uint32_t(rs) * ds4;
     }
     const uint32_t arho = s.rho + 4u * uint32_t((rc - w.dx0) + (rr - w.dy0) * w.ds);
 #pragma unroll
@@ -360,6 +364,29 @@ __device__ __forceinline__ bool advance(int& i, float& o, float v, float cst) {
   return true;
 }
 
+// Boris rotation factors for a magnetic field Bz (src/Particle.mm:157-209),
+// every operation explicitly rounded: fe scales the half-step electric kick
+// (constE * fN1), btz is the rotation parameter t (times fN1 for the order-4/6
+// corrections) and ssz = 2 t / (1 + t0^2). Uniform Bz makes them constants of
+// the launch, computed once per thread instead of once per particle.
+struct BorisFactors {
+  float fe, btz, ssz;
+};
+__device__ __forceinline__ BorisFactors boris_factors(float Bz, float constE, float constB, int boris_order) {
+  const float t0 = __fmul_rn(constB, Bz);
+  const float tt = __fmul_rn(t0, t0);
+  float fN1 = 1.0f;
+  if (boris_order == 4)
+    fN1 = __fadd_rn(1.0f, __fdiv_rn(tt, 3.0f));
+  else if (boris_order == 6)
+    fN1 = __fadd_rn(__fadd_rn(1.0f, __fdiv_rn(tt, 3.0f)), __fdiv_rn(__fmul_rn(__fmul_rn(2.0f, tt), tt), 15.0f));
+  BorisFactors b;
+  b.fe = __fmul_rn(constE, fN1);
+  b.btz = __fmul_rn(t0, fN1);
+  b.ssz = __fdiv_rn(__fmul_rn(2.0f, b.btz), __fadd_rn(1.0f, tt));
+  return b;
+}
+
 // Periodic wrap of a cell index into [ngb, ngb + n): one conditional add or
 // subtract for a move of less than a period, the remainder otherwise.
 __device__ __forceinline__ int wrap_periodic(int i, int ngb, int n) {
@@ -498,6 +525,7 @@ __global__ void __launch_bounds__(kThreads, ORDER == 5 ? 2 : (PUSH && (!BZU || !
   // ---- phase C: particles. The loads of a thread's next particle are issued
   // before the current one is processed, so that their latency overlaps the
   // arithmetic (the kernel is otherwise bound by the load round trip).
+  const BorisFactors bzu = BZU ? boris_factors(c.bz_uniform, c.constE, c.constB, boris_order) : BorisFactors{};
   // per-thread tallies in 4-bit fields of one register (at most kPer each):
   // dead [0,4), wall w [4(w+1), 4(w+2)), invalid [20,24), slow [24,28)
   static_assert(kPer < 16, "tally fields are 4 bits wide");
@@ -568,27 +596,14 @@ __global__ void __launch_bounds__(kThreads, ORDER == 5 ? 2 : (PUSH && (!BZU || !
           else
             gather<ORDER, BZU, false, true>(g, f, w, sx, sy, wxn, wxh, wyn, wyh, sEx, sEy, sBz, Epx, Epy, Bpz);
           if (!in_box_win) tally += 1u << 24;
-          if constexpr (BZU) Bpz = c.bz_uniform;
           // Boris push (src/Particle.mm:157-209); Ez, Bx, By are identically
           // zero in the reference's gather (:134-139).
-          float etx = c.constE * Epx, ety = c.constE * Epy;
-          float btz = c.constB * Bpz;
-          const float btbt = btz * btz;
-          if (boris_order == 4) {
-            const float fN1 = 1.0f + btbt / 3.0f;
-            etx *= fN1;
-            ety *= fN1;
-            btz *= fN1;
-          } else if (boris_order == 6) {
-            const float fN1 = 1.0f + btbt / 3.0f + 2.0f * btbt * btbt / 15.0f;
-            etx *= fN1;
-            ety *= fN1;
-            btz *= fN1;
-          }
+          const BorisFactors bf = BZU ? bzu : boris_factors(Bpz, c.constE, c.constB, boris_order);
+          const float btz = bf.btz, ssz = bf.ssz;
+          const float etx = __fmul_rn(bf.fe, Epx), ety = __fmul_rn(bf.fe, Epy);
           const float umx = vx + etx, umy = vy + ety, umz = vz;
           const float v0x = umx + umy * btz;
           const float v0y = umy - umx * btz;
-          const float ssz = 2.0f * btz / (1.0f + btbt);
           const float upx = umx + v0y * ssz;
           const float upy = umy - v0x * ssz;
           vx = upx + c.constE * Epx;
