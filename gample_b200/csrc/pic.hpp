@@ -185,6 +185,8 @@ class Particle {
   uint32_t last_pulled = 0;
   double last_dt = 0;
 
+  uint32_t stage_records() const;  // AoS records per upload/download chunk
+
   struct Buffer {
     DeviceArray<int32_t> cell;
     DeviceArray<float> ox, oy, vx, vy, vz;

@@ -1,4 +1,5 @@
 // pic_particle.cpp -- Particle host object (one species).
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <stdexcept>
@@ -88,23 +89,42 @@ void Particle::setPNum(uint32_t n) {
   n_bound = n;
 }
 
+// Host AoS records stream through the spare half of the double buffer (free
+// between cycles): chunks that fit in one of its arrays, so that neither
+// direction allocates device memory.
+namespace {
+kern::ParticleArrays offset_view(kern::ParticleArrays p, uint32_t off) {
+  return kern::ParticleArrays{p.cell + off, p.ox + off, p.oy + off, p.vx + off, p.vy + off, p.vz + off};
+}
+}  // namespace
+
+uint32_t Particle::stage_records() const {
+  return uint32_t(std::max<size_t>(1, size_t(pNumMax) * sizeof(int32_t) / sizeof(kern::ParticleStateAoS)));
+}
+
 void Particle::upload_aos(const kern::ParticleStateAoS* host, uint32_t n) {
   if (n > pNumMax) throw std::invalid_argument("pNum > pNumMax");
-  if (n) {
-    DeviceArray<kern::ParticleStateAoS> tmp(n);
-    GP_CUDA(cudaMemcpyAsync(tmp.get(), host, size_t(n) * sizeof(*host), cudaMemcpyHostToDevice, stream));
-    kern::aos_to_soa(tmp.get(), n, arrays(), stream);
-    GP_CUDA(cudaStreamSynchronize(stream));
+  auto* stage = reinterpret_cast<kern::ParticleStateAoS*>(buf[1 - cur].cell.get());
+  const uint32_t chunk = stage_records();
+  for (uint32_t off = 0; off < n; off += chunk) {
+    const uint32_t m = std::min(chunk, n - off);
+    GP_CUDA(cudaMemcpyAsync(stage, host + off, size_t(m) * sizeof(*host), cudaMemcpyHostToDevice, stream));
+    kern::aos_to_soa(stage, m, offset_view(arrays(), off), stream);
   }
+  GP_CUDA(cudaStreamSynchronize(stream));
   setPNum(n);
   needs_sort = true;
 }
 
 void Particle::download_aos(kern::ParticleStateAoS* host, uint32_t n) {
   if (!n) return;
-  DeviceArray<kern::ParticleStateAoS> tmp(n);
-  kern::soa_to_aos(arrays(), n, tmp.get(), stream);
-  GP_CUDA(cudaMemcpyAsync(host, tmp.get(), size_t(n) * sizeof(*host), cudaMemcpyDeviceToHost, stream));
+  auto* stage = reinterpret_cast<kern::ParticleStateAoS*>(buf[1 - cur].cell.get());
+  const uint32_t chunk = stage_records();
+  for (uint32_t off = 0; off < n; off += chunk) {
+    const uint32_t m = std::min(chunk, n - off);
+    kern::soa_to_aos(offset_view(arrays(), off), m, stage, stream);
+    GP_CUDA(cudaMemcpyAsync(host + off, stage, size_t(m) * sizeof(*host), cudaMemcpyDeviceToHost, stream));
+  }
   GP_CUDA(cudaStreamSynchronize(stream));
 }
 
