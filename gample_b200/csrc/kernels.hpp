@@ -105,6 +105,11 @@ size_t sort_key_count(GridDims g);
 size_t sort_scratch_words(GridDims g);
 void sort_by_cell(GridDims g, ParticleArrays src, ParticleArrays dst, const SpeciesCounters* counters,
                   uint32_t* scratch, uint32_t n_bound, cudaStream_t s);
+// The same order for particles in random order, in place in p: whole records
+// are scattered into spare (arrays of capacity words each) and converted
+// back. Returns false (nothing launched) when the records do not fit.
+bool sort_by_cell_staged(GridDims g, ParticleArrays p, ParticleArrays spare, uint32_t capacity,
+                         const SpeciesCounters* counters, uint32_t* scratch, uint32_t n_bound, cudaStream_t s);
 
 // Remove flagged particles, filling each hole (ascending) with the last
 // live particle (descending) -- the permutation of src/Particle.mm:893-966.

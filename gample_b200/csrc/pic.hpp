@@ -169,6 +169,7 @@ class Particle {
   // buffer, then swap). The order of particles is otherwise unspecified.
   void sort();
   bool needs_sort = true;
+  bool random_order = true;  // particles not yet sorted since loading / upload
   int sort_interval = 0;  // cycles between sorts; 0 = when too many chunks miss their window
   int cycles_since_sort = 0;
   uint32_t slow_after_sort = 0;  // particles pushed outside their window right after the last sort

@@ -114,6 +114,7 @@ void Particle::upload_aos(const kern::ParticleStateAoS* host, uint32_t n) {
   GP_CUDA(cudaStreamSynchronize(stream));
   setPNum(n);
   needs_sort = true;
+  random_order = true;
 }
 
 void Particle::download_aos(kern::ParticleStateAoS* host, uint32_t n) {
@@ -129,8 +130,13 @@ void Particle::download_aos(kern::ParticleStateAoS* host, uint32_t n) {
 }
 
 void Particle::sort() {
-  kern::sort_by_cell(dims_, buf[cur].view(), buf[1 - cur].view(), cnt.get(), sort_scratch.get(), n_bound, stream);
-  cur = 1 - cur;
+  // freshly loaded or uploaded particles are in random order: staged records
+  if (!(random_order && kern::sort_by_cell_staged(dims_, buf[cur].view(), buf[1 - cur].view(), pNumMax, cnt.get(),
+                                                  sort_scratch.get(), n_bound, stream))) {
+    kern::sort_by_cell(dims_, buf[cur].view(), buf[1 - cur].view(), cnt.get(), sort_scratch.get(), n_bound, stream);
+    cur = 1 - cur;
+  }
+  random_order = false;
   needs_sort = false;
   cycles_since_sort = 0;
 }

@@ -6,6 +6,15 @@
 // histogram (warp-aggregated atomics: lanes with equal keys add once),
 // exclusive scan of the counts, scatter into the spare buffer (slots claimed
 // with warp-aggregated atomics). The order inside a cell is unspecified.
+//
+// Particles in random order (just loaded or uploaded) take a staged scatter
+// instead: each particle's six SoA words land in different 32-byte sectors
+// when written one by one to random slots, so the staged path writes whole
+// 24-byte records into the spare buffer (its six arrays used as chunks of
+// records) and then converts the records back to SoA with coalesced
+// accesses, about half the DRAM traffic of the direct scatter for random
+// input. Nearly sorted particles (the periodic re-sort) keep the direct
+// scatter, whose writes are already coalesced.
 #include <cuda_runtime.h>
 
 #include "device.hpp"
@@ -151,6 +160,60 @@ __global__ void __launch_bounds__(kThreads) k_cs_scatter(ParticleArrays src, Par
   }
 }
 
+// One particle as a 24-byte record (8-byte aligned: three 64-bit stores).
+struct __align__(8) Record {
+  int32_t cell;
+  float ox, oy, vx, vy, vz;
+};
+struct RecordChunks {  // slot s: chunk s / per, record s % per
+  Record* c[6];
+  uint32_t per;
+};
+
+__global__ void __launch_bounds__(kThreads) k_cs_scatter_rec(ParticleArrays src, RecordChunks dst,
+                                                             const SpeciesCounters* cnt, KeyGeom g,
+                                                             uint32_t* offsets) {
+  const uint32_t n = cnt->n;
+  const int lane = threadIdx.x & 31;
+  const unsigned lt = (1u << lane) - 1u;
+  for (uint32_t base = (blockIdx.x * kThreads + threadIdx.x) & ~31u; base < n; base += gridDim.x * kThreads) {
+    const uint32_t k = base + lane;
+    const int32_t c = k < n ? src.cell[k] : 0;
+    const uint32_t key = k < n ? cell_key(c, g) : kNoKey;
+    const unsigned peers = __match_any_sync(0xffffffffu, key);
+    const int leader = __ffs(peers) - 1;
+    uint32_t slot = 0;
+    if (key != kNoKey && lane == leader) slot = atomicAdd(&offsets[key], uint32_t(__popc(peers)));
+    slot = __shfl_sync(0xffffffffu, slot, leader) + uint32_t(__popc(peers & lt));
+    if (key != kNoKey) {
+      Record r;
+      r.cell = c;
+      r.ox = src.ox[k];
+      r.oy = src.oy[k];
+      r.vx = src.vx[k];
+      r.vy = src.vy[k];
+      r.vz = src.vz[k];
+      const uint32_t q = slot / dst.per;
+      dst.c[q][slot - q * dst.per] = r;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) k_records_to_soa(RecordChunks in, const SpeciesCounters* cnt,
+                                                             ParticleArrays out) {
+  const uint32_t n = cnt->n;
+  for (uint32_t k = blockIdx.x * kThreads + threadIdx.x; k < n; k += gridDim.x * kThreads) {
+    const uint32_t q = k / in.per;
+    const Record r = in.c[q][k - q * in.per];
+    out.cell[k] = r.cell;
+    out.ox[k] = r.ox;
+    out.oy[k] = r.oy;
+    out.vx[k] = r.vx;
+    out.vy[k] = r.vy;
+    out.vz[k] = r.vz;
+  }
+}
+
 KeyGeom geom(GridDims g) {
   KeyGeom k;
   k.ntx = (g.nx + kTile) / kTile;
@@ -179,6 +242,39 @@ size_t sort_key_count(GridDims g) { return size_t(geom(g).nkeys) + 1; }
 size_t sort_scratch_words(GridDims g) {
   const size_t nk = sort_key_count(g);
   return 2 * nk + (nk + kScanChunk - 1) / kScanChunk + 32;
+}
+
+bool sort_by_cell_staged(GridDims g, ParticleArrays p, ParticleArrays spare, uint32_t capacity,
+                         const SpeciesCounters* cnt, uint32_t* scratch, uint32_t n_bound, cudaStream_t s) {
+  RecordChunks rc;
+  rc.per = uint32_t(size_t(capacity) * sizeof(int32_t) / sizeof(Record));
+  if (n_bound == 0 || rc.per == 0 || size_t(n_bound) > 6 * size_t(rc.per)) return false;
+  rc.c[0] = reinterpret_cast<Record*>(spare.cell);
+  rc.c[1] = reinterpret_cast<Record*>(spare.ox);
+  rc.c[2] = reinterpret_cast<Record*>(spare.oy);
+  rc.c[3] = reinterpret_cast<Record*>(spare.vx);
+  rc.c[4] = reinterpret_cast<Record*>(spare.vy);
+  rc.c[5] = reinterpret_cast<Record*>(spare.vz);
+  const KeyGeom kg = geom(g);
+  const uint32_t nk = kg.nkeys + 1;
+  uint32_t* counts = scratch;
+  uint32_t* offsets = scratch + nk;
+  uint32_t* sums = scratch + 2 * size_t(nk);
+  const uint32_t nb = (nk + kScanChunk - 1) / kScanChunk;
+  GP_CUDA(cudaMemsetAsync(counts, 0, size_t(nk) * sizeof(uint32_t), s));
+  k_cs_hist<<<grid_for(n_bound), kThreads, 0, s>>>(p.cell, cnt, kg, counts);
+  GP_LAUNCH_CHECK();
+  k_scan_local<<<nb, kScanThreads, 0, s>>>(counts, offsets, sums, nk);
+  GP_LAUNCH_CHECK();
+  k_scan_sums<<<1, kScanThreads, 0, s>>>(sums, nb);
+  GP_LAUNCH_CHECK();
+  k_scan_add<<<(nk + 255) / 256, 256, 0, s>>>(offsets, sums, nk);
+  GP_LAUNCH_CHECK();
+  k_cs_scatter_rec<<<grid_for(n_bound), kThreads, 0, s>>>(p, rc, cnt, kg, offsets);
+  GP_LAUNCH_CHECK();
+  k_records_to_soa<<<grid_for(n_bound), kThreads, 0, s>>>(rc, cnt, p);
+  GP_LAUNCH_CHECK();
+  return true;
 }
 
 void sort_by_cell(GridDims g, ParticleArrays src, ParticleArrays dst, const SpeciesCounters* cnt, uint32_t* scratch,
