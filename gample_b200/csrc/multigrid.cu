@@ -20,7 +20,7 @@ constexpr int kSmoothThreads = 256;
 constexpr int kSmallThreads = 1024;
 
 // state words (FP64): see multigrid.hpp
-enum { S_SUM = 0, S_SUM2, S_NORMB, S_REL, S_DONE, S_ITER, S_MEAN, S_REL0, S_COUNT };
+enum { S_SUM = 0, S_SUM2, S_NORMB, S_REL, S_DONE, S_ITER, S_MEAN, S_REL0, S_ZQ, S_PQ, S_RP, S_PQOLD, S_COUNT };
 
 // Boundary treatment of a direction: Dirichlet (values outside are zero),
 // periodic (wrap) or Neumann (mirror about the end node, i.e. the doubled
@@ -150,10 +150,48 @@ __global__ void k_clear_if_zero_rhs(double* x, int n, const double* st) {
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) x[k] = 0.0;
 }
 
-// r = b - A x in FP64 with the CSR row of src/EMField.mm:329-400 (diagonal,
-// i-1, i+1, j-1, j+1); stores float(r) and accumulates sum r, sum r^2.
+// (A v)_k in FP64 with the CSR row of src/EMField.mm:329-400 (diagonal,
+// i-1, i+1, j-1, j+1); v(k) returns the vector's entry k.
+template <class V>
+__device__ __forceinline__ double apply_A(const kern::PoissonLayout& L, int k, int i, int j, int mx, V v) {
+  const bool nx_ = L.fbc[0] == kern::FBC_NEUMANN_C, ny_ = L.fbc[2] == kern::FBC_NEUMANN_C;
+  double ax = L.Cd * v(k);
+  if (i > 0)
+    ax += L.Cx * v(k - 1);
+  else if (L.periodic_x)
+    ax += L.Cx * v(k + L.nkx);
+  else if (nx_ && L.nkx > 0)
+    ax += L.Cx * v(k + 1);
+  if (i < L.nkx)
+    ax += L.Cx * v(k + 1);
+  else if (L.periodic_x)
+    ax += L.Cx * v(k - L.nkx);
+  else if (nx_ && L.nkx > 0)
+    ax += L.Cx * v(k - 1);
+  if (j > 0)
+    ax += L.Cy * v(k - mx);
+  else if (L.periodic_y)
+    ax += L.Cy * v(k + L.nky * mx);
+  else if (ny_ && L.nky > 0)
+    ax += L.Cy * v(k + mx);
+  if (j < L.nky)
+    ax += L.Cy * v(k + mx);
+  else if (L.periodic_y)
+    ax += L.Cy * v(k - L.nky * mx);
+  else if (ny_ && L.nky > 0)
+    ax += L.Cy * v(k - mx);
+  return ax;
+}
+
+__device__ __forceinline__ double res_weight(const kern::PoissonLayout& L, int i, int j, int mx, int my) {
+  const bool nx_ = L.fbc[0] == kern::FBC_NEUMANN_C, ny_ = L.fbc[2] == kern::FBC_NEUMANN_C;
+  return double(bc_weight(i, mx, nx_ ? BC_NEU : BC_PER)) * bc_weight(j, my, ny_ ? BC_NEU : BC_PER);
+}
+
+// r = b - A x in FP64; stores r (r64, when given) and float(r) and
+// accumulates sum w r, sum r^2.
 __global__ void k_residual64(const double* __restrict__ x, const double* __restrict__ b, kern::PoissonLayout L,
-                             float* __restrict__ r32, double* st) {
+                             float* __restrict__ r32, double* __restrict__ r64, double* st) {
   __shared__ double sh[32];
   if (st[S_DONE] != 0.0) return;
   const int mx = L.nkx + 1, my = L.nky + 1, n = mx * my;
@@ -161,33 +199,10 @@ __global__ void k_residual64(const double* __restrict__ x, const double* __restr
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
     const int i = k % mx, j = k / mx;
     const bool nx_ = L.fbc[0] == kern::FBC_NEUMANN_C, ny_ = L.fbc[2] == kern::FBC_NEUMANN_C;
-    double ax = L.Cd * x[k];
-    if (i > 0)
-      ax += L.Cx * x[k - 1];
-    else if (L.periodic_x)
-      ax += L.Cx * x[k + L.nkx];
-    else if (nx_ && L.nkx > 0)
-      ax += L.Cx * x[k + 1];
-    if (i < L.nkx)
-      ax += L.Cx * x[k + 1];
-    else if (L.periodic_x)
-      ax += L.Cx * x[k - L.nkx];
-    else if (nx_ && L.nkx > 0)
-      ax += L.Cx * x[k - 1];
-    if (j > 0)
-      ax += L.Cy * x[k - mx];
-    else if (L.periodic_y)
-      ax += L.Cy * x[k + L.nky * mx];
-    else if (ny_ && L.nky > 0)
-      ax += L.Cy * x[k + mx];
-    if (j < L.nky)
-      ax += L.Cy * x[k + mx];
-    else if (L.periodic_y)
-      ax += L.Cy * x[k - L.nky * mx];
-    else if (ny_ && L.nky > 0)
-      ax += L.Cy * x[k - mx];
+    const double ax = apply_A(L, k, i, j, mx, [&](int q) { return x[q]; });
     const double r = b[k] - ax;
     r32[k] = float(r);
+    if (r64) r64[k] = r;
     const double w = double(bc_weight(i, mx, nx_ ? BC_NEU : BC_PER)) * bc_weight(j, my, ny_ ? BC_NEU : BC_PER);
     s1 += w * r;
     s2 += r * r;
@@ -200,8 +215,81 @@ __global__ void k_residual64(const double* __restrict__ x, const double* __restr
   }
 }
 
+// Flexible conjugate gradients with the V-cycle as preconditioner (one
+// retained direction, Notay's FCG(1)): z = M r, p = z + beta p_old with
+// beta = -(z.q_old) / (p_old.q_old), q = A p, alpha = (r.p) / (p.q),
+// x += alpha p, r -= alpha q. The orthogonalisation needs no symmetric or
+// exact preconditioner, so the FP32 V-cycle serves as it is; the first
+// iteration (S_ITER == 1) starts with p = z.
+__global__ void k_fcg_zq(const float* __restrict__ z, const double* __restrict__ q, int n, double* st) {
+  __shared__ double sh[32];
+  if (st[S_DONE] != 0.0 || st[S_ITER] == 1.0) return;
+  double a = 0.0;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) a += double(z[k]) * q[k];
+  a = block_sum(a, sh);
+  if (threadIdx.x == 0) atomicAdd(st + S_ZQ, a);
+}
+
+// p = z + beta p_old (into p), q = A p (neighbour values of p formed on the
+// fly from z and p_old, which no thread writes), dots p.q and r.p.
+__global__ void k_fcg_dir(const float* __restrict__ z, const double* __restrict__ p_old, double* __restrict__ p,
+                          double* __restrict__ q, const double* __restrict__ r, kern::PoissonLayout L, double* st) {
+  __shared__ double sh[32];
+  if (st[S_DONE] != 0.0) return;
+  const double beta = st[S_ITER] == 1.0 ? 0.0 : -st[S_ZQ] / st[S_PQOLD];
+  const int mx = L.nkx + 1, my = L.nky + 1, n = mx * my;
+  double pq = 0.0, rp = 0.0;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+    const int i = k % mx, j = k / mx;
+    auto pv = [&](int t) { return beta == 0.0 ? double(z[t]) : double(z[t]) + beta * p_old[t]; };
+    const double pk = pv(k);
+    const double qk = apply_A(L, k, i, j, mx, pv);
+    p[k] = pk;
+    q[k] = qk;
+    pq += pk * qk;
+    rp += r[k] * pk;
+  }
+  pq = block_sum(pq, sh);
+  rp = block_sum(rp, sh);
+  if (threadIdx.x == 0) {
+    atomicAdd(st + S_PQ, pq);
+    atomicAdd(st + S_RP, rp);
+  }
+  (void)my;
+}
+
+// x += alpha p, r -= alpha q; float(r) is the next V-cycle's right-hand
+// side; accumulates sum w r, sum r^2 for the convergence test.
+__global__ void k_fcg_update(double* __restrict__ x, const double* __restrict__ p, const double* __restrict__ q,
+                             double* __restrict__ r, float* __restrict__ r32, kern::PoissonLayout L, double* st) {
+  __shared__ double sh[32];
+  if (st[S_DONE] != 0.0) return;
+  const double alpha = st[S_PQ] != 0.0 ? st[S_RP] / st[S_PQ] : 0.0;
+  const int mx = L.nkx + 1, my = L.nky + 1, n = mx * my;
+  double s1 = 0.0, s2 = 0.0;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+    const int i = k % mx, j = k / mx;
+    x[k] += alpha * p[k];
+    const double rk = r[k] - alpha * q[k];
+    r[k] = rk;
+    r32[k] = float(rk);
+    s1 += res_weight(L, i, j, mx, my) * rk;
+    s2 += rk * rk;
+  }
+  s1 = block_sum(s1, sh);
+  s2 = block_sum(s2, sh);
+  if (threadIdx.x == 0) {
+    atomicAdd(st + S_SUM, s1);
+    atomicAdd(st + S_SUM2, s2);
+  }
+}
+
 // Convergence test (one thread): AMGCL's ||r|| / ||b|| <= tol or maxiter.
 __global__ void k_check(double* st, double tol, int maxiter, double wsum) {
+  st[S_PQOLD] = st[S_PQ];
+  st[S_PQ] = 0.0;
+  st[S_RP] = 0.0;
+  st[S_ZQ] = 0.0;
   if (st[S_DONE] != 0.0) return;
   const double rel = sqrt(st[S_SUM2] > 0 ? st[S_SUM2] : 0.0) / st[S_NORMB];
   st[S_REL] = rel;
@@ -368,10 +456,6 @@ __global__ void k_zero32(float* u, int n, const double* st) {
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) u[k] = 0.0f;
 }
 
-__global__ void k_add_x(double* x, const float* e, int n, const double* st) {
-  if (st[S_DONE] != 0.0) return;
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) x[k] += double(e[k]);
-}
 
 // ---------------------------------------------------------------- small levels
 struct SmallLevels {
@@ -721,7 +805,10 @@ PoissonMG::PoissonMG(const kern::PoissonLayout& L, int nu_pre, int nu_post)
     GP_CUDA(cudaFuncSetAttribute(k_small_vcycle, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  maxsm - int(fa.sharedSizeBytes)));
   });
-  x2_.resize(size_t(n_), true);
+  r64_.resize(size_t(n_), true);
+  q_.resize(size_t(n_), true);
+  p_[0].resize(size_t(n_), true);
+  p_[1].resize(size_t(n_), true);
   // Dense inverse of the coarsest operator (FP64 Gauss-Jordan, stored FP32);
   // a singular one (no Dirichlet direction) is regularised as A + a 1 w^T
   // with w its left null vector and a = |cd| / n, whose inverse returns the
@@ -864,13 +951,11 @@ MGResult PoissonMG::solve(const double* b, const double* sums_b, double* x, doub
   GP_LAUNCH_CHECK();
   k_clear_if_zero_rhs<<<blocks_for(n_), 256, 0, s>>>(x, n_, st);
   GP_LAUNCH_CHECK();
-  auto residual_and_check = [&]() {
-    k_residual64<<<blocks_for(n_), 256, 0, s>>>(x, b, L_, f.f.get(), st);
-    GP_LAUNCH_CHECK();
-    k_check<<<1, 1, 0, s>>>(st, tol, maxiter, singular_ ? wsum_ : double(n_));
-    GP_LAUNCH_CHECK();
-  };
-  residual_and_check();
+  const double wsum = singular_ ? wsum_ : double(n_);
+  k_residual64<<<blocks_for(n_), 256, 0, s>>>(x, b, L_, f.f.get(), r64_.get(), st);
+  GP_LAUNCH_CHECK();
+  k_check<<<1, 1, 0, s>>>(st, tol, maxiter, wsum);
+  GP_LAUNCH_CHECK();
   // Batches of V-cycles without host synchronisation; every kernel returns at
   // once after convergence. The batch size follows the last solve.
   int batch = last_iters_ > 0 ? last_iters_ : 1;
@@ -881,10 +966,18 @@ MGResult PoissonMG::solve(const double* b, const double* sums_b, double* x, doub
         k_sub_mean32<<<blocks_for(n_), 256, 0, s>>>(f.f.get(), n_, st);
         GP_LAUNCH_CHECK();
       }
-      vcycle(s);
-      k_add_x<<<blocks_for(n_), 256, 0, s>>>(x, result(0), n_, st);
+      vcycle(s);  // z = M r
+      const float* z = result(0);
+      double* p = p_[launched & 1].get();
+      const double* p_old = p_[(launched + 1) & 1].get();
+      k_fcg_zq<<<blocks_for(n_), 256, 0, s>>>(z, q_.get(), n_, st);
       GP_LAUNCH_CHECK();
-      residual_and_check();
+      k_fcg_dir<<<blocks_for(n_), 256, 0, s>>>(z, p_old, p, q_.get(), r64_.get(), L_, st);
+      GP_LAUNCH_CHECK();
+      k_fcg_update<<<blocks_for(n_), 256, 0, s>>>(x, p, q_.get(), r64_.get(), f.f.get(), L_, st);
+      GP_LAUNCH_CHECK();
+      k_check<<<1, 1, 0, s>>>(st, tol, maxiter, wsum);
+      GP_LAUNCH_CHECK();
     }
     GP_CUDA(cudaMemcpyAsync(host_.get(), st, S_COUNT * sizeof(double), cudaMemcpyDeviceToHost, s));
     GP_CUDA(cudaStreamSynchronize(s));

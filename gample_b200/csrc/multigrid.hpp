@@ -50,7 +50,9 @@ class PoissonMG {
   int unknowns() const { return n_; }
   int levels() const { return int(lv_.size()); }
   // b, x: device FP64 vectors of unknowns(); sums_b[0..1] = sum(b), sum(b^2)
-  // already on the device (from kern::build_rhs). x is updated in place.
+  // already on the device (from kern::build_rhs). x is updated in place by
+  // flexible conjugate gradients in FP64 preconditioned with one FP32 V-cycle
+  // per iteration, until ||b - A x|| / ||b|| <= tol.
   MGResult solve(const double* b, const double* sums_b, double* x, double tol, int maxiter, cudaStream_t s);
 
   struct Level {
@@ -78,7 +80,8 @@ class PoissonMG {
   int mx_top() const { return L_.nkx + 1; }
   int my_top() const { return L_.nky + 1; }
   std::vector<Level> lv_;
-  DeviceArray<double> x2_;      // ping-pong buffer of the FP64 update
+  DeviceArray<double> r64_, q_;  // FP64 residual and A p of the flexible CG iteration
+  DeviceArray<double> p_[2];      // search directions (current and previous, alternating)
   DeviceArray<float> coarse_inv_;  // dense inverse of the coarsest operator (small coarsest levels)
   DeviceArray<double> state_;   // [0] sum r [1] sum r^2 [2] ||b|| [3] rel res [4] done [5] iterations [6] mean r [7] initial rel res
   PinnedArray<double> host_;
