@@ -112,6 +112,7 @@ EXPORTS = {
     "gp_version": (C.c_char_p, []),
     "gp_device_count": (C.c_int, []),
     "gp_kernel_launches": (C.c_ulonglong, []),
+    "gp_release_cached_memory": (C.c_int, []),
 }
 
 
@@ -349,6 +350,11 @@ def device_count():
 
 def kernel_launches():
     return int(lib().gp_kernel_launches())
+
+
+def release_cached_memory():
+    """Return the device memory cached from closed simulations to the driver."""
+    check(lib().gp_release_cached_memory())
 
 
 class Net:

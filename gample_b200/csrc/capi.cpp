@@ -10,6 +10,9 @@
 #include "simulation.hpp"
 
 #include <atomic>
+#include <cstdint>
+#include <mutex>
+#include <set>
 
 namespace gample {
 namespace {
@@ -17,6 +20,42 @@ std::atomic<unsigned long long> g_launches{0};
 }
 void note_kernel_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 unsigned long long kernel_launches() { return g_launches.load(std::memory_order_relaxed); }
+
+namespace {
+std::mutex g_pool_mutex;
+std::set<int> g_pool_ready;  // devices whose default pool keeps freed memory
+cudaMemPool_t current_pool() {
+  int dev = 0;
+  GP_CUDA(cudaGetDevice(&dev));
+  cudaMemPool_t pool;
+  GP_CUDA(cudaDeviceGetDefaultMemPool(&pool, dev));
+  std::lock_guard<std::mutex> lk(g_pool_mutex);
+  if (!g_pool_ready.count(dev)) {
+    uint64_t keep = UINT64_MAX;
+    GP_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+    g_pool_ready.insert(dev);
+  }
+  return pool;
+}
+}  // namespace
+
+void* device_alloc(size_t bytes) {
+  void* p = nullptr;
+  GP_CUDA(cudaMallocFromPoolAsync(&p, bytes, current_pool(), 0));
+  GP_CUDA(cudaStreamSynchronize(0));
+  return p;
+}
+
+void device_free(void* p) {
+  // as cudaFree: no kernel may still use the block when it is reused
+  if (cudaDeviceSynchronize() != cudaSuccess) return;
+  cudaFreeAsync(p, 0);
+}
+
+void release_cached_device_memory() {
+  GP_CUDA(cudaDeviceSynchronize());
+  GP_CUDA(cudaMemPoolTrimTo(current_pool(), 0));
+}
 }  // namespace gample
 
 struct gp_init {
@@ -245,6 +284,12 @@ gp_status gp_nn_param(gp_nn* nn, int layer, int which, float* host, size_t count
 
 const char* gp_last_error(void) { return g_error.c_str(); }
 unsigned long long gp_kernel_launches(void) { return gample::kernel_launches(); }
+gp_status gp_release_cached_memory(void) {
+  return guarded([&] {
+    gample::release_cached_device_memory();
+    return GP_OK;
+  });
+}
 const char* gp_version(void) { return "gample_b200 0.1 (sm_100a)"; }
 int gp_device_count(void) {
   int n = 0;

@@ -34,6 +34,18 @@ unsigned long long kernel_launches();
     GP_CUDA(cudaGetLastError());       \
   } while (0)
 
+// Device memory comes from the current device's default stream-ordered pool
+// with an unbounded release threshold: a freed block stays with the process
+// and serves a later allocation of the same size without the driver mapping
+// (or, on free, unmapping) the memory again, which for the multi-GB particle
+// stores costs tens of milliseconds to seconds per simulation created or
+// closed. device_free() first waits for the device, as cudaFree does, since
+// the library's streams do not synchronise with the default stream.
+// release_cached_device_memory() returns the cached blocks to the driver.
+void* device_alloc(size_t bytes);
+void device_free(void* p);
+void release_cached_device_memory();
+
 // Owned device allocation of n elements of T (not initialised unless asked).
 template <typename T>
 class DeviceArray {
@@ -60,7 +72,7 @@ class DeviceArray {
   void resize(size_t n, bool zero = false) {
     release();
     if (n) {
-      GP_CUDA(cudaMalloc(&p_, n * sizeof(T)));
+      p_ = static_cast<T*>(device_alloc(n * sizeof(T)));
       n_ = n;
       if (zero) GP_CUDA(cudaMemset(p_, 0, n * sizeof(T)));
     }
@@ -68,8 +80,7 @@ class DeviceArray {
   // Grow to at least n elements keeping the first `keep` elements.
   void grow(size_t n, size_t keep, cudaStream_t s) {
     if (n <= n_) return;
-    T* q = nullptr;
-    GP_CUDA(cudaMalloc(&q, n * sizeof(T)));
+    T* q = static_cast<T*>(device_alloc(n * sizeof(T)));
     if (p_ && keep) GP_CUDA(cudaMemcpyAsync(q, p_, keep * sizeof(T), cudaMemcpyDeviceToDevice, s));
     GP_CUDA(cudaStreamSynchronize(s));
     release();
@@ -85,7 +96,7 @@ class DeviceArray {
 
  private:
   void release() {
-    if (p_) cudaFree(p_);
+    if (p_) device_free(p_);
     p_ = nullptr;
     n_ = 0;
   }

@@ -245,6 +245,12 @@ const char* gp_version(void);
 int gp_device_count(void);
 /* Kernels this library has launched since it was loaded (all runs). */
 unsigned long long gp_kernel_launches(void);
+/* Device memory of closed simulations stays cached in the process (the
+   current device's stream-ordered pool) so that the next simulation of a
+   similar size starts without the driver mapping gigabytes again; this
+   returns the cached memory of the current device to the driver. No
+   counterpart in the reference (it allocates Metal buffers per run). */
+gp_status gp_release_cached_memory(void);
 
 #ifdef __cplusplus
 }

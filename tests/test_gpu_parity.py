@@ -370,3 +370,27 @@ def test_sources_match_oracle(gpu):
         k = min(len(g), 64)
         np.testing.assert_allclose(np.sort(g["vz"][-k:]), np.sort(o["vz"][-k:]), rtol=1e-4,
                                    atol=1e-3 * np.max(np.abs(o["vz"])))
+
+
+@pytest.mark.gpu
+def test_cached_device_memory_is_reused_and_released(gpu):
+    """Closed simulations leave their device memory in the process's pool; the
+    next simulation reuses it, and gp_release_cached_memory hands it back
+    without disturbing a simulation created afterwards."""
+    cond = condition(ngx=32, ngy=24, order=3, ppc=8, deposit_mode=1, end=3)
+    out = []
+    for release in (False, True):
+        sim = capi.Sim(cond)
+        sim.initialize()
+        sim.run(3)
+        out.append(as_set(sim.particles(0)))
+        sim.close()
+        if release:
+            capi.release_cached_memory()
+    sim = capi.Sim(cond)
+    sim.initialize()
+    sim.run(3)
+    out.append(as_set(sim.particles(0)))
+    sim.close()
+    for o in out[1:]:
+        assert np.array_equal(o.view(np.uint8), out[0].view(np.uint8))
