@@ -9,21 +9,24 @@
 // right-hand side is projected with the left null vector (weight 1/2 at
 // Neumann ends) and the solution is returned with zero mean.
 //
-// Method: defect correction in FP64 around an FP32 V(2,2)-cycle.
+// Method: flexible conjugate gradients in FP64 (one retained direction,
+// FCG(1)) preconditioned by one FP32 V(2,2)-cycle per iteration.
 //   x (FP64, warm-started from the previous step like the reference's
-//   _phi_sol), r = b - A x in FP64, e = V-cycle(r) in FP32, x += e,
+//   _phi_sol), r = b - A x in FP64; per iteration z = V-cycle(r) in FP32,
+//   p = z + beta p_old with beta = -(z.A p_old) / (p_old.A p_old),
+//   alpha = (r.p) / (p.A p), x += alpha p, r -= alpha A p,
 //   until ||r||_2 / ||b||_2 <= tol (AMGCL's relative-residual criterion).
 // Levels: vertex-centred coarsening (Dirichlet n -> (n-1)/2, periodic
 // n -> n/2) while both directions allow it; red-black Gauss-Seidel,
 // full-weighting restriction, bilinear prolongation, re-discretised coarse
 // operators. Kernels per V-cycle:
-//   large levels (> kSmallPoints points): one pre-smoothing launch (two
-//     red-black sweeps in a shared-memory tile with a 4-point halo), one
-//     residual + restriction launch, one prolongation + post-smoothing launch;
+//   large levels (> kSmallPoints points): one launch for the pre-smoothing
+//     (two red-black sweeps in a shared-memory tile with a 6-point halo), the
+//     residual and its restriction, one prolongation + post-smoothing launch;
 //   all small levels: one single-CTA kernel running the rest of the V-cycle
 //     in shared memory; the coarsest level is solved by a precomputed dense
 //     inverse (by CG when it has more than 64 points).
-// The FP64 update + residual and the convergence test run on the device;
+// The FP64 CG passes and the convergence test run on the device;
 // the host synchronises once per solve (it batches as many V-cycles as the
 // previous solve needed and re-checks).
 #pragma once
