@@ -18,7 +18,15 @@ namespace gample {
 namespace {
 std::atomic<unsigned long long> g_launches{0};
 }
-void note_kernel_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+thread_local unsigned long long t_launches = 0;
+void note_kernel_launch() {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  ++t_launches;
+}
+unsigned long long thread_kernel_launches() { return t_launches; }
+void add_kernel_launches(long long n) {
+  g_launches.fetch_add(static_cast<unsigned long long>(n), std::memory_order_relaxed);
+}
 unsigned long long kernel_launches() { return g_launches.load(std::memory_order_relaxed); }
 
 namespace {

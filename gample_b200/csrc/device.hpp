@@ -27,7 +27,9 @@ struct CudaError : std::runtime_error {
 // Every kernel launch is followed by GP_LAUNCH_CHECK(), which also counts it
 // (gp_kernel_launches() in the C ABI).
 void note_kernel_launch();
+void add_kernel_launches(long long n);  // graph launches; negative to uncount captured kernels
 unsigned long long kernel_launches();
+unsigned long long thread_kernel_launches();  // launches issued by the calling host thread
 #define GP_LAUNCH_CHECK()              \
   do {                                 \
     ::gample::note_kernel_launch();    \

@@ -941,6 +941,86 @@ void PoissonMG::vcycle(cudaStream_t s) {
   }
 }
 
+// One FCG iteration (parity: which direction buffer is current).
+void PoissonMG::enqueue_iteration(int parity, double* x, double tol, int maxiter, cudaStream_t s) {
+  double* st = state_.get();
+  Level& f = lv_[0];
+  const double wsum = singular_ ? wsum_ : double(n_);
+  if (singular_) {
+    k_sub_mean32<<<blocks_for(n_), 256, 0, s>>>(f.f.get(), n_, st);
+    GP_LAUNCH_CHECK();
+  }
+  vcycle(s);  // z = M r
+  const float* z = result(0);
+  double* p = p_[parity].get();
+  const double* p_old = p_[parity ^ 1].get();
+  k_fcg_zq<<<blocks_for(n_), 256, 0, s>>>(z, q_.get(), n_, st);
+  GP_LAUNCH_CHECK();
+  k_fcg_dir<<<blocks_for(n_), 256, 0, s>>>(z, p_old, p, q_.get(), r64_.get(), L_, st);
+  GP_LAUNCH_CHECK();
+  k_fcg_update<<<blocks_for(n_), 256, 0, s>>>(x, p, q_.get(), r64_.get(), f.f.get(), L_, st);
+  GP_LAUNCH_CHECK();
+  k_check<<<1, 1, 0, s>>>(st, tol, maxiter, wsum);
+  GP_LAUNCH_CHECK();
+}
+
+// The two iteration graphs (even and odd parity) for this solution vector
+// and stopping rule, captured on first use in thread-local mode (other host
+// threads driving other simulations are not affected). Kernel launches are
+// counted when a graph is launched, not when it is captured. An empty result
+// (exec[0] == nullptr) means direct launches: the stream is already being
+// captured by the caller, or the capture failed.
+PoissonMG::IterationGraphs PoissonMG::iteration_graphs(double* x, double tol, int maxiter, cudaStream_t s) {
+  for (const auto& g : graphs_)
+    if (g.x == x && g.tol == tol && g.maxiter == maxiter) return g;
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  if (!graphs_ok_ || cudaStreamIsCapturing(s, &cap) != cudaSuccess || cap != cudaStreamCaptureStatusNone)
+    return IterationGraphs{};
+  IterationGraphs g{};
+  g.x = x;
+  g.tol = tol;
+  g.maxiter = maxiter;
+  const unsigned long long c0 = thread_kernel_launches();
+  bool ok = true;
+  for (int par = 0; par < 2 && ok; ++par) {
+    cudaGraph_t graph = nullptr;
+    if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+      ok = false;
+      break;
+    }
+    try {
+      enqueue_iteration(par, x, tol, maxiter, s);
+    } catch (...) {
+      ok = false;
+    }
+    if (cudaStreamEndCapture(s, &graph) != cudaSuccess || !graph) ok = false;
+    if (ok && cudaGraphInstantiate(&g.exec[par], graph, 0) != cudaSuccess) ok = false;
+    if (graph) cudaGraphDestroy(graph);
+  }
+  const unsigned long long captured = thread_kernel_launches() - c0;
+  add_kernel_launches(-static_cast<long long>(captured));
+  (void)cudaGetLastError();
+  if (!ok) {
+    for (auto& e : g.exec)
+      if (e) cudaGraphExecDestroy(e);
+    graphs_ok_ = false;
+    return IterationGraphs{};
+  }
+  g.kernels = static_cast<long long>(captured / 2);
+  if (graphs_.size() >= 4) {  // a few solution vectors per system (Poisson, Darwin parts, tests)
+    for (auto& e : graphs_.front().exec) cudaGraphExecDestroy(e);
+    graphs_.erase(graphs_.begin());
+  }
+  graphs_.push_back(g);
+  return g;
+}
+
+PoissonMG::~PoissonMG() {
+  for (auto& g : graphs_)
+    for (auto& e : g.exec)
+      if (e) cudaGraphExecDestroy(e);
+}
+
 MGResult PoissonMG::solve(const double* b, const double* sums_b, double* x, double tol, int maxiter,
                           cudaStream_t s) {
   MGResult res;
@@ -956,28 +1036,20 @@ MGResult PoissonMG::solve(const double* b, const double* sums_b, double* x, doub
   GP_LAUNCH_CHECK();
   k_check<<<1, 1, 0, s>>>(st, tol, maxiter, wsum);
   GP_LAUNCH_CHECK();
-  // Batches of V-cycles without host synchronisation; every kernel returns at
-  // once after convergence. The batch size follows the last solve.
+  // Batches of iterations without host synchronisation; every kernel returns
+  // at once after convergence. The batch size follows the last solve. An
+  // iteration is one CUDA graph launch when its graph could be captured.
+  const IterationGraphs gr = iteration_graphs(x, tol, maxiter, s);
   int batch = last_iters_ > 0 ? last_iters_ : 1;
   int launched = 0;
   for (;;) {
     for (int i = 0; i < batch && launched < maxiter; ++i, ++launched) {
-      if (singular) {
-        k_sub_mean32<<<blocks_for(n_), 256, 0, s>>>(f.f.get(), n_, st);
-        GP_LAUNCH_CHECK();
+      if (gr.exec[0]) {
+        GP_CUDA(cudaGraphLaunch(gr.exec[launched & 1], s));
+        add_kernel_launches(gr.kernels);
+      } else {
+        enqueue_iteration(launched & 1, x, tol, maxiter, s);
       }
-      vcycle(s);  // z = M r
-      const float* z = result(0);
-      double* p = p_[launched & 1].get();
-      const double* p_old = p_[(launched + 1) & 1].get();
-      k_fcg_zq<<<blocks_for(n_), 256, 0, s>>>(z, q_.get(), n_, st);
-      GP_LAUNCH_CHECK();
-      k_fcg_dir<<<blocks_for(n_), 256, 0, s>>>(z, p_old, p, q_.get(), r64_.get(), L_, st);
-      GP_LAUNCH_CHECK();
-      k_fcg_update<<<blocks_for(n_), 256, 0, s>>>(x, p, q_.get(), r64_.get(), f.f.get(), L_, st);
-      GP_LAUNCH_CHECK();
-      k_check<<<1, 1, 0, s>>>(st, tol, maxiter, wsum);
-      GP_LAUNCH_CHECK();
     }
     GP_CUDA(cudaMemcpyAsync(host_.get(), st, S_COUNT * sizeof(double), cudaMemcpyDeviceToHost, s));
     GP_CUDA(cudaStreamSynchronize(s));

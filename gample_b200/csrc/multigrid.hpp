@@ -50,6 +50,9 @@ struct MGResult {
 class PoissonMG {
  public:
   PoissonMG(const kern::PoissonLayout& L, int nu_pre = 2, int nu_post = 2);
+  ~PoissonMG();
+  PoissonMG(const PoissonMG&) = delete;
+  PoissonMG& operator=(const PoissonMG&) = delete;
   int unknowns() const { return n_; }
   int levels() const { return int(lv_.size()); }
   // b, x: device FP64 vectors of unknowns(); sums_b[0..1] = sum(b), sum(b^2)
@@ -70,6 +73,17 @@ class PoissonMG {
 
  private:
   void vcycle(cudaStream_t s);
+  void enqueue_iteration(int parity, double* x, double tol, int maxiter, cudaStream_t s);
+  struct IterationGraphs {
+    double* x = nullptr;
+    double tol = 0;
+    int maxiter = 0;
+    cudaGraphExec_t exec[2] = {nullptr, nullptr};
+    long long kernels = 0;  // kernels per graph launch
+  };
+  IterationGraphs iteration_graphs(double* x, double tol, int maxiter, cudaStream_t s);
+  std::vector<IterationGraphs> graphs_;
+  bool graphs_ok_ = true;
   const float* result(int l) const { return lv_[l].result_in_u2 ? lv_[l].u2.get() : lv_[l].u.get(); }
   kern::PoissonLayout L_;
   int n_;
