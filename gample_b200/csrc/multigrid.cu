@@ -482,7 +482,7 @@ __device__ __forceinline__ float nb_sum(const float* u, const LevelDesc& d, int 
   return d.cx * (l + r) + d.cy * (b + t);
 }
 
-__device__ void sb_smooth(float* u, const float* f, const LevelDesc& d, int color) {
+__device__ __forceinline__ void sb_smooth(float* u, const float* f, const LevelDesc& d, int color) {
   const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
   const int hx = (d.mx + 1) >> 1;
   const float inv = 1.0f / d.cd;
@@ -496,13 +496,20 @@ __device__ void sb_smooth(float* u, const float* f, const LevelDesc& d, int colo
   __syncthreads();
 }
 
-__device__ void sb_zero(float* u, const LevelDesc& d) {
-  for (int k = threadIdx.x; k < d.mx * d.my; k += kSmallThreads) u[k] = 0.0f;
+// The first red half-sweep from u = 0: every neighbour is zero, so the red
+// points become f / cd and the black ones stay zero (the same values as
+// zeroing u and sweeping, in one pass).
+__device__ __forceinline__ void sb_first_red(float* u, const float* f, const LevelDesc& d) {
+  const float inv = 1.0f / d.cd;
+  for (int k = threadIdx.x; k < d.mx * d.my; k += kSmallThreads) {
+    const int i = k % d.mx, j = k / d.mx;
+    u[k] = ((i + j) & 1) == 0 ? (f[k] - 0.0f) * inv : 0.0f;
+  }
   __syncthreads();
 }
 
 // r = f - A u, then full weighting of r onto the coarse right-hand side.
-__device__ void sb_restrict(const float* u, const float* f, float* r, const LevelDesc& d, float* fc,
+__device__ __forceinline__ void sb_restrict(const float* u, const float* f, float* r, const LevelDesc& d, float* fc,
                             const LevelDesc& c) {
   const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
   for (int j = ty; j < d.my; j += kRows)
@@ -533,7 +540,7 @@ __device__ void sb_restrict(const float* u, const float* f, float* r, const Leve
   __syncthreads();
 }
 
-__device__ void sb_prolong_add(float* u, const LevelDesc& d, const float* uc, const LevelDesc& c) {
+__device__ __forceinline__ void sb_prolong_add(float* u, const LevelDesc& d, const float* uc, const LevelDesc& c) {
   const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
   for (int j = ty; j < d.my; j += kRows)
     for (int i = tx; i < d.mx; i += 32) u[i + j * d.mx] += prolong_at(uc, c, d, i, j);
@@ -543,7 +550,7 @@ __device__ void sb_prolong_add(float* u, const LevelDesc& d, const float* uc, co
 // u = M (f - mean f) with M (in shared memory) the inverse of the coarsest
 // operator (of A + a 11^T for the doubly periodic one, whose zero-mean
 // solutions it returns).
-__device__ void sm_dense_solve(float* u, const float* f, const LevelDesc& d, const float* M, double* sh,
+__device__ __forceinline__ void sm_dense_solve(float* u, const float* f, const LevelDesc& d, const float* M, double* sh,
                                double* sval) {
   const int n = d.mx * d.my;
   const bool singular = d.bx != BC_DIR && d.by != BC_DIR;
@@ -583,7 +590,7 @@ __device__ void sm_dense_solve(float* u, const float* f, const LevelDesc& d, con
 // Neumann ends, making the operator symmetric; 1 otherwise). A singular
 // level (no Dirichlet direction) is solved in its range: f is projected with
 // the weights and u returned with zero mean.
-__device__ void sm_coarse_cg(float* u, const float* f, const LevelDesc& d, float* work, double* sh, double* sval) {
+__device__ __forceinline__ void sm_coarse_cg(float* u, const float* f, const LevelDesc& d, float* work, double* sh, double* sval) {
   const int n = d.mx * d.my;
   float* r = work;
   float* p = work + n;
@@ -662,6 +669,9 @@ __device__ void sm_coarse_cg(float* u, const float* f, const LevelDesc& d, float
 // The V-cycle of every small level in one CTA: f of the first small level is
 // read from global memory, its correction u written back (and added to the
 // FP64 solution when it is the finest level).
+// BX, BY: the boundary type of each direction (the same on every level), a
+// compile-time constant in the stencil code.
+template <int BX, int BY>
 __global__ void __launch_bounds__(kSmallThreads) k_small_vcycle(SmallLevels S, const float* __restrict__ f_in,
                                                                 float* __restrict__ u_out, double* x, int nu_pre,
                                                                 int nu_post, const double* st) {
@@ -669,7 +679,13 @@ __global__ void __launch_bounds__(kSmallThreads) k_small_vcycle(SmallLevels S, c
   __shared__ double sh[32];
   __shared__ double sval;
   if (st[S_DONE] != 0.0) return;
-  const LevelDesc& d0 = S.d[0];
+  auto level = [&](int l) {
+    LevelDesc d = S.d[l];
+    d.bx = BX;
+    d.by = BY;
+    return d;
+  };
+  const LevelDesc d0 = level(0);
   const int n0 = d0.mx * d0.my;
   for (int k = threadIdx.x; k < n0; k += blockDim.x) sm[S.off[0] + n0 + k] = f_in[k];
   if (S.cinv) {
@@ -680,19 +696,25 @@ __global__ void __launch_bounds__(kSmallThreads) k_small_vcycle(SmallLevels S, c
   __syncthreads();
   const int last = S.count - 1;
   for (int l = 0; l < last; ++l) {
-    const LevelDesc d = S.d[l];
-    const LevelDesc c = S.d[l + 1];
+    const LevelDesc d = level(l);
+    const LevelDesc c = level(l + 1);
     const int n = d.mx * d.my;
     float* u = sm + S.off[l];
-    sb_zero(u, d);
     for (int it = 0; it < nu_pre; ++it) {
-      sb_smooth(u, u + n, d, 0);
+      if (it == 0)
+        sb_first_red(u, u + n, d);
+      else
+        sb_smooth(u, u + n, d, 0);
       sb_smooth(u, u + n, d, 1);
+    }
+    if (nu_pre == 0) {
+      for (int k = threadIdx.x; k < n; k += kSmallThreads) u[k] = 0.0f;
+      __syncthreads();
     }
     sb_restrict(u, u + n, u + 2 * n, d, sm + S.off[l + 1] + c.mx * c.my, c);
   }
   {
-    const LevelDesc d = S.d[last];
+    const LevelDesc d = level(last);
     float* u = sm + S.off[last];
     if (S.cinv) {
       sm_dense_solve(u, u + d.mx * d.my, d, sm + S.cg_off, sh, &sval);
@@ -702,8 +724,8 @@ __global__ void __launch_bounds__(kSmallThreads) k_small_vcycle(SmallLevels S, c
     }
   }
   for (int l = last - 1; l >= 0; --l) {
-    const LevelDesc d = S.d[l];
-    const LevelDesc c = S.d[l + 1];
+    const LevelDesc d = level(l);
+    const LevelDesc c = level(l + 1);
     const int n = d.mx * d.my;
     float* u = sm + S.off[l];
     sb_prolong_add(u, d, sm + S.off[l + 1], c);
@@ -717,6 +739,15 @@ __global__ void __launch_bounds__(kSmallThreads) k_small_vcycle(SmallLevels S, c
     u_out[k] = v;
     if (x) x[k] += double(v);
   }
+}
+
+using SmallKernel = void (*)(SmallLevels, const float*, float*, double*, int, int, const double*);
+SmallKernel small_kernel(int bx, int by) {
+  static const SmallKernel table[9] = {
+      k_small_vcycle<BC_DIR, BC_DIR>, k_small_vcycle<BC_DIR, BC_PER>, k_small_vcycle<BC_DIR, BC_NEU>,
+      k_small_vcycle<BC_PER, BC_DIR>, k_small_vcycle<BC_PER, BC_PER>, k_small_vcycle<BC_PER, BC_NEU>,
+      k_small_vcycle<BC_NEU, BC_DIR>, k_small_vcycle<BC_NEU, BC_PER>, k_small_vcycle<BC_NEU, BC_NEU>};
+  return table[bx * 3 + by];
 }
 
 int blocks_for(int n) {
@@ -800,10 +831,12 @@ PoissonMG::PoissonMG(const kern::PoissonLayout& L, int nu_pre, int nu_post)
   // (ensemble members run concurrently): allow the device's maximum once.
   static std::once_flag once;
   std::call_once(once, [maxsm] {
-    cudaFuncAttributes fa{};
-    GP_CUDA(cudaFuncGetAttributes(&fa, k_small_vcycle));
-    GP_CUDA(cudaFuncSetAttribute(k_small_vcycle, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 maxsm - int(fa.sharedSizeBytes)));
+    for (int b = 0; b < 9; ++b) {
+      const SmallKernel k = small_kernel(b / 3, b % 3);
+      cudaFuncAttributes fa{};
+      GP_CUDA(cudaFuncGetAttributes(&fa, k));
+      GP_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm - int(fa.sharedSizeBytes)));
+    }
   });
   r64_.resize(size_t(n_), true);
   q_.resize(size_t(n_), true);
@@ -911,8 +944,8 @@ void PoissonMG::vcycle(cudaStream_t s) {
     }
     S.cg_off = int(off);
     S.cinv = coarse_inv_.size() ? coarse_inv_.get() : nullptr;
-    k_small_vcycle<<<1, kSmallThreads, small_smem_, s>>>(S, lv_[ls_].f.get(), lv_[ls_].u.get(), nullptr, nu_pre_,
-                                                        nu_post_, st);
+    small_kernel(bx_, by_)<<<1, kSmallThreads, small_smem_, s>>>(S, lv_[ls_].f.get(), lv_[ls_].u.get(), nullptr,
+                                                                 nu_pre_, nu_post_, st);
     GP_LAUNCH_CHECK();
     lv_[ls_].result_in_u2 = false;
   }
