@@ -97,6 +97,15 @@ def load_peaks():
         return 6650.0, "fallback"
 
 
+def load_tensor_peak():
+    """Sustained dense BF16 TFLOP/s of this pool's B200s (cuBLAS, seconds-long loop)."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["bf16_tflops_sustained"]), "measured"
+    except Exception:
+        return 1400.0, "fallback"
+
+
 def load_traffic():
     """DRAM bytes per pushed particle of the push kernel, from the committed ncu
     summary (a 64-ppc capture of the same kernel; traffic scales with the
@@ -173,6 +182,20 @@ NET_SPECS = [(2, 32, 0), (32, 32, 0), (32, 64, 1), (64, 64, 1), (64, 128, 2), (1
              (256, 256, 3), (384, 128, 2), (192, 64, 1), (96, 32, 0), (32, 1, 0)]
 
 
+def poisson_block(vcycles, unknowns, solve_ms, peak):
+    """The solve against its memory roofline: about 96 algorithmic bytes per
+    fine point per V(2,2) cycle (2 x 2 sweeps of 12 B, the 16-B FP64 residual
+    and 8 B of transfer, times 4/3 for the coarser levels)."""
+    per_cycle = 96.0 * unknowns
+    ms_cycle = solve_ms / vcycles if vcycles else None
+    achieved = per_cycle / (ms_cycle * 1e-3) / 1e9 if ms_cycle else None
+    return {"vcycles_last_step": vcycles, "tolerance": 1e-8, "solve_ms_per_step": solve_ms,
+            "ms_per_vcycle_incl_cg": ms_cycle, "algorithmic_bytes_per_vcycle": per_cycle,
+            "achieved_gbs": achieved, "frac_of_hbm": achieved / peak if achieved else None,
+            "note": "latency-bound: ~13 dependent launches per CG iteration (one CUDA graph), "
+                    "levels <= 4096 points in one CTA"}
+
+
 def learned_leg(cond, train_steps, eval_steps):
     """Poisson ms/step and V-cycles to the same 1e-8 residual from the plain
     warm start (previous phi) and from previous phi + the warm-start network,
@@ -206,6 +229,7 @@ def learned_leg(cond, train_steps, eval_steps):
             "start_residual_plain": mean("rel0_plain"), "start_residual_learned": mean("rel0_learned"),
             "speedup": mean("ms_plain") / mean("ms_learned"), "network_ms": ms_net,
             "network_tflops": flops / (ms_net * 1e-3) / 1e12 if ms_net > 0 else None,
+            "network_tensor_frac": (flops / (ms_net * 1e-3) / 1e12) / load_tensor_peak()[0] if ms_net > 0 else None,
             "network_gflop_per_forward": flops / 1e9, "train_steps": train_steps,
             "train_s": train_s, "loss_first": losses[0] if losses else None,
             "loss_last10": sum(losses[-10:]) / max(1, len(losses[-10:])), "eval_steps": eval_steps,
@@ -356,6 +380,7 @@ def run_b200(args):
         pg.all_reduce(t, op=pg.ReduceOp.MAX)
         ms_max = float(t.item())
     iters_last = sim.last_solve().iterations
+    unknowns = (sim.nkx + 1) * (sim.nky + 1)
     pushes_rank = 0.5 * (n0 + n1) * args.steps
     value = pushes_rank * world / (ms_max / 1e3)
 
@@ -447,7 +472,8 @@ def run_b200(args):
                 "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
                 "gpu_launches": launches, "gpu_launches_per_step": launches / args.steps,
-                "poisson": {"vcycles_last_step": iters_last, "tolerance": 1e-8}, "learned_warm_start": learned,
+                "poisson": poisson_block(iters_last, unknowns, roofline["phase_ms_per_step"]["solve"], peak),
+                "learned_warm_start": learned,
                 "ensemble": ensemble}
         print(json.dumps(line), flush=True)
     if pg:
