@@ -910,7 +910,9 @@ struct FlowStats {
 // src/Particle.mm:893-968. With `faithful`, the reference's extra pull when a
 // tail scan runs out of live particles (it re-counts the next, already
 // scanned, dead slot: :908-925 after :942-964) is reproduced; without it every
-// flagged particle is counted exactly once.
+// flagged particle is counted exactly once. When every particle is flagged
+// the tail scan has pulled all n and there is no slot left to re-count (the
+// reference would pull n + 1 and underflow pNum): the extra pull is skipped.
 template <typename R>
 FlowStats reduce_particles(Particles<R>& P, float q, bool faithful) {
   FlowStats fs;
@@ -930,7 +932,7 @@ FlowStats reduce_particles(Particles<R>& P, float q, bool faithful) {
   };
   for (int k1 = 0; k1 < n; k1++) {
     if (k1 >= kmax) {
-      if (faithful && P.piflag[k1] > 0) {
+      if (faithful && P.piflag[k1] > 0 && pulln < n) {
         pulln++;
         count(P.piflag[k1]);
       }
