@@ -88,6 +88,34 @@ def test_ragged_particle_counts_match_the_oracle(gpu, n):
     sim.close()
 
 
+@pytest.mark.parametrize("n", [5, 200_003])
+def test_upload_in_random_order_is_sorted_by_tile(gpu, n):
+    """Uploaded particles are in no particular order; initialize() sorts them
+    through the staged record scatter: the same particles come back, ordered
+    by 8x8 tile, then row and column inside the tile."""
+    cond = condition(ngx=40, ngy=24, order=1, ppc=2, xbc="periodic", ybc="Dirichlet", pnum_max=250_000)
+    sim = capi.Sim(cond)
+    rng = np.random.default_rng(n)
+    x = rng.uniform(0, 40, n).astype(np.float32)
+    y = rng.uniform(0.5, 23.5, n).astype(np.float32)
+    v = rng.normal(0.0, 1e5, (3, n)).astype(np.float32)
+    for s in range(2):
+        sim.set_particles(s, _records(x, y, v[0], v[1], v[2]))
+    before = [sim.particles_raw(s) for s in range(2)]
+    sim.initialize()
+    cols = ("cell", "ox", "oy", "vx", "vy", "vz")
+    for s in range(2):
+        after = sim.particles_raw(s)
+        assert len(after["cell"]) == n
+        ix, iy = after["cell"] & 0xFFFF, after["cell"] >> 16
+        key = (((iy // 8).astype(np.int64) * 4096 + ix // 8) * 8 + iy % 8) * 8 + ix % 8
+        assert np.all(np.diff(key) >= 0)
+        as_bits = lambda d: np.stack([d[c].view(np.uint32) for c in cols])
+        a, b = as_bits(before[s]), as_bits(after)
+        np.testing.assert_array_equal(a[:, np.lexsort(a[::-1])], b[:, np.lexsort(b[::-1])])
+    sim.close()
+
+
 def test_upload_beyond_the_capacity_is_an_error(gpu):
     cond = condition(ngx=16, ngy=16, order=1, ppc=2, pnum_max=1000)
     sim = capi.Sim(cond)
