@@ -37,6 +37,8 @@ constexpr int kWin = 1600;                   // entries of a shared-memory windo
 constexpr int kMargin = 2;                   // deposit-window margin for the motion of one step (cells)
 constexpr int kReach = 12;                   // window box: cells within kReach of the chunk's middle particle
 constexpr size_t kDepositBudget = 98304;     // shared-memory bytes for the deposit window copies
+constexpr int kPW = 20;                      // row stride of a lane-private deposit window (entries)
+constexpr int kPrivWords = 10752;            // words for 32 lane-private windows (42 KB)
 
 __device__ __forceinline__ uint32_t warp_sum(uint32_t v) { return __reduce_add_sync(0xffffffffu, v); }
 __device__ __forceinline__ double warp_sum(double v) {
@@ -86,6 +88,8 @@ struct Window {  // shared-memory windows of one CTA (array-index coordinates)
   int gx0, gy0, gw, gh;  // gather window (origin, size)
   int dx0, dy0, dw, dh;  // deposit window
   int ds;                // deposit window row stride (>= dw, congruent to ORDER + 1 mod 32)
+  int priv;              // 1: 32 lane-private deposit windows, row stride kPW
+  int ps;                // their copy stride (odd, >= kPW * dh)
 };
 
 // r[t] = w[(t + sh) mod N] for a per-lane shift sh in [0, N).
@@ -156,12 +160,17 @@ struct DepositLayout {
   }
   static constexpr int kCopies = copies();
   static constexpr int kArrayBytes = kCopies * kStride * int(sizeof(int));  // one array, all copies
-  static constexpr size_t kBytes = size_t(kCopies) * kCopyBytes;
+  static constexpr size_t kSharedBytes = size_t(kCopies) * kCopyBytes;
+  // the single-word layout may also hold 32 lane-private windows (kPrivWords)
+  static constexpr size_t kBytes =
+      kSingle && size_t(kPrivWords) * sizeof(int) > kSharedBytes ? size_t(kPrivWords) * sizeof(int) : kSharedBytes;
   // single word: a copy receives at most kChunk / kCopies contributions per
   // node, each at most the largest stencil weight (1, (2/3)^2, (11/20)^2)
   static constexpr double kMaxW = ORDER == 1 ? 1.0 : (ORDER == 3 ? 0.4445 : 0.3026);
   static_assert(!kSingle || double(kChunk / kCopies) * kMaxW * double(1 << kQBits) < 2147483647.0,
                 "single-word deposit window could overflow");
+  static_assert(!kSingle || 32.0 * kPer * kMaxW * double(1 << kQBits) < 2147483647.0,
+                "sum of the 32 lane-private windows could overflow");
 };
 
 // This lane's copy of the window arrays: shared-memory byte address of its rho
@@ -284,6 +293,36 @@ __device__ __forceinline__ void deposit_one(const GridDims& g, const Window& w, 
         }
     }
   }
+}
+
+// Lane-private single-word windows: when 32 copies of a small deposit window
+// fit, lane L adds into its own copy at L * ps words (ps odd, so lanes adding
+// to the same node of their copies hit 32 distinct banks). No stencil
+// rotation is needed, and every node offset is a compile-time immediate of
+// the row stride kPW. A copy receives at most kPer contributions per node.
+// The products rn(wx * 2^kQBits * wy) are those of the shared layout, so the
+// integer window sums are the same.
+template <int N, int K = 0>
+__device__ __forceinline__ void priv_add(uint32_t a0, const float (&rx)[N], const float (&ry)[N]) {
+  if constexpr (K < N * N) {
+    asm volatile("red.shared.add.s32 [%0+%1], %2;" ::"r"(a0), "n"(4 * (K % N + (K / N) * kPW)),
+                 "r"(__float2int_rn(__fmul_rn(rx[K % N], ry[K / N])))
+                 : "memory");
+    priv_add<N, K + 1>(a0, rx, ry);
+  }
+}
+
+template <int ORDER>
+__device__ __forceinline__ void deposit_priv(const Window& w, uint32_t lane_base, int ngb, const Stagger& sx,
+                                             const Stagger& sy, const float (&wxn)[ORDER + 1],
+                                             const float (&wyn)[ORDER + 1]) {
+  constexpr int N = ORDER + 1;
+  constexpr float kUnit = float(1 << DepositLayout<ORDER, false, false>::kQBits);
+  float rx[N];
+#pragma unroll
+  for (int t = 0; t < N; ++t) rx[t] = __fmul_rn(wxn[t], kUnit);
+  const uint32_t a0 = lane_base + 4u * uint32_t((sx.node - ngb - w.dx0) + (sy.node - ngb - w.dy0) * kPW);
+  priv_add<N>(a0, rx, wyn);
 }
 
 // Gather Ex, Ey (and Bz) for one particle (src/Particle.mm:142-154).
@@ -485,6 +524,8 @@ __global__ void __launch_bounds__(kThreads, ORDER == 5 ? 2 : (PUSH && (!BZU || !
       w.mxy = max(w.mxy, s_red[3][q]);
     }
     w.use = 0;
+    w.priv = 0;
+    w.ps = 1;
     if (w.mnx != INT_MAX) {
       w.gx0 = w.mnx - ngb;
       w.gy0 = w.mny - ngb;
@@ -497,11 +538,15 @@ __global__ void __launch_bounds__(kThreads, ORDER == 5 ? 2 : (PUSH && (!BZU || !
       w.dh = w.gh + 2 * m;
       w.ds = w.dw + (((ORDER + 1 - w.dw) % 32) + 32) % 32;
       w.use = (w.ds * w.dh <= kWin && w.gw * w.gh <= kWin) ? 1 : 0;
+      w.priv = 0;
+      w.ps = (kPW * w.dh) | 1;
+      if (DEP && DL::kSingle && w.use && w.dw <= kPW && 32 * w.ps + 3 <= kPrivWords) w.priv = 1;
     }
     s_w = w;
   }
   __syncthreads();
   const Window w = s_w;
+  const uint32_t priv_base = static_cast<uint32_t>(__cvta_generic_to_shared(sDep)) + 4u * uint32_t(lane * w.ps);
 
   // ---- phase B: stage the field window, clear the deposit window
   if (w.use) {
@@ -515,9 +560,14 @@ __global__ void __launch_bounds__(kThreads, ORDER == 5 ? 2 : (PUSH && (!BZU || !
       }
     }
     if constexpr (DEP) {
-      const int used = w.ds * w.dh;
-      for (int e = tid; e < DL::kArrays * DL::kCopies * used; e += kThreads)
-        sDep[(e / used) * DL::kStride + e % used] = 0;
+      if (w.priv) {
+        int4* z = reinterpret_cast<int4*>(sDep);  // 32 * ps rounded up to 4 words stays within kPrivWords
+        for (int e = tid; e < (32 * w.ps + 3) / 4; e += kThreads) z[e] = make_int4(0, 0, 0, 0);
+      } else {
+        const int used = w.ds * w.dh;
+        for (int e = tid; e < DL::kArrays * DL::kCopies * used; e += kThreads)
+          sDep[(e / used) * DL::kStride + e % used] = 0;
+      }
     }
   }
   __syncthreads();
@@ -574,7 +624,9 @@ __global__ void __launch_bounds__(kThreads, ORDER == 5 ? 2 : (PUSH && (!BZU || !
             vx = l_vx;
             vy = l_vy;
           }
-          if (in_box_win && sublight<CUR>(vx, vy))
+          if (DL::kSingle && in_box_win && w.priv)
+            deposit_priv<ORDER>(w, priv_base, ngb, sx, sy, wxn, wyn);
+          else if (in_box_win && sublight<CUR>(vx, vy))
             deposit_one<ORDER, DET, CUR, true, false>(g, w, lane, sx, sy, wxn, wxh, wyn, wyh, c.scale, vx, vy, d, sw);
           else if (inside)
             deposit_one<ORDER, DET, CUR, false, false>(g, w, lane, sx, sy, wxn, wxh, wyn, wyh, c.scale, vx, vy, d, sw);
@@ -661,7 +713,9 @@ __global__ void __launch_bounds__(kThreads, ORDER == 5 ? 2 : (PUSH && (!BZU || !
               }
               const bool in_win = w.use && ix >= w.mnx - kMargin && ix <= w.mxx + kMargin &&
                                   iy >= w.mny - kMargin && iy <= w.mxy + kMargin;
-              if (in_win && sublight<CUR>(vx, vy))
+              if (DL::kSingle && in_win && w.priv)
+                deposit_priv<ORDER>(w, priv_base, ngb, nsx, nsy, wxn, wyn);
+              else if (in_win && sublight<CUR>(vx, vy))
                 deposit_one<ORDER, DET, CUR, true, false>(g, w, lane, nsx, nsy, wxn, wxh, wyn, wyh, c.scale, vx, vy, d,
                                                           sw);
               else
@@ -686,7 +740,19 @@ __global__ void __launch_bounds__(kThreads, ORDER == 5 ? 2 : (PUSH && (!BZU || !
   // ---- phase D: flush the deposit window
   if constexpr (DEP) {
     __syncthreads();
-    if (w.use) {
+    if (DL::kSingle && w.priv) {
+      const int nx = g.nx, ny = g.ny;
+      const double fr = double(c.scale) / double(1 << DL::kQBits);
+      for (int e = tid; e < kPW * w.dh; e += kThreads) {
+        const int cc = e % kPW;
+        if (cc >= w.dw) continue;
+        const int col = w.dx0 + cc, row = w.dy0 + e / kPW;
+        int r = 0;  // at most 32 * kPer contributions: no overflow (DepositLayout)
+#pragma unroll 8
+        for (int q = 0; q < 32; ++q) r += sDep[q * w.ps + e];
+        if (r != 0 && in_box(col, row, nx + 1, ny + 1)) atomicAdd(d.f64_rho + col + row * (nx + 1), double(r) * fr);
+      }
+    } else if (w.use) {
       const int nx = g.nx, ny = g.ny;
       for (int e = tid; e < w.ds * w.dh; e += kThreads) {
         if (e % w.ds >= w.dw) continue;  // stride padding, never written
