@@ -178,6 +178,26 @@ def test_deposit_atomic_dense_cells_error_bound(gpu):
     assert rel_inf(got, ref) < 2e-7
 
 
+@pytest.mark.parametrize("order", [1, 3, 5])
+def test_fused_deposit_dense_cells_matches_fp64(gpu, order):
+    """256 particles per cell on a small grid: a 2048-particle chunk covers a
+    few cells, so the fused push + deposit accumulates in lane-private
+    windows. The charge of the pushed particles matches the oracle's FP64
+    deposit of the same particles."""
+    cond = condition(ngx=16, ngy=16, order=order, ppc=256, xbc="periodic", ybc="periodic", te=10.0,
+                     bz_tesla=0.02, dt=1e-11)
+    sim, ora = pair(cond, real64=True)
+    sim.reset_charge()
+    sim.update(0, cond["ParamForTimeIntegration"]["TimeStep"], fused_deposit=True)
+    g = sim.particles(0)
+    live = g["piflag"] == 0
+    assert np.count_nonzero(live) > 0.99 * len(g)
+    ora.set_particles(0, g["x"][live], g["y"][live], g["vx"][live], g["vy"][live], g["vz"][live])
+    ora.reset_charge()
+    ora.deposit(0)
+    assert rel_inf(sim.field("rho"), ora.field("rho")) < 2e-7
+
+
 def combine_fixed(accs, scales, extra=1.0):
     v = np.zeros(accs[0].shape, np.float64)
     for a, s in zip(accs, scales):
