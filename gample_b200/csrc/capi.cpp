@@ -11,6 +11,7 @@
 
 #include <atomic>
 #include <cstdint>
+#include <map>
 #include <mutex>
 #include <set>
 
@@ -60,9 +61,37 @@ void device_free(void* p) {
   cudaFreeAsync(p, 0);
 }
 
+namespace {
+std::mutex g_pinned_mutex;
+std::multimap<size_t, void*> g_pinned_free;  // kept page-locked blocks by size
+}  // namespace
+
+void* pinned_alloc(size_t bytes) {
+  {
+    std::lock_guard<std::mutex> lk(g_pinned_mutex);
+    auto it = g_pinned_free.find(bytes);
+    if (it != g_pinned_free.end()) {
+      void* p = it->second;
+      g_pinned_free.erase(it);
+      return p;
+    }
+  }
+  void* p = nullptr;
+  GP_CUDA(cudaMallocHost(&p, bytes));
+  return p;
+}
+
+void pinned_free(void* p, size_t bytes) {
+  std::lock_guard<std::mutex> lk(g_pinned_mutex);
+  g_pinned_free.emplace(bytes, p);
+}
+
 void release_cached_device_memory() {
   GP_CUDA(cudaDeviceSynchronize());
   GP_CUDA(cudaMemPoolTrimTo(current_pool(), 0));
+  std::lock_guard<std::mutex> lk(g_pinned_mutex);
+  for (auto& b : g_pinned_free) cudaFreeHost(b.second);
+  g_pinned_free.clear();
 }
 }  // namespace gample
 

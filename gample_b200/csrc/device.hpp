@@ -48,6 +48,13 @@ void* device_alloc(size_t bytes);
 void device_free(void* p);
 void release_cached_device_memory();
 
+// Page-locked host memory for the small diagnostics read-backs. Freed blocks
+// are kept per size and handed out again: cudaMallocHost costs 1-3 ms per
+// call, which every simulation created would pay for each of its read-back
+// buffers. release_cached_device_memory() frees the kept blocks as well.
+void* pinned_alloc(size_t bytes);
+void pinned_free(void* p, size_t bytes);
+
 // Owned device allocation of n elements of T (not initialised unless asked).
 template <typename T>
 class DeviceArray {
@@ -113,15 +120,16 @@ class PinnedArray {
   PinnedArray() = default;
   explicit PinnedArray(size_t n) { resize(n); }
   ~PinnedArray() {
-    if (p_) cudaFreeHost(p_);
+    if (p_) pinned_free(p_, n_ * sizeof(T));
   }
   PinnedArray(const PinnedArray&) = delete;
   PinnedArray& operator=(const PinnedArray&) = delete;
   void resize(size_t n) {
-    if (p_) cudaFreeHost(p_);
+    if (p_) pinned_free(p_, n_ * sizeof(T));
     p_ = nullptr;
+    n_ = 0;
+    if (n) p_ = static_cast<T*>(pinned_alloc(n * sizeof(T)));
     n_ = n;
-    if (n) GP_CUDA(cudaMallocHost(&p_, n * sizeof(T)));
   }
   T* get() const { return p_; }
   T& operator[](size_t i) { return p_[i]; }
