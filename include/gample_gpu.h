@@ -247,9 +247,11 @@ int gp_device_count(void);
 unsigned long long gp_kernel_launches(void);
 /* Device memory of closed simulations stays cached in the process (the
    current device's stream-ordered pool) so that the next simulation of a
-   similar size starts without the driver mapping gigabytes again; this
-   returns the cached memory of the current device to the driver. No
-   counterpart in the reference (it allocates Metal buffers per run). */
+   similar size starts without the driver mapping gigabytes again, and its
+   page-locked read-back buffers are kept for reuse; this returns the cached
+   memory of the current device to the driver and frees the kept page-locked
+   buffers. No counterpart in the reference (it allocates Metal buffers per
+   run). */
 gp_status gp_release_cached_memory(void);
 
 #ifdef __cplusplus

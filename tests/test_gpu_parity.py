@@ -157,13 +157,14 @@ def test_deposit_atomic_matches_fp64(gpu, order, current):
         assert rel_inf(sim.field("jy"), ora.field("jy"), jscale) < 1e-6
 
 
-@pytest.mark.gpu
-def test_deposit_atomic_dense_cells_error_bound(gpu):
-    """The atomic mode without currents sums 2^-22 fixed-point weights in one
-    word per node: with 256 particles per cell per species (thousands of
-    contributions per node) the error stays far below the FP32 atomic
-    accumulation of the reference's deposit."""
-    cond = condition(ngx=16, ngy=16, order=3, ppc=256, xbc="Dirichlet", ybc="periodic", te=10.0)
+@pytest.mark.parametrize("order", [1, 3, 5])
+def test_deposit_atomic_dense_cells_error_bound(gpu, order):
+    """The atomic mode without currents sums 2^-22 (order 5: 2^-21)
+    fixed-point weights in one word per node: with 256 particles per cell per
+    species (thousands of contributions per node, lane-private windows) the
+    error stays far below the FP32 atomic accumulation of the reference's
+    deposit."""
+    cond = condition(ngx=16, ngy=16, order=order, ppc=256, xbc="Dirichlet", ybc="periodic", te=10.0)
     sim, ora = pair(cond, real64=True)
     for s in range(2):
         g = sim.particles(s)
