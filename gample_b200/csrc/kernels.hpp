@@ -107,9 +107,12 @@ void sort_by_cell(GridDims g, ParticleArrays src, ParticleArrays dst, const Spec
                   uint32_t* scratch, uint32_t n_bound, cudaStream_t s);
 // The same order for particles in random order, in place in p: whole records
 // are scattered into spare (arrays of capacity words each) and converted
-// back. Returns false (nothing launched) when the records do not fit.
+// back. extra is a second idle buffer the call may use (extra_capacity words
+// per array, 0 for none); with it the records are sector-sized. Returns false
+// (nothing launched) when the records do not fit.
 bool sort_by_cell_staged(GridDims g, ParticleArrays p, ParticleArrays spare, uint32_t capacity,
-                         const SpeciesCounters* counters, uint32_t* scratch, uint32_t n_bound, cudaStream_t s);
+                         ParticleArrays extra, uint32_t extra_capacity, const SpeciesCounters* counters,
+                         uint32_t* scratch, uint32_t n_bound, cudaStream_t s);
 
 // Remove flagged particles, filling each hole (ascending) with the last
 // live particle (descending) -- the permutation of src/Particle.mm:893-966.

@@ -167,7 +167,9 @@ class Particle {
   kern::SpeciesCounters counters();  // synchronous
   // Reorder the particles by cell (counting sort into the spare
   // buffer, then swap). The order of particles is otherwise unspecified.
-  void sort();
+  // Cell sort. lender: another species on the same stream whose spare buffer
+  // is idle during the call (it may be overwritten), or null.
+  void sort(Particle* lender = nullptr);
   bool needs_sort = true;
   bool random_order = true;  // particles not yet sorted since loading / upload
   int sort_interval = 0;  // cycles between sorts; 0 = when too many chunks miss their window

@@ -129,10 +129,13 @@ void Particle::download_aos(kern::ParticleStateAoS* host, uint32_t n) {
   GP_CUDA(cudaStreamSynchronize(stream));
 }
 
-void Particle::sort() {
+void Particle::sort(Particle* lender) {
   // freshly loaded or uploaded particles are in random order: staged records
-  if (!(random_order && kern::sort_by_cell_staged(dims_, buf[cur].view(), buf[1 - cur].view(), pNumMax, cnt.get(),
-                                                  sort_scratch.get(), n_bound, stream))) {
+  // (in sector-sized records when another species lends its idle spare buffer)
+  const kern::ParticleArrays extra = lender ? lender->buf[1 - lender->cur].view() : kern::ParticleArrays{};
+  const uint32_t extra_cap = lender && lender->stream == stream ? lender->pNumMax : 0u;
+  if (!(random_order && kern::sort_by_cell_staged(dims_, buf[cur].view(), buf[1 - cur].view(), pNumMax, extra,
+                                                  extra_cap, cnt.get(), sort_scratch.get(), n_bound, stream))) {
     kern::sort_by_cell(dims_, buf[cur].view(), buf[1 - cur].view(), cnt.get(), sort_scratch.get(), n_bound, stream);
     cur = 1 - cur;
   }

@@ -73,8 +73,10 @@ void Simulation::initialize() {
   // src/main.mm:124-147: the logger is still switched off here.
   const int start = init.paramForTimeIntegration.Start;
   if (start != 0 && !loadProgress(start, ptrs, init)) throw std::runtime_error("[Fatal] restart failed.");
-  for (auto* p : ptrs)
-    if (p->needs_sort) p->sort();  // cell order for the freshly loaded particles
+  // cell order for the freshly loaded particles; the species sort one after
+  // the other, so each may use the next one's idle spare buffer
+  for (size_t i = 0; i < ptrs.size(); ++i)
+    if (ptrs[i]->needs_sort) ptrs[i]->sort(ptrs.size() > 1 ? ptrs[(i + 1) % ptrs.size()] : nullptr);
   field->resetChargeDensity();
   for (auto* p : ptrs) p->integrateChargeDensity(*field);
   last_solve = field->solvePoisson(0.0, logger.get());

@@ -10,11 +10,15 @@
 // Particles in random order (just loaded or uploaded) take a staged scatter
 // instead: each particle's six SoA words land in different 32-byte sectors
 // when written one by one to random slots, so the staged path writes whole
-// 24-byte records into the spare buffer (its six arrays used as chunks of
-// records) and then converts the records back to SoA with coalesced
-// accesses, about half the DRAM traffic of the direct scatter for random
-// input. Nearly sorted particles (the periodic re-sort) keep the direct
-// scatter, whose writes are already coalesced.
+// records into the spare buffer (its six arrays used as chunks of records)
+// and then converts the records back to SoA with coalesced accesses. When
+// the caller lends a second idle buffer (another species' spare), the
+// records are padded to 32 bytes: each is then one whole, aligned sector,
+// which the L2 writes back without first reading the rest of the sector from
+// DRAM (a 24-byte record shares its sectors with records that arrive at
+// other times). Otherwise they are 24-byte records. Nearly sorted particles
+// (the periodic re-sort) keep the direct scatter, whose writes are already
+// coalesced.
 #include <cuda_runtime.h>
 
 #include "device.hpp"
@@ -199,6 +203,55 @@ __global__ void __launch_bounds__(kThreads) k_cs_scatter_rec(ParticleArrays src,
   }
 }
 
+// 32-byte records: slot s in chunk s / per, as two int4 (cell, ox, oy, vx),
+// (vy, vz, 0, 0); the chunks start 32-byte aligned.
+struct SectorChunks {
+  int4* c[12];
+  uint32_t per;
+};
+
+__global__ void __launch_bounds__(kThreads) k_cs_scatter_sec(ParticleArrays src, SectorChunks dst,
+                                                             const SpeciesCounters* cnt, KeyGeom g,
+                                                             uint32_t* offsets) {
+  const uint32_t n = cnt->n;
+  const int lane = threadIdx.x & 31;
+  const unsigned lt = (1u << lane) - 1u;
+  for (uint32_t base = (blockIdx.x * kThreads + threadIdx.x) & ~31u; base < n; base += gridDim.x * kThreads) {
+    const uint32_t k = base + lane;
+    const int32_t c = k < n ? src.cell[k] : 0;
+    const uint32_t key = k < n ? cell_key(c, g) : kNoKey;
+    const unsigned peers = __match_any_sync(0xffffffffu, key);
+    const int leader = __ffs(peers) - 1;
+    uint32_t slot = 0;
+    if (key != kNoKey && lane == leader) slot = atomicAdd(&offsets[key], uint32_t(__popc(peers)));
+    slot = __shfl_sync(0xffffffffu, slot, leader) + uint32_t(__popc(peers & lt));
+    if (key != kNoKey) {
+      const int4 a = make_int4(c, __float_as_int(src.ox[k]), __float_as_int(src.oy[k]), __float_as_int(src.vx[k]));
+      const int4 b = make_int4(__float_as_int(src.vy[k]), __float_as_int(src.vz[k]), 0, 0);
+      const uint32_t q = slot / dst.per;
+      int4* r = dst.c[q] + 2 * size_t(slot - q * dst.per);
+      r[0] = a;
+      r[1] = b;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) k_sectors_to_soa(SectorChunks in, const SpeciesCounters* cnt,
+                                                             ParticleArrays out) {
+  const uint32_t n = cnt->n;
+  for (uint32_t k = blockIdx.x * kThreads + threadIdx.x; k < n; k += gridDim.x * kThreads) {
+    const uint32_t q = k / in.per;
+    const int4* r = in.c[q] + 2 * size_t(k - q * in.per);
+    const int4 a = r[0], b = r[1];
+    out.cell[k] = a.x;
+    out.ox[k] = __int_as_float(a.y);
+    out.oy[k] = __int_as_float(a.z);
+    out.vx[k] = __int_as_float(a.w);
+    out.vy[k] = __int_as_float(b.x);
+    out.vz[k] = __int_as_float(b.y);
+  }
+}
+
 __global__ void __launch_bounds__(kThreads) k_records_to_soa(RecordChunks in, const SpeciesCounters* cnt,
                                                              ParticleArrays out) {
   const uint32_t n = cnt->n;
@@ -245,10 +298,25 @@ size_t sort_scratch_words(GridDims g) {
 }
 
 bool sort_by_cell_staged(GridDims g, ParticleArrays p, ParticleArrays spare, uint32_t capacity,
-                         const SpeciesCounters* cnt, uint32_t* scratch, uint32_t n_bound, cudaStream_t s) {
+                         ParticleArrays extra, uint32_t extra_capacity, const SpeciesCounters* cnt,
+                         uint32_t* scratch, uint32_t n_bound, cudaStream_t s) {
+  // 32-byte records in the spare arrays and, if lent, the extra ones
+  SectorChunks sc{};
+  sc.per = uint32_t(size_t(capacity) * sizeof(int32_t) / 32);
+  int nsc = 0;
+  auto add_chunks = [&](const ParticleArrays& a) {
+    void* arrs[6] = {a.cell, a.ox, a.oy, a.vx, a.vy, a.vz};
+    for (void* q : arrs) {
+      if (reinterpret_cast<uintptr_t>(q) % 32 != 0) return false;
+      sc.c[nsc++] = static_cast<int4*>(q);
+    }
+    return true;
+  };
+  const bool sectors = n_bound > 0 && sc.per > 0 && extra_capacity >= capacity && add_chunks(spare) &&
+                       add_chunks(extra) && size_t(n_bound) <= size_t(nsc) * sc.per;
   RecordChunks rc;
   rc.per = uint32_t(size_t(capacity) * sizeof(int32_t) / sizeof(Record));
-  if (n_bound == 0 || rc.per == 0 || size_t(n_bound) > 6 * size_t(rc.per)) return false;
+  if (!sectors && (n_bound == 0 || rc.per == 0 || size_t(n_bound) > 6 * size_t(rc.per))) return false;
   rc.c[0] = reinterpret_cast<Record*>(spare.cell);
   rc.c[1] = reinterpret_cast<Record*>(spare.ox);
   rc.c[2] = reinterpret_cast<Record*>(spare.oy);
@@ -270,10 +338,17 @@ bool sort_by_cell_staged(GridDims g, ParticleArrays p, ParticleArrays spare, uin
   GP_LAUNCH_CHECK();
   k_scan_add<<<(nk + 255) / 256, 256, 0, s>>>(offsets, sums, nk);
   GP_LAUNCH_CHECK();
-  k_cs_scatter_rec<<<grid_for(n_bound), kThreads, 0, s>>>(p, rc, cnt, kg, offsets);
-  GP_LAUNCH_CHECK();
-  k_records_to_soa<<<grid_for(n_bound), kThreads, 0, s>>>(rc, cnt, p);
-  GP_LAUNCH_CHECK();
+  if (sectors) {
+    k_cs_scatter_sec<<<grid_for(n_bound), kThreads, 0, s>>>(p, sc, cnt, kg, offsets);
+    GP_LAUNCH_CHECK();
+    k_sectors_to_soa<<<grid_for(n_bound), kThreads, 0, s>>>(sc, cnt, p);
+    GP_LAUNCH_CHECK();
+  } else {
+    k_cs_scatter_rec<<<grid_for(n_bound), kThreads, 0, s>>>(p, rc, cnt, kg, offsets);
+    GP_LAUNCH_CHECK();
+    k_records_to_soa<<<grid_for(n_bound), kThreads, 0, s>>>(rc, cnt, p);
+    GP_LAUNCH_CHECK();
+  }
   return true;
 }
 

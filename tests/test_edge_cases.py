@@ -91,9 +91,12 @@ def test_ragged_particle_counts_match_the_oracle(gpu, n):
 @pytest.mark.parametrize("n", [5, 200_003])
 def test_upload_in_random_order_is_sorted_by_tile(gpu, n):
     """Uploaded particles are in no particular order; initialize() sorts them
-    through the staged record scatter: the same particles come back, ordered
-    by 8x8 tile, then row and column inside the tile."""
-    cond = condition(ngx=40, ngy=24, order=1, ppc=2, xbc="periodic", ybc="Dirichlet", pnum_max=250_000)
+    through the staged record scatter (32-byte records in the spare buffers
+    of both species): the same particles come back, ordered by 8x8 tile, then
+    row and column inside the tile. An upload between cycles is sorted by the
+    next cycle (24-byte records in the species' own spare buffer)."""
+    cond = condition(ngx=40, ngy=24, order=1, ppc=2, xbc="periodic", ybc="Dirichlet", pnum_max=250_000,
+                     dt=1e-18)
     sim = capi.Sim(cond)
     rng = np.random.default_rng(n)
     x = rng.uniform(0, 40, n).astype(np.float32)
@@ -113,6 +116,16 @@ def test_upload_in_random_order_is_sorted_by_tile(gpu, n):
         as_bits = lambda d: np.stack([d[c].view(np.uint32) for c in cols])
         a, b = as_bits(before[s]), as_bits(after)
         np.testing.assert_array_equal(a[:, np.lexsort(a[::-1])], b[:, np.lexsort(b[::-1])])
+    # particles at rest and a 1e-18 s step: the cycle's push keeps every cell
+    z = np.zeros(n, np.float32)
+    sim.set_particles(0, _records(x, y, z, z, z))
+    sim.run(1)
+    after = sim.particles_raw(0)
+    assert len(after["cell"]) == n
+    ix, iy = after["cell"] & 0xFFFF, after["cell"] >> 16
+    key = (((iy // 8).astype(np.int64) * 4096 + ix // 8) * 8 + iy % 8) * 8 + ix % 8
+    assert np.all(np.diff(key) >= 0)
+    np.testing.assert_array_equal(np.sort(after["cell"]), np.sort(before[0]["cell"]))
     sim.close()
 
 
