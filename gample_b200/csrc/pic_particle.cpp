@@ -102,16 +102,45 @@ uint32_t Particle::stage_records() const {
   return uint32_t(std::max<size_t>(1, size_t(pNumMax) * sizeof(int32_t) / sizeof(kern::ParticleStateAoS)));
 }
 
+// Two staging areas (the spare buffer's cell and ox arrays) alternate, and
+// the copies run on a second stream, so that the copy of one chunk overlaps
+// the layout conversion of the previous one.
+namespace {
+struct Staging {
+  cudaStream_t xfer = nullptr;
+  cudaEvent_t ev[5] = {};  // [0, 2): copy done per area, [2, 4): conversion done per area, [4]: start
+  Staging() {
+    GP_CUDA(cudaStreamCreateWithFlags(&xfer, cudaStreamNonBlocking));
+    for (auto& e : ev) GP_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  }
+  ~Staging() {
+    for (auto& e : ev) cudaEventDestroy(e);
+    cudaStreamDestroy(xfer);
+  }
+};
+}  // namespace
+
 void Particle::upload_aos(const kern::ParticleStateAoS* host, uint32_t n) {
   if (n > pNumMax) throw std::invalid_argument("pNum > pNumMax");
-  auto* stage = reinterpret_cast<kern::ParticleStateAoS*>(buf[1 - cur].cell.get());
+  kern::ParticleStateAoS* stage[2] = {reinterpret_cast<kern::ParticleStateAoS*>(buf[1 - cur].cell.get()),
+                                      reinterpret_cast<kern::ParticleStateAoS*>(buf[1 - cur].ox.get())};
   const uint32_t chunk = stage_records();
-  for (uint32_t off = 0; off < n; off += chunk) {
+  Staging st;
+  GP_CUDA(cudaEventRecord(st.ev[4], stream));  // earlier work on the spare buffer
+  GP_CUDA(cudaStreamWaitEvent(st.xfer, st.ev[4], 0));
+  int i = 0;
+  for (uint32_t off = 0; off < n; off += chunk, ++i) {
+    const int a = i & 1;
     const uint32_t m = std::min(chunk, n - off);
-    GP_CUDA(cudaMemcpyAsync(stage, host + off, size_t(m) * sizeof(*host), cudaMemcpyHostToDevice, stream));
-    kern::aos_to_soa(stage, m, offset_view(arrays(), off), stream);
+    if (i >= 2) GP_CUDA(cudaStreamWaitEvent(st.xfer, st.ev[2 + a], 0));  // area read by the conversion
+    GP_CUDA(cudaMemcpyAsync(stage[a], host + off, size_t(m) * sizeof(*host), cudaMemcpyHostToDevice, st.xfer));
+    GP_CUDA(cudaEventRecord(st.ev[a], st.xfer));
+    GP_CUDA(cudaStreamWaitEvent(stream, st.ev[a], 0));
+    kern::aos_to_soa(stage[a], m, offset_view(arrays(), off), stream);
+    GP_CUDA(cudaEventRecord(st.ev[2 + a], stream));
   }
   GP_CUDA(cudaStreamSynchronize(stream));
+  GP_CUDA(cudaStreamSynchronize(st.xfer));
   setPNum(n);
   needs_sort = true;
   random_order = true;
@@ -119,13 +148,22 @@ void Particle::upload_aos(const kern::ParticleStateAoS* host, uint32_t n) {
 
 void Particle::download_aos(kern::ParticleStateAoS* host, uint32_t n) {
   if (!n) return;
-  auto* stage = reinterpret_cast<kern::ParticleStateAoS*>(buf[1 - cur].cell.get());
+  kern::ParticleStateAoS* stage[2] = {reinterpret_cast<kern::ParticleStateAoS*>(buf[1 - cur].cell.get()),
+                                      reinterpret_cast<kern::ParticleStateAoS*>(buf[1 - cur].ox.get())};
   const uint32_t chunk = stage_records();
-  for (uint32_t off = 0; off < n; off += chunk) {
+  Staging st;
+  int i = 0;
+  for (uint32_t off = 0; off < n; off += chunk, ++i) {
+    const int a = i & 1;
     const uint32_t m = std::min(chunk, n - off);
-    kern::soa_to_aos(offset_view(arrays(), off), m, stage, stream);
-    GP_CUDA(cudaMemcpyAsync(host + off, stage, size_t(m) * sizeof(*host), cudaMemcpyDeviceToHost, stream));
+    if (i >= 2) GP_CUDA(cudaStreamWaitEvent(stream, st.ev[a], 0));  // area read by the copy
+    kern::soa_to_aos(offset_view(arrays(), off), m, stage[a], stream);
+    GP_CUDA(cudaEventRecord(st.ev[2 + a], stream));
+    GP_CUDA(cudaStreamWaitEvent(st.xfer, st.ev[2 + a], 0));
+    GP_CUDA(cudaMemcpyAsync(host + off, stage[a], size_t(m) * sizeof(*host), cudaMemcpyDeviceToHost, st.xfer));
+    GP_CUDA(cudaEventRecord(st.ev[a], st.xfer));
   }
+  GP_CUDA(cudaStreamSynchronize(st.xfer));
   GP_CUDA(cudaStreamSynchronize(stream));
 }
 
