@@ -756,6 +756,21 @@ int blocks_for(int n) {
   return int(b < 2368 ? b : 2368);
 }
 
+// Grid of the kernels that end in a global FP64 reduction: two CTAs per SM,
+// so that each adds its partial sums once (the adds to one address are
+// serialised in the L2) and each thread covers several points.
+int reduce_blocks(int n) {
+  static int cap = 0;
+  if (!cap) {
+    int dev = 0, sms = 0;
+    GP_CUDA(cudaGetDevice(&dev));
+    GP_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    cap = 2 * sms;
+  }
+  const int b = blocks_for(n);
+  return b < cap ? b : cap;
+}
+
 LevelDesc desc(const PoissonMG::Level& l) { return LevelDesc{l.mx, l.my, l.bx, l.by, l.cx, l.cy, l.cd}; }
 
 bool can_coarsen(int n, int b) { return b == BC_PER ? (n >= 4 && n % 2 == 0) : (n >= 3 && n % 2 == 1); }
@@ -987,11 +1002,11 @@ void PoissonMG::enqueue_iteration(int parity, double* x, double tol, int maxiter
   const float* z = result(0);
   double* p = p_[parity].get();
   const double* p_old = p_[parity ^ 1].get();
-  k_fcg_zq<<<blocks_for(n_), 256, 0, s>>>(z, q_.get(), n_, st);
+  k_fcg_zq<<<reduce_blocks(n_), 256, 0, s>>>(z, q_.get(), n_, st);
   GP_LAUNCH_CHECK();
-  k_fcg_dir<<<blocks_for(n_), 256, 0, s>>>(z, p_old, p, q_.get(), r64_.get(), L_, st);
+  k_fcg_dir<<<reduce_blocks(n_), 256, 0, s>>>(z, p_old, p, q_.get(), r64_.get(), L_, st);
   GP_LAUNCH_CHECK();
-  k_fcg_update<<<blocks_for(n_), 256, 0, s>>>(x, p, q_.get(), r64_.get(), f.f.get(), L_, st);
+  k_fcg_update<<<reduce_blocks(n_), 256, 0, s>>>(x, p, q_.get(), r64_.get(), f.f.get(), L_, st);
   GP_LAUNCH_CHECK();
   k_check<<<1, 1, 0, s>>>(st, tol, maxiter, wsum);
   GP_LAUNCH_CHECK();
@@ -1065,7 +1080,7 @@ MGResult PoissonMG::solve(const double* b, const double* sums_b, double* x, doub
   k_clear_if_zero_rhs<<<blocks_for(n_), 256, 0, s>>>(x, n_, st);
   GP_LAUNCH_CHECK();
   const double wsum = singular_ ? wsum_ : double(n_);
-  k_residual64<<<blocks_for(n_), 256, 0, s>>>(x, b, L_, f.f.get(), r64_.get(), st);
+  k_residual64<<<reduce_blocks(n_), 256, 0, s>>>(x, b, L_, f.f.get(), r64_.get(), st);
   GP_LAUNCH_CHECK();
   k_check<<<1, 1, 0, s>>>(st, tol, maxiter, wsum);
   GP_LAUNCH_CHECK();
