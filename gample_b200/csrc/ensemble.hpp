@@ -3,8 +3,11 @@
 // Every member is a full Simulation with its own CUDA stream; a pool of host
 // threads drives them concurrently, so the kernels of different members
 // overlap on the GPU and the host synchronisation points of one member
-// (diagnostics, counter reads) do not stall the others. Members share no
-// state: each one's results equal the same run alone.
+// (diagnostics, counter reads) do not stall the others. The threads take
+// members from a shared queue, largest first (particle capacity times
+// species, then grid cells), so that one thread does not end up with several
+// large members while the others idle. Members share no state: each one's
+// results equal the same run alone.
 #pragma once
 
 #include <memory>
@@ -26,6 +29,7 @@ class Ensemble {
   template <typename F>
   void parallel(F&& f);
   int threads_ = 1;
+  std::vector<size_t> order_;  // members by decreasing size: the pool takes the largest first
 };
 
 }  // namespace gample
