@@ -287,6 +287,21 @@ def dist_setup():
     return world, rank, local
 
 
+def aggregate_ranks(ms, pushes, pg=None, device="cuda"):
+    """Whole-job numbers of a replica run: the step time is the maximum over
+    ranks (each rank's own CUDA-event time), the pushes the sum over ranks.
+    Returns (ms_max, total pushes, pushes per second)."""
+    ms_max, total = float(ms), float(pushes)
+    if pg is not None:
+        import torch
+        t = torch.tensor([ms], device=device, dtype=torch.float64)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        c = torch.tensor([pushes], device=device, dtype=torch.float64)
+        pg.all_reduce(c, op=pg.ReduceOp.SUM)
+        ms_max, total = float(t.item()), float(c.item())
+    return ms_max, total, total / (ms_max / 1e3)
+
+
 def cpu_baseline_run(steps, warmup, ppc_sample, threads=None):
     """The oracle (C++ restatement of the reference's CPU arithmetic, OpenMP)
     on the same grid/physics with ppc_sample particles per cell per species."""
@@ -374,15 +389,10 @@ def run_b200(args):
                               "gpu_launches": launches}), flush=True)
         sim.close()
         return 0
-    ms_max = ms
-    if pg:
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        ms_max = float(t.item())
     iters_last = sim.last_solve().iterations
     unknowns = (sim.nkx + 1) * (sim.nky + 1)
     pushes_rank = 0.5 * (n0 + n1) * args.steps
-    value = pushes_rank * world / (ms_max / 1e3)
+    ms_max, _, value = aggregate_ranks(ms, pushes_rank, pg)
 
     # Roofline of the dominant kernel (push + fused deposit): a few more
     # cycles with per-phase CUDA events on the library's stream.
