@@ -110,12 +110,19 @@ struct Staging {
   cudaStream_t xfer = nullptr;
   cudaEvent_t ev[5] = {};  // [0, 2): copy done per area, [2, 4): conversion done per area, [4]: start
   Staging() {
-    GP_CUDA(cudaStreamCreateWithFlags(&xfer, cudaStreamNonBlocking));
-    for (auto& e : ev) GP_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    try {
+      GP_CUDA(cudaStreamCreateWithFlags(&xfer, cudaStreamNonBlocking));
+      for (auto& e : ev) GP_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    } catch (...) {
+      release();
+      throw;
+    }
   }
-  ~Staging() {
-    for (auto& e : ev) cudaEventDestroy(e);
-    cudaStreamDestroy(xfer);
+  ~Staging() { release(); }
+  void release() {
+    for (auto& e : ev)
+      if (e) cudaEventDestroy(e);
+    if (xfer) cudaStreamDestroy(xfer);
   }
 };
 }  // namespace
