@@ -39,6 +39,14 @@ constexpr int kReach = 12;                   // window box: cells within kReach 
 constexpr size_t kDepositBudget = 98304;     // shared-memory bytes for the deposit window copies
 constexpr int kPW = 20;                      // row stride of a lane-private deposit window (entries)
 constexpr int kPrivWords = 10752;            // words for 32 lane-private windows (42 KB)
+// Gather table: per cell 16 float4 of coefficients and one float4 of padding
+// (17 = 1 mod 8), rows of cells padded to a multiple of 8 plus 3 float4, so
+// that a 16-byte load of cell (col, row) falls in bank group
+// (col + 3 row) mod 8: the 8 lanes served together by a 16-byte shared load,
+// whose particles lie in neighbouring cells, mostly use distinct banks.
+constexpr int kTabStride = 17;                              // float4 per cell
+constexpr int kTabFloat4 = 2 * kWin / 4;                    // float4 that fit in the Ex/Ey windows
+__host__ __device__ constexpr int tab_row_stride(int tbw) { return tbw * kTabStride + ((3 - tbw * kTabStride) & 7); }
 
 __device__ __forceinline__ uint32_t warp_sum(uint32_t v) { return __reduce_add_sync(0xffffffffu, v); }
 __device__ __forceinline__ double warp_sum(double v) {
@@ -90,6 +98,9 @@ struct Window {  // shared-memory windows of one CTA (array-index coordinates)
   int ds;                // deposit window row stride (>= dw, congruent to ORDER + 1 mod 32)
   int priv;              // 1: 32 lane-private deposit windows, row stride kPW
   int ps;                // their copy stride (odd, >= kPW * dh)
+  int tab;               // 1: gather table of the box's cells instead of the field windows
+  int tbw;               // box width in cells
+  int trs;               // table row stride in float4 (tab_row_stride(tbw))
 };
 
 // r[t] = w[(t + sh) mod N] for a per-lane shift sh in [0, N).
@@ -325,12 +336,70 @@ __device__ __forceinline__ void deposit_priv(const Window& w, uint32_t lane_base
   priv_add<N>(a0, rx, wyn);
 }
 
+// Gather table (order 3, uniform Bz). Inside one cell, for a fixed choice of
+// the half-shifted stencil (offset below or above 1/2), the gathered field is
+// a bicubic polynomial of the particle's offsets: Ex(hx, oy) with hx the
+// half-shifted x offset and Ey(ox, hy). The CTA tabulates the monomial
+// coefficients of the four polynomials of every cell of its box,
+//   C[n][m] = sum_i sum_j A[i][m] A[j][n] F(tap i, tap j),
+// with A[i][m] the coefficient of h^m in the cubic B-spline weight of tap i
+// (shape<3>), and a particle evaluates its two polynomials by Horner's rule:
+// 8 shared 16-byte loads and 30 multiply-adds instead of four weight vectors,
+// 32 loads and 40 multiply-adds. The sums equal the stencil sums up to FP32
+// rounding.
+__device__ __forceinline__ float cubic_coef(int tap, int m) {
+  // rows: taps 0..3; columns: powers h^0..h^3 of shape<3>'s weights
+  constexpr float kA[4][4] = {{1.0f / 6.0f, -0.5f, 0.5f, -1.0f / 6.0f},
+                              {2.0f / 3.0f, 0.0f, -1.0f, 0.5f},
+                              {1.0f / 6.0f, 0.5f, 0.5f, -0.5f},
+                              {0.0f, 0.0f, 0.0f, 1.0f / 6.0f}};
+  return kA[tap][m];
+}
+
+// Coefficients of one polynomial from its 4 x 4 taps F[i + 4 j] (i: column
+// tap, j: row tap), stored as four float4 rows c[n] = (C[n][0], ..., C[n][3]).
+__device__ __forceinline__ void tab_build(const float (&F)[16], float4* c) {
+  float T[4][4];  // T[i][n] = sum_j F(i, j) A[j][n]
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int n = 0; n < 4; ++n) {
+      float t = 0.0f;
+#pragma unroll
+      for (int j = 0; j < 4; ++j) t = fmaf(F[i + 4 * j], cubic_coef(j, n), t);
+      T[i][n] = t;
+    }
+#pragma unroll
+  for (int n = 0; n < 4; ++n) {
+    float r[4];
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+      float t = 0.0f;
+#pragma unroll
+      for (int i = 0; i < 4; ++i) t = fmaf(cubic_coef(i, m), T[i][n], t);
+      r[m] = t;
+    }
+    c[n] = make_float4(r[0], r[1], r[2], r[3]);
+  }
+}
+
+// sum_n k^n sum_m C[n][m] h^m
+__device__ __forceinline__ float tab_eval(const float4* c, float h, float k) {
+  const float4 c0 = c[0], c1 = c[1], c2 = c[2], c3 = c[3];
+  const float p0 = fmaf(fmaf(fmaf(c0.w, h, c0.z), h, c0.y), h, c0.x);
+  const float p1 = fmaf(fmaf(fmaf(c1.w, h, c1.z), h, c1.y), h, c1.x);
+  const float p2 = fmaf(fmaf(fmaf(c2.w, h, c2.z), h, c2.y), h, c2.x);
+  const float p3 = fmaf(fmaf(fmaf(c3.w, h, c3.z), h, c3.y), h, c3.x);
+  return fmaf(fmaf(fmaf(p3, k, p2), k, p1), k, p0);
+}
+
 // Gather Ex, Ey (and Bz) for one particle (src/Particle.mm:142-154).
 // WIN: from the staged windows; CHECKED: global with bounds checks (a tap
 // outside the arrays contributes zero). Every path evaluates the same
 // separable sum -- each stencil row reduced with the x weights, then the row
 // sums with the y weights (20 instead of 32 multiply-adds per component) --
-// so a particle's result does not depend on which path its chunk takes.
+// so a particle's result does not depend on which path its chunk takes (the
+// gather tables of the atomic mode excepted: they agree to FP32 rounding).
 template <int ORDER, bool BZU, bool WIN, bool CHECKED>
 __device__ __forceinline__ void gather(const GridDims& g, const FieldPtrs& f, const Window& w, const Stagger& sx,
                                        const Stagger& sy, const float (&wxn)[ORDER + 1],
@@ -453,6 +522,11 @@ __global__ void __launch_bounds__(kThreads, ORDER == 5 ? 2 : (PUSH && (!BZU || !
                                                   int boris_order, DepositTargets d, SpeciesCounters* cnt,
                                                   uint32_t* dead_bits, int injected_only) {
   using DL = DepositLayout<ORDER, CUR, DET>;
+  // Gather tables (they replace the Ex/Ey windows) round differently from the
+  // stencil sum that every other path evaluates, so a particle's field would
+  // depend on its chunk's box; the deterministic mode (DET, also passed to its
+  // pushes without deposit) keeps the stencil sum everywhere.
+  constexpr bool kTab = PUSH && BZU && ORDER == 3 && !DET;
   extern __shared__ __align__(16) unsigned char smem[];
   float* sEx = reinterpret_cast<float*>(smem);
   float* sEy = sEx + (PUSH ? kWin : 0);
@@ -526,6 +600,9 @@ __global__ void __launch_bounds__(kThreads, ORDER == 5 ? 2 : (PUSH && (!BZU || !
     w.use = 0;
     w.priv = 0;
     w.ps = 1;
+    w.tab = 0;
+    w.tbw = 1;
+    w.trs = 0;
     if (w.mnx != INT_MAX) {
       w.gx0 = w.mnx - ngb;
       w.gy0 = w.mny - ngb;
@@ -541,6 +618,9 @@ __global__ void __launch_bounds__(kThreads, ORDER == 5 ? 2 : (PUSH && (!BZU || !
       w.priv = 0;
       w.ps = (kPW * w.dh) | 1;
       if (DEP && DL::kSingle && w.use && w.dw <= kPW && 32 * w.ps + 3 <= kPrivWords) w.priv = 1;
+      w.tbw = w.mxx - w.mnx + 1;
+      w.trs = tab_row_stride(w.tbw);
+      w.tab = (kTab && w.use && w.trs * (w.mxy - w.mny + 1) <= kTabFloat4) ? 1 : 0;
     }
     s_w = w;
   }
@@ -550,7 +630,26 @@ __global__ void __launch_bounds__(kThreads, ORDER == 5 ? 2 : (PUSH && (!BZU || !
 
   // ---- phase B: stage the field window, clear the deposit window
   if (w.use) {
-    if constexpr (PUSH) {
+    if (kTab && w.tab) {
+      // four polynomials per box cell: Ex below / above the half offset, Ey likewise
+      const int nx = g.nx;
+      float4* tb = reinterpret_cast<float4*>(sEx);
+      const int cells = w.tbw * (w.mxy - w.mny + 1);
+      for (int e = tid; e < 4 * cells; e += kThreads) {
+        const int c = e >> 2, q = e & 3, p = q & 1;
+        const int col = c % w.tbw, row = c / w.tbw;
+        const int ix = w.mnx + col, iy = w.mny + row;
+        const float* src = q < 2 ? f.Ex : f.Ey;
+        const int stride = q < 2 ? nx + 2 : nx + 1;
+        const int c0 = q < 2 ? ix - ngb + p : ix - ngb, r0 = q < 2 ? iy - ngb : iy - ngb + p;
+        float F[16];
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+          for (int i = 0; i < 4; ++i) F[i + 4 * j] = __ldg(src + (c0 + i) + (r0 + j) * stride);
+        tab_build(F, tb + row * w.trs + kTabStride * col + 4 * q);
+      }
+    } else if constexpr (PUSH) {
       const int nx = g.nx, ny = g.ny;
       for (int e = tid; e < w.gw * w.gh; e += kThreads) {
         const int col = w.gx0 + e % w.gw, row = w.gy0 + e / w.gw;
@@ -636,17 +735,24 @@ __global__ void __launch_bounds__(kThreads, ORDER == 5 ? 2 : (PUSH && (!BZU || !
           float vx = l_vx, vy = l_vy, vz = l_vz;
           const Stagger sx = stagger(ix, ox), sy = stagger(iy, oy);
           float wxn[ORDER + 1], wxh[ORDER + 1], wyn[ORDER + 1], wyh[ORDER + 1];
-          shape<ORDER>(sx.hnode, wxn);
-          shape<ORDER>(sx.hhalf, wxh);
-          shape<ORDER>(sy.hnode, wyn);
-          shape<ORDER>(sy.hhalf, wyh);
           float Epx = 0.0f, Epy = 0.0f, Bpz = 0.0f;
-          if (in_box_win)
-            gather<ORDER, BZU, true, false>(g, f, w, sx, sy, wxn, wxh, wyn, wyh, sEx, sEy, sBz, Epx, Epy, Bpz);
-          else if (inside)
-            gather<ORDER, BZU, false, false>(g, f, w, sx, sy, wxn, wxh, wyn, wyh, sEx, sEy, sBz, Epx, Epy, Bpz);
-          else
-            gather<ORDER, BZU, false, true>(g, f, w, sx, sy, wxn, wxh, wyn, wyh, sEx, sEy, sBz, Epx, Epy, Bpz);
+          if (kTab && in_box_win && s_w.tab) {  // read from shared memory: no register held across the loop
+            const float4* tb =
+                reinterpret_cast<const float4*>(sEx) + (iy - w.mny) * s_w.trs + kTabStride * (ix - w.mnx);
+            Epx = tab_eval(tb + (ox >= 0.5f ? 4 : 0), sx.hhalf, oy);
+            Epy = tab_eval(tb + (oy >= 0.5f ? 12 : 8), ox, sy.hhalf);
+          } else {
+            shape<ORDER>(sx.hnode, wxn);
+            shape<ORDER>(sx.hhalf, wxh);
+            shape<ORDER>(sy.hnode, wyn);
+            shape<ORDER>(sy.hhalf, wyh);
+            if (in_box_win)
+              gather<ORDER, BZU, true, false>(g, f, w, sx, sy, wxn, wxh, wyn, wyh, sEx, sEy, sBz, Epx, Epy, Bpz);
+            else if (inside)
+              gather<ORDER, BZU, false, false>(g, f, w, sx, sy, wxn, wxh, wyn, wyh, sEx, sEy, sBz, Epx, Epy, Bpz);
+            else
+              gather<ORDER, BZU, false, true>(g, f, w, sx, sy, wxn, wxh, wyn, wyh, sEx, sEy, sBz, Epx, Epy, Bpz);
+          }
           if (!in_box_win) tally += 1u << 24;
           // Boris push (src/Particle.mm:157-209); Ez, Bx, By are identically
           // zero in the reference's gather (:134-139).
@@ -834,8 +940,11 @@ void dispatch_pic(bool dep, bool det, bool cur, bool bzu, uint32_t nblocks, cuda
 #define GP_PIC(DEP, DET, CUR, BZU) \
   launch_pic<ORDER, PUSH, DEP, DET, CUR, BZU>(nblocks, s, g, p, f, c, boris, d, cnt, bits, injected_only)
   if constexpr (PUSH) {
-    if (!dep) {
-      bzu ? GP_PIC(false, false, false, true) : GP_PIC(false, false, false, false);
+    if (!dep) {  // DET only selects the bit-reproducible gather here
+      if (det)
+        bzu ? GP_PIC(false, true, false, true) : GP_PIC(false, true, false, false);
+      else
+        bzu ? GP_PIC(false, false, false, true) : GP_PIC(false, false, false, false);
     } else if (det) {
       if (cur)
         bzu ? GP_PIC(true, true, true, true) : GP_PIC(true, true, true, false);

@@ -125,6 +125,46 @@ def test_push_matches_oracle(gpu, order, boris, bcs):
         assert np.all(ey <= 0), ("y", np.max(ey), int(np.argmax(ey)))
 
 
+@pytest.mark.parametrize("order", [1, 3, 5])
+def test_push_dense_sorted_uniform_bz_matches_oracle(gpu, order):
+    """256 particles per cell in tile order with a uniform Bz: chunks cover a
+    few cells, so order 3 gathers through the per-cell polynomial tables and
+    orders 1 and 5 through the staged windows; rough random Ex, Ey make every
+    tap matter. Same tolerances as the push test above."""
+    ngx = ngy = 16
+    cond = condition(ngx=ngx, ngy=ngy, order=order, ppc=256, xbc="periodic", ybc="periodic", bz_tesla=0.05,
+                     dt=2e-11)
+    sim, ora = pair(cond)
+    ora.load_initial()
+    rng = np.random.default_rng(100 + order)
+    random_fields(ora, rng, emag=30.0)
+    for name in ("Ex", "Ey"):
+        sim.set_field(name, ora.field(name).astype(np.float32))
+    for s in range(2):
+        o = ora.particles(s, f32=True)
+        ix, iy = np.floor(o["x"]).astype(np.int64), np.floor(o["y"]).astype(np.int64)
+        perm = np.lexsort((ix % 8, iy % 8, ix // 8, iy // 8))  # 8x8 tiles, row-major inside
+        o = {c: o[c][perm] for c in ("x", "y", "vx", "vy", "vz")}
+        ora.set_particles(s, o["x"], o["y"], o["vx"], o["vy"], o["vz"], f32=True)
+        sim.set_particles(s, to_aos(o["x"], o["y"], o["vx"], o["vy"], o["vz"]))
+        ora.push(s)
+        sim.update(s, cond["ParamForTimeIntegration"]["TimeStep"], fused_deposit=False)
+        g, r = sim.particles(s), ora.particles(s, f32=True)
+        assert np.array_equal(g["piflag"], r["piflag"])
+        vth = np.sqrt(np.mean(r["vx"].astype(np.float64) ** 2))
+        for c in ("vx", "vy", "vz"):
+            a, b = g[c].astype(np.float64), r[c].astype(np.float64)
+            assert np.all(np.abs(a - b) <= 1e-5 * (np.abs(b) + vth)), c
+        cst = ora.species_consts(s)
+        for c, period, k in (("x", ngx, "constX"), ("y", ngy, "constY")):
+            x0 = o[c].astype(np.float64)
+            dg = g[c].astype(np.float64) - x0
+            dr = r[c].astype(np.float64) - x0
+            dg = (dg - dr + period / 2) % period - period / 2 + dr  # periodic wrap on either side
+            ulp = np.spacing((np.abs(r[c]) + period).astype(np.float32)).astype(np.float64)
+            assert np.all(np.abs(dg - dr) <= 4 * ulp + 1e-5 * (np.abs(dr) + vth * cst[k])), c
+
+
 # ---------------------------------------------------------------- deposit
 @pytest.mark.parametrize("order", [1, 3, 5])
 @pytest.mark.parametrize("current", [0, 1])
