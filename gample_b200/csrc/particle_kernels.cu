@@ -39,14 +39,16 @@ constexpr int kReach = 12;                   // window box: cells within kReach 
 constexpr size_t kDepositBudget = 98304;     // shared-memory bytes for the deposit window copies
 constexpr int kPW = 20;                      // row stride of a lane-private deposit window (entries)
 constexpr int kPrivWords = 10752;            // words for 32 lane-private windows (42 KB)
-// Gather table: per cell 16 float4 of coefficients and one float4 of padding
-// (17 = 1 mod 8), rows of cells padded to a multiple of 8 plus 3 float4, so
-// that a 16-byte load of cell (col, row) falls in bank group
-// (col + 3 row) mod 8: the 8 lanes served together by a 16-byte shared load,
-// whose particles lie in neighbouring cells, mostly use distinct banks.
-constexpr int kTabStride = 17;                              // float4 per cell
+// Gather tables: one polynomial (4 float4 of coefficients) per entry, entries
+// 5 float4 apart and rows padded to 2 mod 8 float4, so that a 16-byte load of
+// entry (col, row) falls in bank group (5 col + 2 row + const) mod 8 and the 8
+// lanes served together by a 16-byte shared load, whose particles lie in
+// neighbouring cells, mostly use distinct banks.
+constexpr int kTabEntry = 5;                                // float4 per polynomial
 constexpr int kTabFloat4 = 2 * kWin / 4;                    // float4 that fit in the Ex/Ey windows
-__host__ __device__ constexpr int tab_row_stride(int tbw) { return tbw * kTabStride + ((3 - tbw * kTabStride) & 7); }
+__host__ __device__ constexpr int tab_row_stride(int entries) {
+  return entries * kTabEntry + ((2 - entries * kTabEntry) & 7);
+}
 
 __device__ __forceinline__ uint32_t warp_sum(uint32_t v) { return __reduce_add_sync(0xffffffffu, v); }
 __device__ __forceinline__ double warp_sum(double v) {
@@ -99,8 +101,8 @@ struct Window {  // shared-memory windows of one CTA (array-index coordinates)
   int priv;              // 1: 32 lane-private deposit windows, row stride kPW
   int ps;                // their copy stride (odd, >= kPW * dh)
   int tab;               // 1: gather table of the box's cells instead of the field windows
-  int tbw;               // box width in cells
-  int trs;               // table row stride in float4 (tab_row_stride(tbw))
+  int tbw, tbh;          // box size in cells
+  int xrs, yrs, yoff;    // Ex / Ey table row strides and the Ey table's start (float4)
 };
 
 // r[t] = w[(t + sh) mod N] for a per-lane shift sh in [0, N).
@@ -601,8 +603,8 @@ __global__ void __launch_bounds__(kThreads, ORDER == 5 ? 2 : (PUSH && (!BZU || !
     w.priv = 0;
     w.ps = 1;
     w.tab = 0;
-    w.tbw = 1;
-    w.trs = 0;
+    w.tbw = w.tbh = 1;
+    w.xrs = w.yrs = w.yoff = 0;
     if (w.mnx != INT_MAX) {
       w.gx0 = w.mnx - ngb;
       w.gy0 = w.mny - ngb;
@@ -619,8 +621,11 @@ __global__ void __launch_bounds__(kThreads, ORDER == 5 ? 2 : (PUSH && (!BZU || !
       w.ps = (kPW * w.dh) | 1;
       if (DEP && DL::kSingle && w.use && w.dw <= kPW && 32 * w.ps + 3 <= kPrivWords) w.priv = 1;
       w.tbw = w.mxx - w.mnx + 1;
-      w.trs = tab_row_stride(w.tbw);
-      w.tab = (kTab && w.use && w.trs * (w.mxy - w.mny + 1) <= kTabFloat4) ? 1 : 0;
+      w.tbh = w.mxy - w.mny + 1;
+      w.xrs = tab_row_stride(w.tbw + 1);
+      w.yrs = tab_row_stride(w.tbw);
+      w.yoff = w.tbh * w.xrs;
+      w.tab = (kTab && w.use && w.yoff + (w.tbh + 1) * w.yrs <= kTabFloat4) ? 1 : 0;
     }
     s_w = w;
   }
@@ -633,21 +638,24 @@ __global__ void __launch_bounds__(kThreads, ORDER == 5 ? 2 : (PUSH && (!BZU || !
     if (kTab && w.tab) {
       // four polynomials per box cell: Ex below / above the half offset, Ey likewise
       const int nx = g.nx;
+      // Ex: one polynomial per half-shifted column h (half = mnx - 1 + h, h in
+      // [0, tbw]) and row; Ey: per column and half-shifted row (as h in y).
       float4* tb = reinterpret_cast<float4*>(sEx);
-      const int cells = w.tbw * (w.mxy - w.mny + 1);
-      for (int e = tid; e < 4 * cells; e += kThreads) {
-        const int c = e >> 2, q = e & 3, p = q & 1;
-        const int col = c % w.tbw, row = c / w.tbw;
-        const int ix = w.mnx + col, iy = w.mny + row;
-        const float* src = q < 2 ? f.Ex : f.Ey;
-        const int stride = q < 2 ? nx + 2 : nx + 1;
-        const int c0 = q < 2 ? ix - ngb + p : ix - ngb, r0 = q < 2 ? iy - ngb : iy - ngb + p;
+      const int nxe = (w.tbw + 1) * w.tbh, total = nxe + w.tbw * (w.tbh + 1);
+      for (int e = tid; e < total; e += kThreads) {
+        const bool ex = e < nxe;
+        const int t = ex ? e : e - nxe;
+        const int rw = ex ? w.tbw + 1 : w.tbw;  // entries per table row
+        const int col = t % rw, row = t / rw;
+        const float* src = ex ? f.Ex : f.Ey;
+        const int stride = ex ? nx + 2 : nx + 1;
+        const int c0 = w.mnx - ngb + col, r0 = w.mny - ngb + row;  // taps c0..c0+3, r0..r0+3
         float F[16];
 #pragma unroll
         for (int j = 0; j < 4; ++j)
 #pragma unroll
           for (int i = 0; i < 4; ++i) F[i + 4 * j] = __ldg(src + (c0 + i) + (r0 + j) * stride);
-        tab_build(F, tb + row * w.trs + kTabStride * col + 4 * q);
+        tab_build(F, tb + (ex ? row * w.xrs : w.yoff + row * w.yrs) + kTabEntry * col);
       }
     } else if constexpr (PUSH) {
       const int nx = g.nx, ny = g.ny;
@@ -737,10 +745,10 @@ __global__ void __launch_bounds__(kThreads, ORDER == 5 ? 2 : (PUSH && (!BZU || !
           float wxn[ORDER + 1], wxh[ORDER + 1], wyn[ORDER + 1], wyh[ORDER + 1];
           float Epx = 0.0f, Epy = 0.0f, Bpz = 0.0f;
           if (kTab && in_box_win && s_w.tab) {  // read from shared memory: no register held across the loop
-            const float4* tb =
-                reinterpret_cast<const float4*>(sEx) + (iy - w.mny) * s_w.trs + kTabStride * (ix - w.mnx);
-            Epx = tab_eval(tb + (ox >= 0.5f ? 4 : 0), sx.hhalf, oy);
-            Epy = tab_eval(tb + (oy >= 0.5f ? 12 : 8), ox, sy.hhalf);
+            const float4* tb = reinterpret_cast<const float4*>(sEx);
+            const int cx = ix - w.mnx, cy = iy - w.mny;
+            Epx = tab_eval(tb + cy * s_w.xrs + kTabEntry * (cx + (ox >= 0.5f ? 1 : 0)), sx.hhalf, oy);
+            Epy = tab_eval(tb + s_w.yoff + (cy + (oy >= 0.5f ? 1 : 0)) * s_w.yrs + kTabEntry * cx, ox, sy.hhalf);
           } else {
             shape<ORDER>(sx.hnode, wxn);
             shape<ORDER>(sx.hhalf, wxh);
