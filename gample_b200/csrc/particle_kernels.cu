@@ -528,7 +528,8 @@ __global__ void __launch_bounds__(kThreads, ORDER == 5 ? 2 : (PUSH && (!BZU || !
   // stencil sum that every other path evaluates, so a particle's field would
   // depend on its chunk's box; the deterministic mode (DET, also passed to its
   // pushes without deposit) keeps the stencil sum everywhere.
-  constexpr bool kTab = PUSH && BZU && ORDER == 3 && !DET;
+  // (not with currents: the two paths together exceed the 64 registers of order 3)
+  constexpr bool kTab = PUSH && BZU && ORDER == 3 && !DET && !CUR;
   extern __shared__ __align__(16) unsigned char smem[];
   float* sEx = reinterpret_cast<float*>(smem);
   float* sEy = sEx + (PUSH ? kWin : 0);
