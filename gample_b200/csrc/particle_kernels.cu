@@ -341,8 +341,10 @@ __device__ __forceinline__ void deposit_priv(const Window& w, uint32_t lane_base
 // Gather table (order 3, uniform Bz). Inside one cell, for a fixed choice of
 // the half-shifted stencil (offset below or above 1/2), the gathered field is
 // a bicubic polynomial of the particle's offsets: Ex(hx, oy) with hx the
-// half-shifted x offset and Ey(ox, hy). The CTA tabulates the monomial
-// coefficients of the four polynomials of every cell of its box,
+// half-shifted x offset and Ey(ox, hy). An Ex polynomial belongs to a
+// half-shifted column (the upper half of one cell and the lower half of the
+// next) and a row, an Ey polynomial to a column and a half-shifted row. The
+// CTA tabulates the monomial coefficients of every polynomial its box needs,
 //   C[n][m] = sum_i sum_j A[i][m] A[j][n] F(tap i, tap j),
 // with A[i][m] the coefficient of h^m in the cubic B-spline weight of tap i
 // (shape<3>), and a particle evaluates its two polynomials by Horner's rule:
