@@ -336,7 +336,7 @@ def run_reference(args):
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1e3 * el / max(args.steps, 1), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded reference loader)",
-            "config": config_block(256),
+            "config": config_block(ppc),
             "cpu_baseline": {"value": value, "unit": "particle-pushes/s", "cores": cores, "kind": "port",
                              "sample": f"full 512x512 grid and field solve, {ppc} ppc/species "
                                        f"({2 * ppc * 512 * 512 / 1e6:.1f} M particles) per step; the "
@@ -501,7 +501,7 @@ def main():
     ap.add_argument("--ppc", type=int, default=256)
     ap.add_argument("--cpu-ppc", type=int, default=256)
     ap.add_argument("--cpu-steps", type=int, default=2)
-    ap.add_argument("--ref-ppc", type=int, default=128)
+    ap.add_argument("--ref-ppc", type=int, default=256)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--learned-train", type=int, default=100, help="online training steps of the warm-start network")
     ap.add_argument("--learned-eval", type=int, default=20)

@@ -214,14 +214,18 @@ __global__ void __launch_bounds__(kHoleBlock) k_fill_holes(ParticleArrays p, con
   }
 }
 
-__global__ void k_aos_to_soa(const ParticleStateAoS* in, uint32_t n, ParticleArrays p) {
+// A record is kept live only if its cell lies within the field arrays
+// (0 <= ix <= nx, 0 <= iy <= ny): the cell sort's keys and every stencil
+// start from there. Anything else, or a non-finite position, is an invalid state.
+__global__ void k_aos_to_soa(const ParticleStateAoS* in, uint32_t n, ParticleArrays p, int nx, int ny) {
   for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
     const ParticleStateAoS r = in[k];
-    const float fx = floorf(r.x), fy = floorf(r.y);
+    const bool fin = isfinite(r.x) && isfinite(r.y) && fabsf(r.x) < 1.0e7f && fabsf(r.y) < 1.0e7f;
+    const float fx = fin ? floorf(r.x) : 0.0f, fy = fin ? floorf(r.y) : 0.0f;
     int ix = int(fx), iy = int(fy);
-    bool ok = isfinite(r.x) && isfinite(r.y) && ix >= 0 && iy >= 0 && ix < 65536 && iy < 32768;
-    if (r.piflag > 0 || !ok) {
-      p.cell[k] = -(r.piflag > 0 ? (r.piflag <= 5 ? r.piflag : 5) : 5);
+    bool ok = fin && ix >= 0 && iy >= 0 && ix <= nx && iy <= ny;
+    if (r.piflag != 0 || !ok) {  // a wall code 1..4 is kept; anything else is an invalid state
+      p.cell[k] = -(r.piflag >= 1 && r.piflag <= 4 ? r.piflag : 5);
       p.ox[k] = 0.0f;
       p.oy[k] = 0.0f;
     } else {
@@ -274,9 +278,9 @@ void compact(ParticleArrays p, SpeciesCounters* cnt, const uint32_t* dead_bits, 
   GP_LAUNCH_CHECK();
 }
 
-void aos_to_soa(const ParticleStateAoS* in, uint32_t n, ParticleArrays p, cudaStream_t s) {
+void aos_to_soa(const ParticleStateAoS* in, uint32_t n, ParticleArrays p, int nx, int ny, cudaStream_t s) {
   if (!n) return;
-  k_aos_to_soa<<<grid_for(n), kBlock, 0, s>>>(in, n, p);
+  k_aos_to_soa<<<grid_for(n), kBlock, 0, s>>>(in, n, p, nx, ny);
   GP_LAUNCH_CHECK();
 }
 

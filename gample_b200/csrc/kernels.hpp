@@ -126,7 +126,7 @@ struct ParticleStateAoS {
   float x, y, vx, vy, vz;
   int piflag;
 };
-void aos_to_soa(const ParticleStateAoS* in, uint32_t n, ParticleArrays p, cudaStream_t s);
+void aos_to_soa(const ParticleStateAoS* in, uint32_t n, ParticleArrays p, int nx, int ny, cudaStream_t s);
 void soa_to_aos(ParticleArrays p, uint32_t n, ParticleStateAoS* out, cudaStream_t s);
 
 // ------------------------------------------------------------- generation

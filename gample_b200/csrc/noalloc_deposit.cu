@@ -13,7 +13,11 @@
 //
 // Scratch: the int64 accumulator lives in a file-scope __device__ array of
 // kMaxNodes entries (8 MiB), so grids with (nx+1)(ny+1) > kMaxNodes are
-// rejected. Its address is taken with cudaGetSymbolAddress once per device.
+// rejected. Its device address is looked up with cudaGetSymbolAddress on every
+// call, in the caller's current context (a lookup, not an allocation): an
+// address kept from an earlier call would be stale after cudaDeviceReset or
+// in another context on the same device. The first call on a device may load
+// this library's device code, so it should come before any stream capture.
 // Every call clears the part it uses before depositing (cudaMemsetAsync, no
 // allocation), so nothing has to start at zero; rho is overwritten. All calls
 // on one device share the array: calls that overlap in time (different
@@ -21,7 +25,6 @@
 // each other's results.
 #include <cuda_runtime.h>
 
-#include <mutex>
 #include <stdexcept>
 #include <string>
 
@@ -35,13 +38,9 @@ namespace kern {
 namespace {
 
 constexpr size_t kMaxNodes = size_t(1) << 20;
-constexpr int kMaxDevices = 64;
 constexpr int kBlock = 256;
 
 static __device__ __align__(256) unsigned long long g_noalloc_acc[kMaxNodes];
-
-std::mutex g_addr_mutex;
-unsigned long long* g_addr[kMaxDevices] = {};
 
 // Deterministic fixed-point deposit of one particle record per thread; the
 // record is split into cell and offset as the handle API's upload does, and
@@ -54,7 +53,7 @@ __global__ void k_deposit_records(const ParticleStateAoS* in, uint32_t n, GridDi
     const float fx = floorf(r.x), fy = floorf(r.y);
     const int ix = int(fx), iy = int(fy);
     const bool ok = isfinite(r.x) && isfinite(r.y) && ix >= 0 && iy >= 0 && ix < 65536 && iy < 32768;
-    if (r.piflag > 0 || !ok) continue;
+    if (r.piflag != 0 || !ok) continue;
     const Stagger sx = stagger(ix, __fsub_rn(r.x, fx)), sy = stagger(iy, __fsub_rn(r.y, fy));
     float wx[ORDER + 1], wy[ORDER + 1];
     shape<ORDER>(sx.hnode, wx);
@@ -78,18 +77,11 @@ __global__ void k_round_records(const unsigned long long* acc, size_t n, double 
 }
 
 unsigned long long* scratch_address() {
-  int dev = 0;
-  GP_CUDA(cudaGetDevice(&dev));
-  if (dev < 0 || dev >= kMaxDevices) throw std::invalid_argument("device ordinal out of range");
-  std::lock_guard<std::mutex> lock(g_addr_mutex);
-  if (!g_addr[dev]) {
-    void* p = nullptr;
-    const cudaError_t rc = cudaGetSymbolAddress(&p, g_noalloc_acc);
-    if (rc != cudaSuccess || !p)
-      throw CudaError(rc, std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(rc));
-    g_addr[dev] = static_cast<unsigned long long*>(p);
-  }
-  return g_addr[dev];
+  void* p = nullptr;
+  const cudaError_t rc = cudaGetSymbolAddress(&p, g_noalloc_acc);
+  if (rc != cudaSuccess || !p)
+    throw CudaError(rc, std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(rc));
+  return static_cast<unsigned long long*>(p);
 }
 
 int blocks_for(size_t work) {

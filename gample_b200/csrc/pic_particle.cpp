@@ -143,7 +143,7 @@ void Particle::upload_aos(const kern::ParticleStateAoS* host, uint32_t n) {
     GP_CUDA(cudaMemcpyAsync(stage[a], host + off, size_t(m) * sizeof(*host), cudaMemcpyHostToDevice, st.xfer));
     GP_CUDA(cudaEventRecord(st.ev[a], st.xfer));
     GP_CUDA(cudaStreamWaitEvent(stream, st.ev[a], 0));
-    kern::aos_to_soa(stage[a], m, offset_view(arrays(), off), stream);
+    kern::aos_to_soa(stage[a], m, offset_view(arrays(), off), dims_.nx, dims_.ny, stream);
     GP_CUDA(cudaEventRecord(st.ev[2 + a], stream));
   }
   GP_CUDA(cudaStreamSynchronize(stream));

@@ -101,6 +101,7 @@ __global__ void __launch_bounds__(kThreads) k_gemm(const __nv_bfloat16* __restri
   constexpr int NS = stages<BN, BK>();
   extern __shared__ __align__(128) unsigned char gsm[];
   __shared__ __align__(8) uint64_t mbar[NS];
+  __shared__ __align__(8) uint64_t mbar_drain;  // time-out path: completion of every MMA issued
   __shared__ uint32_t tbase;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
@@ -115,6 +116,7 @@ __global__ void __launch_bounds__(kThreads) k_gemm(const __nv_bfloat16* __restri
   }
   if (tid == 0) {
     for (int i = 0; i < NS; ++i) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(su32(&mbar[i])) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(su32(&mbar_drain)) : "memory");
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -183,18 +185,21 @@ __global__ void __launch_bounds__(kThreads) k_gemm(const __nv_bfloat16* __restri
   for (int t = 0; t < nsteps && ok; ++t) {
     const int tn = t + NS - 2;
     if (tn < nsteps) {
+      bool free_stage = true;
       if (t >= 2) {
         const int sp = (t - 2) % NS;
-        ok = mbar_wait(&mbar[sp], phase[sp]);  // the MMAs of step t - 2 have read it
+        free_stage = mbar_wait(&mbar[sp], phase[sp]);  // the MMAs of step t - 2 have read it
         phase[sp] ^= 1;
-        if (!ok) break;
       }
-      load_step(tn);
+      if (free_stage) load_step(tn);
+      ok = ok && free_stage;
     }
     cp_async_commit();
     cp_async_wait<NS - 2>();
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    __syncthreads();
+    // every thread leaves the loop together when any wait gave up
+    ok = __syncthreads_and(ok) != 0;
+    if (!ok) break;
     if (tid == 0) {
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       const uint32_t aaddr = base + uint32_t((t % NS) * stage_bytes<BN, BK>()), baddr = aaddr + BM * BK * 2;
@@ -221,10 +226,21 @@ __global__ void __launch_bounds__(kThreads) k_gemm(const __nv_bfloat16* __restri
     const int sl = (nsteps - 1) % NS;
     ok = mbar_wait(&mbar[sl], phase[sl]);
   }
-  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  ok = __syncthreads_and(ok) != 0;
   if (!ok) {
-    if (tid == 0) atomicExch(err, 1);
-  } else if (kbeg < kend) {
+    // A wait gave up: MMAs already issued may still read the stages and write
+    // the accumulator. One more commit arrives on mbar_drain once all of them
+    // are complete; wait for it (bounded) before the columns are released.
+    // The launch reports the error either way, so its output is discarded.
+    if (tid == 0)
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                       su32(&mbar_drain))
+                   : "memory");
+    const bool drained = mbar_wait(&mbar_drain, 0);
+    if (tid == 0) atomicExch(err, drained ? 1 : 2);
+  }
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (ok && kbeg < kend) {
     const int row = m0 + warp * 32 + lane;
 #pragma unroll 1
     for (int c0 = 0; c0 < BN; c0 += 16) {

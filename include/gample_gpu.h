@@ -194,10 +194,11 @@ gp_status gp_collision_flux_reinjection(gp_sim* sim, double dt, int* addn);
  * device array); a larger grid returns GP_ERR_CAPACITY. The scratch is
  * cleared by every call, so nothing needs to start at zero. The scratch is
  * shared by all calls on a device: calls that overlap in time (other streams
- * or host threads without ordering) race, so serialise them. The first call
- * on each device looks up the scratch address (cudaGetSymbolAddress) and
- * should come before any stream capture on that device. Asynchronous: errors
- * of the kernels themselves surface at the next synchronisation. */
+ * or host threads without ordering) race, so serialise them. Every call looks
+ * up the scratch address in the current context (cudaGetSymbolAddress, no
+ * allocation); the first call on a device may load the library's device code
+ * and should come before any stream capture on that device. Asynchronous:
+ * errors of the kernels themselves surface at the next synchronisation. */
 gp_status gp_deposit_charge_noalloc(int weighting_order, int ngx, int ngy, const gp_particle_state* particles,
                                     uint32_t n, float scale, float* rho, void* stream);
 

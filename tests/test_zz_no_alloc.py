@@ -1,6 +1,7 @@
 """gp_deposit_charge_noalloc: the allocation-free charge deposit against the
 handle API's deterministic deposit of the same species (bit-identical), two
-calls in a row on caller-owned device memory, plus its capacity check."""
+calls in a row on caller-owned device memory, with flagged records and
+particles on the far walls, plus its capacity check."""
 import ctypes
 
 import numpy as np
@@ -42,8 +43,16 @@ def test_noalloc_deposit_matches_handle_api_twice_in_a_row(gpu, order):
     # against the handle API's deposit of that species alone
     for s in (0, 1):
         recs = sim.particles(s)
-        if s == 0:  # a few flagged records are skipped by both paths
+        if s == 0:
+            # flagged records (a wall code, and a negative code that is no
+            # valid state) are skipped by both paths
             recs["piflag"][::97] = 1
+            recs["piflag"][50::113] = -2
+            # particles exactly on the far walls: the stencil nodes beyond the
+            # arrays carry weight zero and are skipped
+            live = np.nonzero(recs["piflag"] == 0)[0]
+            recs["x"][live[3]] = np.float32(ngx + ngb)
+            recs["y"][live[7]] = np.float32(ngy + ngb)
             sim.set_particles(s, recs)
         dev = torch.from_numpy(recs.view(np.uint8).copy()).cuda()
         scale = float(np.float32(ora.species_consts(s)["scale"]))
