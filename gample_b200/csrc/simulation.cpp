@@ -2,7 +2,9 @@
 #include "simulation.hpp"
 
 #include <sys/stat.h>
+#include <unistd.h>
 
+#include <cstdio>
 #include <stdexcept>
 
 #include "fileio.hpp"
@@ -34,6 +36,11 @@ Simulation::~Simulation() {
     cudaEventDestroy(e.second.first);
     cudaEventDestroy(e.second.second);
   }
+  for (auto& e : timed_) {
+    cudaEventDestroy(e.second.first);
+    cudaEventDestroy(e.second.second);
+  }
+  for (auto e : event_pool_) cudaEventDestroy(e);
   particles.clear();
   field.reset();
   collision.reset();
@@ -54,6 +61,68 @@ void Simulation::mark(int phase, bool begin) {
     events_.push_back({phase, {open_, e}});
     open_ = nullptr;
   }
+}
+
+cudaEvent_t Simulation::take_event() {
+  if (!event_pool_.empty()) {
+    cudaEvent_t e = event_pool_.back();
+    event_pool_.pop_back();
+    return e;
+  }
+  cudaEvent_t e;
+  GP_CUDA(cudaEventCreate(&e));
+  return e;
+}
+
+void Simulation::tic(const std::string& name) {
+  if (!logger || !logger->on()) return;
+  cudaEvent_t a = take_event();
+  GP_CUDA(cudaEventRecord(a, stream));
+  timed_.push_back({name, {a, nullptr}});
+}
+
+void Simulation::toc() {
+  if (!logger || !logger->on() || timed_.empty() || timed_.back().second.second) return;
+  cudaEvent_t b = take_event();
+  GP_CUDA(cudaEventRecord(b, stream));
+  timed_.back().second.second = b;
+}
+
+// elapsedTime (us per timed call) and memoryUsage (kB) of a logged cycle,
+// src/main.mm:237-248. The reference's host clock around synchronous Metal
+// dispatches measures the device work; here each call is bracketed by events
+// on the run's stream. memoryUsage: residentSetSize is the host RSS;
+// physicalFootprint adds the device memory the process holds in its pool
+// (the reference's unified-memory footprint counts its GPU buffers).
+void Simulation::log_resources() {
+  if (!logger || !logger->on()) return;
+  GP_CUDA(cudaStreamSynchronize(stream));
+  std::map<std::string, std::string> et;
+  for (auto& e : timed_) {
+    float ms = 0;
+    if (e.second.second) GP_CUDA(cudaEventElapsedTime(&ms, e.second.first, e.second.second));
+    et[e.first] = std::to_string(static_cast<long long>(double(ms) * 1e3));
+    event_pool_.push_back(e.second.first);
+    if (e.second.second) event_pool_.push_back(e.second.second);
+  }
+  timed_.clear();
+  logger->logSection("elapsedTime", et);
+  long rss_pages = 0;
+  if (FILE* f = std::fopen("/proc/self/statm", "r")) {
+    long total = 0;
+    if (std::fscanf(f, "%ld %ld", &total, &rss_pages) != 2) rss_pages = 0;
+    std::fclose(f);
+  }
+  const unsigned long long rss_kb = static_cast<unsigned long long>(rss_pages) * sysconf(_SC_PAGESIZE) / 1024;
+  unsigned long long dev_bytes = 0;
+  int dev = 0;
+  cudaMemPool_t pool;
+  if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+    size_t used = 0;
+    if (cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used) == cudaSuccess) dev_bytes = used;
+  }
+  logger->logSection("memoryUsage", {{"physicalFootprint", std::to_string(rss_kb + dev_bytes / 1024)},
+                                     {"residentSetSize", std::to_string(rss_kb)}});
 }
 
 void Simulation::phase_times(double out[PH_COUNT]) {
@@ -109,14 +178,24 @@ void Simulation::cycle() {
   if (!fused) {
     mark(PH_DEPOSIT, true);
     field->resetChargeDensity();
-    for (auto* p : ptrs) p->integrateChargeDensity(*field);
+    for (auto* p : ptrs) {
+      tic("integCDens_" + p->pName);
+      p->integrateChargeDensity(*field);
+      toc();
+    }
     mark(PH_DEPOSIT, false);
   }
   const int em = init.flagForEquation.EMField;
   if (em == 1 || em == 2) {
     mark(PH_SOLVE, true);
+    tic("solvePoisson");
     last_solve = field->solvePoisson(dt, logger.get());
-    if (em == 2) field->solveVectorPotential(dt, logger.get());  // src/main.mm:187-190
+    toc();
+    if (em == 2) {  // src/main.mm:187-190
+      tic("solveVectorPotential");
+      field->solveVectorPotential(dt, logger.get());
+      toc();
+    }
     mark(PH_SOLVE, false);
   }
   const bool field_out = file_output && T.FieldOutput != 0 && cycle_no % T.FieldOutput == 0;
@@ -129,10 +208,14 @@ void Simulation::cycle() {
       mark(PH_SORT, false);
     }
     mark(PH_PUSH, true);
+    tic("update_" + ptrs[s]->pName);
     ptrs[s]->update(dt, *field, fused);
+    toc();
     mark(PH_PUSH, false);
     mark(PH_REDUCE, true);
+    tic("reduce_" + ptrs[s]->pName);
     last_flow[s] = ptrs[s]->reduce(logger.get());
+    toc();
     mark(PH_REDUCE, false);
     if (file_output && T.ParticleOutput != 0 && cycle_no % T.ParticleOutput == 0)  // :211-214
       outputPhaseSpace(cycle_no, *ptrs[s], init);
@@ -142,16 +225,27 @@ void Simulation::cycle() {
     }
   }
   mark(PH_SOURCE, true);
+  tic("artificialIonization");
   last_ai = collision->artificialIonization(dt, ptrs, logger.get());
+  toc();
+  tic("hollowCathode");
   last_hc = collision->hollowCathode(dt, ptrs, logger.get());
+  toc();
+  tic("fluxReinjection");
   last_reflux = collision->fluxReinjection(dt, ptrs, logger.get());
-  if (fused)
-    for (auto* p : ptrs) p->integrateChargeDensity(*field, true);
+  toc();
+  if (fused)  // the injected particles' charge (the rest came with the push)
+    for (auto* p : ptrs) {
+      tic("integCDens_" + p->pName);
+      p->integrateChargeDensity(*field, true);
+      toc();
+    }
   mark(PH_SOURCE, false);
   // src/main.mm:237-243 (guarded by FieldOutput there; a zero ProgressOutput
   // would divide by zero and is treated as "never")
   if (file_output && T.FieldOutput != 0 && T.ProgressOutput != 0 && cycle_no % T.ProgressOutput == 0)
     if (!saveProgress(cycle_no, ptrs, init)) throw std::runtime_error("output progress failed.");
+  log_resources();
   if (logger) logger->logCycleEnd();
 }
 

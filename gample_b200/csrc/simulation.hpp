@@ -57,6 +57,14 @@ class Simulation {
 
  private:
   void mark(int phase, bool begin);
+  // elapsedTime section of a logged cycle (src/main.mm:167-243): device time
+  // of each timed call between two events on the run's stream, in us.
+  void tic(const std::string& name);
+  void toc();
+  void log_resources();
+  cudaEvent_t take_event();
+  std::vector<std::pair<std::string, std::pair<cudaEvent_t, cudaEvent_t>>> timed_;
+  std::vector<cudaEvent_t> event_pool_;
   bool profiling_ = false;
   std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> events_;
   cudaEvent_t open_ = nullptr;

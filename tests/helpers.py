@@ -117,3 +117,75 @@ def read_field_file(path):
         records[name] = (tid, np.frombuffer(buf[off + 36:off + 36 + 4 * n], np.float32).reshape(shape))
         off += 36 + 4 * n
     return {"ngx": int(ngx), "ngy": int(ngy), "ngb": int(ngb), "dx": float(dx), "dy": float(dy)}, records
+
+
+C_LIGHT = 2.99792458e10
+EV_ERG = 1.6021764262e-12
+
+
+def plasma_scales(density=5e10, te_ev=10.0):
+    """Debye length (cm) and electron plasma frequency (rad/s) of an
+    electron population (CGS)."""
+    import math
+    lam_d = math.sqrt(te_ev * EV_ERG / (4 * math.pi * density * EC ** 2))
+    wpe = math.sqrt(4 * math.pi * density * EC ** 2 / ME)
+    return lam_d, wpe
+
+
+def config1(end=200, ppc=64, ngx=128, ngy=128, **kw):
+    """Plain ES-PIC on a doubly periodic grid: dx = 0.5 Debye length, CIC
+    weighting, Boris push in a uniform Bz with w_ce / w_pe = 0.5,
+    dt * w_pe = 0.1, Te = 10 eV, Ti = 0.1 eV, 64 particles per cell per
+    species, Poisson to 1e-8 relative residual."""
+    lam_d, wpe = plasma_scales()
+    bz_gauss = 0.5 * wpe * ME * C_LIGHT / EC
+    args = dict(ngx=ngx, ngy=ngy, order=1, ppc=ppc, xbc="periodic", ybc="periodic", dx=0.5 * lam_d,
+                dt=0.1 / wpe, te=10.0, ti=0.1, bz_tesla=bz_gauss / 1e4, boris=2, density=5e10, end=end, tol=1e-8,
+                maxiter=200)
+    args.update(kw)
+    return condition(**args)
+
+
+def config2(ppc=8, ngx=512, ngy=512, end=1000, reflux=True, **kw):
+    """3rd-order ES-PIC: Dirichlet x walls (phi = 0) with absorbing
+    particles, periodic y, Bz = 0.02 T, dt * w_pe = 0.05, dx = 0.5 Debye
+    length, Te = 10 eV, Ti = 0.1 eV, every absorbed particle re-injected at
+    x = 0 from a flux Maxwellian (GenerateType fluxMaxwellianAtXmin)."""
+    lam_d, wpe = plasma_scales()
+    sources = None
+    if reflux:
+        sources = [{"ParticleName": name, "GenerateType": "fluxMaxwellianAtXmin",
+                    "SrcSetMethod": "AbsorbedParticleNumber", "GenerateTemp": t}
+                   for name, t in (("electron", 10.0), ("ion_Xe1", 0.1))]
+    args = dict(ngx=ngx, ngy=ngy, order=3, ppc=ppc, xbc="Dirichlet", ybc="periodic", pbc_x="Delete",
+                pbc_y="periodic", dx=0.5 * lam_d, dt=0.05 / wpe, te=10.0, ti=0.1, bz_tesla=0.02, boris=2,
+                density=5e10, end=end, tol=1e-8, maxiter=100, sources=sources,
+                pnum_max=int(2 * ppc * ngx * ngy * 1.05) + 4096)
+    args.update(kw)
+    return condition(**args)
+
+
+def multiset_match(a, b, scales, periods):
+    """Match two particle sets (dicts or record arrays with x, y, vx, vy, vz)
+    one to one by nearest neighbour in scaled coordinates (positions over
+    `scales[0:2]`, velocities over `scales[2:5]`; `periods` gives the
+    periodic length of each position coordinate or None). Returns the largest
+    matched distance and whether the matching is a bijection."""
+    from scipy.spatial import cKDTree
+    big = 1e6
+
+    def pts(p):
+        cols = []
+        for i, c in enumerate(("x", "y", "vx", "vy", "vz")):
+            v = np.asarray(p[c], np.float64) / scales[i]
+            if i < 2 and periods[i] is not None:
+                v = np.mod(v, periods[i] / scales[i])
+            else:
+                v = v + big / 2
+            cols.append(v)
+        return np.stack(cols, axis=1)
+
+    box = [periods[i] / scales[i] if i < 2 and periods[i] is not None else 4 * big for i in range(5)]
+    tree = cKDTree(pts(b), boxsize=box)
+    d, idx = tree.query(pts(a), k=1)
+    return float(np.max(d)) if len(d) else 0.0, bool(np.unique(idx).size == len(idx) == len(b))
