@@ -521,38 +521,17 @@ __host__ __device__ constexpr size_t smem_bytes() {
          (DEP ? DepositLayout<ORDER, CUR, DET>::kBytes : 0);
 }
 
+// Phases A and B of a chunk (shared by the push / deposit kernels): the box
+// of the chunk's cells, the shared-memory field window or gather table
+// covering it, and the cleared deposit window. Returns the window (also in s_w).
 template <int ORDER, bool PUSH, bool DEP, bool DET, bool CUR, bool BZU>
-__global__ void __launch_bounds__(kThreads, ORDER == 5 ? 2 : (PUSH && (!BZU || !DEP) ? 3 : 4)) k_pic(GridDims g, ParticleArrays p, FieldPtrs f, PushConsts c,
-                                                  int boris_order, DepositTargets d, SpeciesCounters* cnt,
-                                                  uint32_t* dead_bits, int injected_only) {
+__device__ __forceinline__ Window chunk_setup(const GridDims& g, const ParticleArrays& p, const FieldPtrs& f,
+                                            uint32_t n, uint32_t base, int tid, int lane, int wid, float* sEx,
+                                            float* sEy, float* sBz, int* sDep, int (*s_red)[kThreads / 32],
+                                            Window& s_w, int32_t& s_ref) {
   using DL = DepositLayout<ORDER, CUR, DET>;
-  // Gather tables (they replace the Ex/Ey windows) round differently from the
-  // stencil sum that every other path evaluates, so a particle's field would
-  // depend on its chunk's box; the deterministic mode (DET, also passed to its
-  // pushes without deposit) keeps the stencil sum everywhere.
-  // (not with currents: the two paths together exceed the 64 registers of order 3)
   constexpr bool kTab = PUSH && BZU && ORDER == 3 && !DET && !CUR;
-  extern __shared__ __align__(16) unsigned char smem[];
-  float* sEx = reinterpret_cast<float*>(smem);
-  float* sEy = sEx + (PUSH ? kWin : 0);
-  float* sBz = sEy + (PUSH ? kWin : 0);
-  // copy c of array a starts at (a * kCopies + c) * kStride; arrays: rho hi,
-  // rho lo, jx hi, jx lo, jy hi, jy lo
-  int* sDep = reinterpret_cast<int*>(smem + (PUSH ? (BZU ? 2 : 3) * size_t(kWin) * sizeof(float) : 0));
-  __shared__ int s_red[4][kThreads / 32];
-  __shared__ Window s_w;
-  __shared__ int32_t s_ref;
-
-  const uint32_t n = cnt->n;
-  const uint32_t first = (!PUSH && injected_only) ? n - cnt->n_injected : 0u;
-  const uint32_t base = first + blockIdx.x * uint32_t(kChunk);
-  if (base >= n) return;  // uniform over the block
-  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   const int ngb = g.ngb;
-  const int copy = (lane / DL::kN2) % DL::kCopies;
-  WinPtrs sw;
-  sw.rho = static_cast<uint32_t>(__cvta_generic_to_shared(sDep + copy * DL::kStride));
-
   // ---- phase A: box of the chunk's cells (re-read from L1 below). Only
   // particles within kReach cells of the chunk's middle particle count, so
   // that a few strays (holes filled by compaction, injected particles) do not
@@ -634,7 +613,6 @@ __global__ void __launch_bounds__(kThreads, ORDER == 5 ? 2 : (PUSH && (!BZU || !
   }
   __syncthreads();
   const Window w = s_w;
-  const uint32_t priv_base = static_cast<uint32_t>(__cvta_generic_to_shared(sDep)) + 4u * uint32_t(lane * w.ps);
 
   // ---- phase B: stage the field window, clear the deposit window
   if (w.use) {
@@ -681,6 +659,127 @@ __global__ void __launch_bounds__(kThreads, ORDER == 5 ? 2 : (PUSH && (!BZU || !
     }
   }
   __syncthreads();
+
+  return w;
+}
+
+// Phase D: flush the chunk's deposit window with one global atomic per node.
+template <int ORDER, bool DET, bool CUR>
+__device__ __forceinline__ void chunk_flush(const GridDims& g, const PushConsts& c, const DepositTargets& d,
+                                            const int* sDep, const Window& w, int tid) {
+  using DL = DepositLayout<ORDER, CUR, DET>;
+  if (DL::kSingle && w.priv) {
+    const int nx = g.nx, ny = g.ny;
+    const double fr = double(c.scale) / double(1 << DL::kQBits);
+    for (int e = tid; e < kPW * w.dh; e += kThreads) {
+      const int cc = e % kPW;
+      if (cc >= w.dw) continue;
+      const int col = w.dx0 + cc, row = w.dy0 + e / kPW;
+      int r = 0;  // at most 32 * kPer contributions: no overflow (DepositLayout)
+#pragma unroll 8
+      for (int q = 0; q < 32; ++q) r += sDep[q * w.ps + e];
+      if (r != 0 && in_box(col, row, nx + 1, ny + 1)) atomicAdd(d.f64_rho + col + row * (nx + 1), double(r) * fr);
+    }
+  } else if (w.use) {
+    const int nx = g.nx, ny = g.ny;
+    for (int e = tid; e < w.ds * w.dh; e += kThreads) {
+      if (e % w.ds >= w.dw) continue;  // stride padding, never written
+      const int col = w.dx0 + e % w.ds, row = w.dy0 + e / w.ds;
+      long long r = 0, a = 0, b = 0;
+#pragma unroll
+      for (int q = 0; q < DL::kCopies; ++q) {
+        if constexpr (DL::kSingle)
+          r += static_cast<long long>(sDep[q * DL::kStride + e]);
+        else
+          r += wsum(sDep, (0 * DL::kCopies + q) * DL::kStride + e, (1 * DL::kCopies + q) * DL::kStride + e);
+        if constexpr (CUR) {
+          a += wsum(sDep, (2 * DL::kCopies + q) * DL::kStride + e, (3 * DL::kCopies + q) * DL::kStride + e);
+          b += wsum(sDep, (4 * DL::kCopies + q) * DL::kStride + e, (5 * DL::kCopies + q) * DL::kStride + e);
+        }
+      }
+      // fast mode: FP64 sums of w * scale (currents w * scale * v)
+      const double unit = DL::kSingle ? 1.0 / double(1 << DL::kQBits) : 0x1p-40;
+      const double fr = double(c.scale) * unit, fj = fr * 2.99792458e10;
+      if (r != 0 && in_box(col, row, nx + 1, ny + 1)) {
+        if constexpr (DET)
+          gadd(d.acc_rho + col + row * (nx + 1), r);
+        else
+          atomicAdd(d.f64_rho + col + row * (nx + 1), double(r) * fr);
+      }
+      if constexpr (CUR) {
+        if (a != 0 && in_box(col, row, nx + 2, ny + 1)) {
+          if constexpr (DET)
+            gadd(d.acc_jx + col + row * (nx + 2), a);
+          else
+            atomicAdd(d.f64_jx + col + row * (nx + 2), double(a) * fj);
+        }
+        if (b != 0 && in_box(col, row, nx + 1, ny + 2)) {
+          if constexpr (DET)
+            gadd(d.acc_jy + col + row * (nx + 1), b);
+          else
+            atomicAdd(d.f64_jy + col + row * (nx + 1), double(b) * fj);
+        }
+      }
+    }
+  }
+}
+
+// Per-warp sums of the push tallies and kinetic energy into the counters.
+__device__ __forceinline__ void flush_tallies(uint32_t tally, double ke, const PushConsts& c, SpeciesCounters* cnt,
+                                              int lane) {
+  auto field = [&](int f) { return warp_sum((tally >> (4 * f)) & 0xFu); };
+  const uint32_t s_dead = field(0);
+  const uint32_t s_w0 = field(1), s_w1 = field(2);
+  const uint32_t s_w2 = field(3), s_w3 = field(4);
+  const uint32_t s_inv = field(5), s_slow = field(6);
+  const double s_ke = warp_sum(ke) * c.ke_half_m * c.ke_w;  // kinetic energy, src/Particle.mm:980-982
+  if (lane == 0) {
+    if (s_dead) atomicAdd(&cnt->n_dead, s_dead);
+    if (s_w0) atomicAdd(&cnt->wall[0], s_w0);
+    if (s_w1) atomicAdd(&cnt->wall[1], s_w1);
+    if (s_w2) atomicAdd(&cnt->wall[2], s_w2);
+    if (s_w3) atomicAdd(&cnt->wall[3], s_w3);
+    if (s_inv) atomicAdd(&cnt->invalid, s_inv);
+    if (s_slow) atomicAdd(&cnt->n_slow, s_slow);
+    if (s_ke != 0.0) atomicAdd(&cnt->ke, s_ke);
+  }
+}
+
+template <int ORDER, bool PUSH, bool DEP, bool DET, bool CUR, bool BZU>
+__global__ void __launch_bounds__(kThreads, ORDER == 5 ? 2 : (PUSH && (!BZU || !DEP) ? 3 : 4)) k_pic(GridDims g, ParticleArrays p, FieldPtrs f, PushConsts c,
+                                                  int boris_order, DepositTargets d, SpeciesCounters* cnt,
+                                                  uint32_t* dead_bits, int injected_only) {
+  using DL = DepositLayout<ORDER, CUR, DET>;
+  // Gather tables (they replace the Ex/Ey windows) round differently from the
+  // stencil sum that every other path evaluates, so a particle's field would
+  // depend on its chunk's box; the deterministic mode (DET, also passed to its
+  // pushes without deposit) keeps the stencil sum everywhere.
+  // (not with currents: the two paths together exceed the 64 registers of order 3)
+  constexpr bool kTab = PUSH && BZU && ORDER == 3 && !DET && !CUR;
+  extern __shared__ __align__(16) unsigned char smem[];
+  float* sEx = reinterpret_cast<float*>(smem);
+  float* sEy = sEx + (PUSH ? kWin : 0);
+  float* sBz = sEy + (PUSH ? kWin : 0);
+  // copy c of array a starts at (a * kCopies + c) * kStride; arrays: rho hi,
+  // rho lo, jx hi, jx lo, jy hi, jy lo
+  int* sDep = reinterpret_cast<int*>(smem + (PUSH ? (BZU ? 2 : 3) * size_t(kWin) * sizeof(float) : 0));
+  __shared__ int s_red[4][kThreads / 32];
+  __shared__ Window s_w;
+  __shared__ int32_t s_ref;
+
+  const uint32_t n = cnt->n;
+  const uint32_t first = (!PUSH && injected_only) ? n - cnt->n_injected : 0u;
+  const uint32_t base = first + blockIdx.x * uint32_t(kChunk);
+  if (base >= n) return;  // uniform over the block
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  const int ngb = g.ngb;
+  const int copy = (lane / DL::kN2) % DL::kCopies;
+  WinPtrs sw;
+  sw.rho = static_cast<uint32_t>(__cvta_generic_to_shared(sDep + copy * DL::kStride));
+
+  const Window w = chunk_setup<ORDER, PUSH, DEP, DET, CUR, BZU>(g, p, f, n, base, tid, lane, wid, sEx, sEy, sBz, sDep,
+                                                                s_red, s_w, s_ref);
+  const uint32_t priv_base = static_cast<uint32_t>(__cvta_generic_to_shared(sDep)) + 4u * uint32_t(lane * w.ps);
 
   // ---- phase C: particles. The loads of a thread's next particle are issued
   // before the current one is processed, so that their latency overlaps the
@@ -857,80 +956,213 @@ __global__ void __launch_bounds__(kThreads, ORDER == 5 ? 2 : (PUSH && (!BZU || !
   // ---- phase D: flush the deposit window
   if constexpr (DEP) {
     __syncthreads();
-    if (DL::kSingle && w.priv) {
-      const int nx = g.nx, ny = g.ny;
-      const double fr = double(c.scale) / double(1 << DL::kQBits);
-      for (int e = tid; e < kPW * w.dh; e += kThreads) {
-        const int cc = e % kPW;
-        if (cc >= w.dw) continue;
-        const int col = w.dx0 + cc, row = w.dy0 + e / kPW;
-        int r = 0;  // at most 32 * kPer contributions: no overflow (DepositLayout)
-#pragma unroll 8
-        for (int q = 0; q < 32; ++q) r += sDep[q * w.ps + e];
-        if (r != 0 && in_box(col, row, nx + 1, ny + 1)) atomicAdd(d.f64_rho + col + row * (nx + 1), double(r) * fr);
-      }
-    } else if (w.use) {
-      const int nx = g.nx, ny = g.ny;
-      for (int e = tid; e < w.ds * w.dh; e += kThreads) {
-        if (e % w.ds >= w.dw) continue;  // stride padding, never written
-        const int col = w.dx0 + e % w.ds, row = w.dy0 + e / w.ds;
-        long long r = 0, a = 0, b = 0;
-#pragma unroll
-        for (int q = 0; q < DL::kCopies; ++q) {
-          if constexpr (DL::kSingle)
-            r += static_cast<long long>(sDep[q * DL::kStride + e]);
-          else
-            r += wsum(sDep, (0 * DL::kCopies + q) * DL::kStride + e, (1 * DL::kCopies + q) * DL::kStride + e);
-          if constexpr (CUR) {
-            a += wsum(sDep, (2 * DL::kCopies + q) * DL::kStride + e, (3 * DL::kCopies + q) * DL::kStride + e);
-            b += wsum(sDep, (4 * DL::kCopies + q) * DL::kStride + e, (5 * DL::kCopies + q) * DL::kStride + e);
-          }
-        }
-        // fast mode: FP64 sums of w * scale (currents w * scale * v)
-        const double unit = DL::kSingle ? 1.0 / double(1 << DL::kQBits) : 0x1p-40;
-        const double fr = double(c.scale) * unit, fj = fr * 2.99792458e10;
-        if (r != 0 && in_box(col, row, nx + 1, ny + 1)) {
-          if constexpr (DET)
-            gadd(d.acc_rho + col + row * (nx + 1), r);
-          else
-            atomicAdd(d.f64_rho + col + row * (nx + 1), double(r) * fr);
-        }
-        if constexpr (CUR) {
-          if (a != 0 && in_box(col, row, nx + 2, ny + 1)) {
-            if constexpr (DET)
-              gadd(d.acc_jx + col + row * (nx + 2), a);
-            else
-              atomicAdd(d.f64_jx + col + row * (nx + 2), double(a) * fj);
-          }
-          if (b != 0 && in_box(col, row, nx + 1, ny + 2)) {
-            if constexpr (DET)
-              gadd(d.acc_jy + col + row * (nx + 1), b);
-            else
-              atomicAdd(d.f64_jy + col + row * (nx + 1), double(b) * fj);
-          }
-        }
-      }
+    chunk_flush<ORDER, DET, CUR>(g, c, d, sDep, w, tid);
+  }
+  if constexpr (PUSH) flush_tallies(tally, ke, c, cnt, lane);
+}
+
+// Push + fused deposit for the atomic mode without currents in a uniform Bz
+// (the 512 x 512 benchmark workload and most ensemble members). Phases A, B
+// and D are k_pic's; phase C evaluates the same expressions in the same order
+// (gather tables for order 3, staged windows for orders 1 and 5, Boris,
+// move, boundary conditions, lane-private or rotated single-word deposit
+// windows), so particle states and window sums are bit-identical to
+// k_pic<ORDER, 1, 1, 0, 0, 1>. What differs is the bookkeeping around them:
+// the window parameters a particle needs stay in registers with the box
+// origin folded into the shared-memory base addresses (one multiply-add per
+// address), box tests are one unsigned comparison per axis, and the
+// per-particle reads of the window descriptor from shared memory are gone.
+template <int ORDER>
+__global__ void __launch_bounds__(kThreads, ORDER == 5 ? 2 : 4)
+    k_push_fast(GridDims g, ParticleArrays p, FieldPtrs f, PushConsts c, int boris_order, DepositTargets d,
+                SpeciesCounters* cnt, uint32_t* dead_bits) {
+  using DL = DepositLayout<ORDER, false, false>;
+  constexpr int N = ORDER + 1;
+  constexpr bool kTab = ORDER == 3;
+  extern __shared__ __align__(16) unsigned char smem[];
+  float* sEx = reinterpret_cast<float*>(smem);
+  float* sEy = sEx + kWin;
+  int* sDep = reinterpret_cast<int*>(smem + 2 * size_t(kWin) * sizeof(float));
+  __shared__ int s_red[4][kThreads / 32];
+  __shared__ Window s_w;
+  __shared__ int32_t s_ref;
+
+  const uint32_t n = cnt->n;
+  const uint32_t base = blockIdx.x * uint32_t(kChunk);
+  if (base >= n) return;  // uniform over the block
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  const int ngb = g.ngb;
+  const Window w = chunk_setup<ORDER, true, true, false, false, true>(g, p, f, n, base, tid, lane, wid, sEx, sEy,
+                                                                      nullptr, sDep, s_red, s_w, s_ref);
+  WinPtrs sw;
+  sw.rho = static_cast<uint32_t>(__cvta_generic_to_shared(sDep + ((lane / DL::kN2) % DL::kCopies) * DL::kStride));
+
+  // ---- phase C
+  const BorisFactors bz = boris_factors(c.bz_uniform, c.constE, c.constB, boris_order);
+  const bool use = w.use != 0;
+  const bool tab = kTab && use && w.tab;
+  const bool priv = use && w.priv;
+  const int mnx = w.mnx, mny = w.mny;
+  const uint32_t bw = uint32_t(w.mxx - w.mnx), bh = uint32_t(w.mxy - w.mny);
+  // deposit window in cells: [mnx - kMargin, mxx + kMargin] x [mny - kMargin, mxy + kMargin]
+  const int wx0 = mnx - kMargin, wy0 = mny - kMargin;
+  const uint32_t ww = bw + 2 * kMargin, wh = bh + 2 * kMargin;
+  // gather table (float4 units): Ex entry of box cell (cx, cy) and upper half
+  // ux at cy * xrs + 5 (cx + ux), Ey entry at yoff + (cy + uy) * yrs + 5 cx
+  const float4* tbx = reinterpret_cast<const float4*>(sEx) - (mny * w.xrs + kTabEntry * mnx);
+  const float4* tby = reinterpret_cast<const float4*>(sEx) + w.yoff - (mny * w.yrs + kTabEntry * mnx);
+  const int xrs = w.xrs, yrs = w.yrs;
+  // lane-private deposit window: node (col, row) of this lane's copy at
+  // pbase + 4 (col + row kPW) with col = ix (x node index of the stencil base)
+  const uint32_t pbase = static_cast<uint32_t>(__cvta_generic_to_shared(sDep)) + 4u * uint32_t(lane * w.ps) -
+                         4u * uint32_t((ngb + w.dx0) + (ngb + w.dy0) * kPW);
+  constexpr float kUnit = float(1 << DL::kQBits);
+
+  uint32_t tally = 0;
+  double ke = 0.0;
+  int32_t q_cell = -1;
+  float q_ox = 0.0f, q_oy = 0.0f, q_vx = 0.0f, q_vy = 0.0f, q_vz = 0.0f;
+  auto fetch = [&](uint32_t k) {
+    if (k < n) {
+      q_cell = p.cell[k];
+      q_ox = p.ox[k];
+      q_oy = p.oy[k];
+      q_vx = p.vx[k];
+      q_vy = p.vy[k];
+      q_vz = p.vz[k];
     }
+  };
+  fetch(base + uint32_t(tid));
+#pragma unroll 1
+  for (int i = 0; i < kPer; ++i) {
+    const uint32_t k = base + uint32_t(i * kThreads + tid);
+    const int32_t cell = q_cell;
+    float ox = q_ox, oy = q_oy, vx = q_vx, vy = q_vy, vz = q_vz;
+    if (i + 1 < kPer) fetch(k + uint32_t(kThreads));
+    int fl = 0;
+    if (k < n) {
+      if (cell < 0) {
+        fl = -cell;  // flagged before this push and not yet compacted: keep the flag
+      } else {
+        int ix = cell_ix(cell), iy = cell_iy(cell);
+        const bool inb = use && uint32_t(ix - mnx) <= bw && uint32_t(iy - mny) <= bh;
+        float Epx = 0.0f, Epy = 0.0f;
+        if (tab && inb) {
+          const int ux = ox >= 0.5f ? 1 : 0, uy = oy >= 0.5f ? 1 : 0;
+          const float hx = ux ? __fsub_rn(ox, 0.5f) : __fadd_rn(ox, 0.5f);
+          const float hy = uy ? __fsub_rn(oy, 0.5f) : __fadd_rn(oy, 0.5f);
+          Epx = tab_eval(tbx + iy * xrs + kTabEntry * (ix + ux), hx, oy);
+          Epy = tab_eval(tby + (iy + uy) * yrs + kTabEntry * ix, ox, hy);
+        } else {
+          const Stagger sx = stagger(ix, ox), sy = stagger(iy, oy);
+          float wxn[N], wxh[N], wyn[N], wyh[N];
+          shape<ORDER>(sx.hnode, wxn);
+          shape<ORDER>(sx.hhalf, wxh);
+          shape<ORDER>(sy.hnode, wyn);
+          shape<ORDER>(sy.hhalf, wyh);
+          float Bpz = 0.0f;
+          if (inb)
+            gather<ORDER, true, true, false>(g, f, w, sx, sy, wxn, wxh, wyn, wyh, sEx, sEy, nullptr, Epx, Epy, Bpz);
+          else if (interior(g, ix, iy))
+            gather<ORDER, true, false, false>(g, f, w, sx, sy, wxn, wxh, wyn, wyh, sEx, sEy, nullptr, Epx, Epy, Bpz);
+          else
+            gather<ORDER, true, false, true>(g, f, w, sx, sy, wxn, wxh, wyn, wyh, sEx, sEy, nullptr, Epx, Epy, Bpz);
+          if (!inb) tally += 1u << 24;
+        }
+        // Boris push (src/Particle.mm:157-209) with the launch's Bz factors
+        const float etx = __fmul_rn(bz.fe, Epx), ety = __fmul_rn(bz.fe, Epy);
+        const float umx = vx + etx, umy = vy + ety, umz = vz;
+        const float v0x = umx + umy * bz.btz;
+        const float v0y = umy - umx * bz.btz;
+        const float upx = umx + v0y * bz.ssz;
+        const float upy = umy - v0x * bz.ssz;
+        vx = upx + c.constE * Epx;
+        vy = upy + c.constE * Epy;
+        vz = umz;
+        // position update and boundary conditions (src/Particle.mm:212-269)
+        const bool okx = advance(ix, ox, vx, c.constX);
+        const bool oky = advance(iy, oy, vy, c.constY);
+        if (!(okx && oky) || !isfinite(vz)) {
+          fl = 5;
+        } else if (!interior(g, ix, iy)) {
+          if (c.bc[0] == 0) ix = wrap_periodic(ix, ngb, g.ngx);
+          if (c.bc[2] == 0) iy = wrap_periodic(iy, ngb, g.ngy);
+          if (c.bc[0] == 1 && ix < ngb) fl = 1;
+          if (c.bc[1] == 1 && ix >= ngb + g.ngx) fl = 2;
+          if (c.bc[2] == 1 && iy < ngb) fl = 3;
+          if (c.bc[3] == 1 && iy >= ngb + g.ngy) fl = 4;
+          if (c.bc[0] == 2 && ix < ngb) {
+            reflect(ix, ox, ngb);
+            vx = -vx;
+          }
+          if (c.bc[1] == 2 && ix >= ngb + g.ngx) {
+            reflect(ix, ox, ngb + g.ngx);
+            vx = -vx;
+          }
+          if (c.bc[2] == 2 && iy < ngb) {
+            reflect(iy, oy, ngb);
+            vy = -vy;
+          }
+          if (c.bc[3] == 2 && iy >= ngb + g.ngy) {
+            reflect(iy, oy, ngb + g.ngy);
+            vy = -vy;
+          }
+          if (fl == 0 && !interior(g, ix, iy)) fl = 5;
+        }
+        p.vx[k] = vx;
+        p.vy[k] = vy;
+        p.vz[k] = vz;
+        if (fl == 0) {
+          p.cell[k] = pack_cell(ix, iy);
+          p.ox[k] = ox;
+          p.oy[k] = oy;
+          const float vv = __fadd_rn(__fadd_rn(__fmul_rn(vx, vx), __fmul_rn(vy, vy)), __fmul_rn(vz, vz));
+          ke += double(vv);
+          // deposit of the new position (node-centred weights, base = cell)
+          float wxn[N], wyn[N];
+          shape<ORDER>(ox, wxn);
+          shape<ORDER>(oy, wyn);
+          const bool in_win = use && uint32_t(ix - wx0) <= ww && uint32_t(iy - wy0) <= wh;
+          if (priv && in_win) {
+            float rx[N];
+#pragma unroll
+            for (int t = 0; t < N; ++t) rx[t] = __fmul_rn(wxn[t], kUnit);
+            priv_add<N>(pbase + 4u * uint32_t(ix + iy * kPW), rx, wyn);
+          } else {
+            const Stagger nsx = stagger(ix, ox), nsy = stagger(iy, oy);
+            float unused[N];
+            if (in_win)
+              deposit_one<ORDER, false, false, true, false>(g, w, lane, nsx, nsy, wxn, unused, wyn, unused, c.scale,
+                                                            vx, vy, d, sw);
+            else
+              deposit_one<ORDER, false, false, false, false>(g, w, lane, nsx, nsy, wxn, unused, wyn, unused, c.scale,
+                                                             vx, vy, d, sw);
+          }
+        } else {
+          p.cell[k] = -fl;
+        }
+      }
+      if (fl) tally += 1u + (fl <= 4 ? 1u << (4 * fl) : 1u << 20);
+    }
+    const uint32_t wbase = base + uint32_t(i * kThreads + wid * 32);
+    const uint32_t bits = __ballot_sync(0xffffffffu, fl != 0);
+    if (lane == 0 && wbase < n) dead_bits[wbase >> 5] = bits;
   }
 
-  if constexpr (PUSH) {
-    auto field = [&](int f) { return warp_sum((tally >> (4 * f)) & 0xFu); };
-    const uint32_t s_dead = field(0);
-    const uint32_t s_w0 = field(1), s_w1 = field(2);
-    const uint32_t s_w2 = field(3), s_w3 = field(4);
-    const uint32_t s_inv = field(5), s_slow = field(6);
-    const double s_ke = warp_sum(ke) * c.ke_half_m * c.ke_w;  // kinetic energy, src/Particle.mm:980-982
-    if (lane == 0) {
-      if (s_dead) atomicAdd(&cnt->n_dead, s_dead);
-      if (s_w0) atomicAdd(&cnt->wall[0], s_w0);
-      if (s_w1) atomicAdd(&cnt->wall[1], s_w1);
-      if (s_w2) atomicAdd(&cnt->wall[2], s_w2);
-      if (s_w3) atomicAdd(&cnt->wall[3], s_w3);
-      if (s_inv) atomicAdd(&cnt->invalid, s_inv);
-      if (s_slow) atomicAdd(&cnt->n_slow, s_slow);
-      if (s_ke != 0.0) atomicAdd(&cnt->ke, s_ke);
-    }
-  }
+  // ---- phase D
+  __syncthreads();
+  chunk_flush<ORDER, false, false>(g, c, d, sDep, w, tid);
+  flush_tallies(tally, ke, c, cnt, lane);
+}
+
+template <int ORDER>
+void launch_push_fast(uint32_t nblocks, cudaStream_t s, GridDims g, ParticleArrays p, FieldPtrs f, PushConsts c,
+                      int boris, DepositTargets d, SpeciesCounters* cnt, uint32_t* bits) {
+  auto kern = k_push_fast<ORDER>;
+  constexpr size_t bytes = smem_bytes<ORDER, true, true, false, false, true>();
+  static std::once_flag once;
+  std::call_once(once, [&] { GP_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes))); });
+  kern<<<nblocks, kThreads, bytes, s>>>(g, p, f, c, boris, d, cnt, bits);
 }
 
 template <int ORDER, bool PUSH, bool DEP, bool DET, bool CUR, bool BZU>
@@ -985,6 +1217,16 @@ void push(int order, int boris_order, bool dep, bool det, bool cur, bool bzu, Gr
   GP_CUDA(cudaMemsetAsync(&cnt->n_dead, 0, sizeof(SpeciesCounters) - offsetof(SpeciesCounters, n_dead), s));
   if (n_bound == 0) return;
   const uint32_t nblocks = (n_bound + kChunk - 1) / kChunk;
+  if (dep && !det && !cur && bzu) {  // the lean kernel of the common configuration
+    switch (order) {
+      case 1: launch_push_fast<1>(nblocks, s, g, p, f, c, boris_order, d, cnt, dead_bits); break;
+      case 3: launch_push_fast<3>(nblocks, s, g, p, f, c, boris_order, d, cnt, dead_bits); break;
+      case 5: launch_push_fast<5>(nblocks, s, g, p, f, c, boris_order, d, cnt, dead_bits); break;
+      default: throw std::invalid_argument("WeightingOrder must be 1, 3 or 5");
+    }
+    GP_LAUNCH_CHECK();
+    return;
+  }
   switch (order) {
     case 1: dispatch_pic<1, true>(dep, det, cur, bzu, nblocks, s, g, p, f, c, boris_order, d, cnt, dead_bits, 0); break;
     case 3: dispatch_pic<3, true>(dep, det, cur, bzu, nblocks, s, g, p, f, c, boris_order, d, cnt, dead_bits, 0); break;

@@ -49,43 +49,64 @@ def _vth(p):
 
 
 # ------------------------------------------------------------------ config 1
+def _within_fp32_spread(label, err_gpu, err_fp32, floor=1e-6):
+    """Over many cycles two FP32 runs part through the particles' chaotic
+    motion. The CUDA path must stay as close to the FP64 oracle as the FP32
+    oracle (the reference's arithmetic) does: within 3 times its distance."""
+    print(f"{label}: CUDA vs FP64 oracle {err_gpu:.2e}, FP32 oracle vs FP64 oracle {err_fp32:.2e}")
+    assert err_gpu <= 3.0 * err_fp32 + floor, (label, err_gpu, err_fp32)
+
+
 def test_config1_twenty_cycles_match_oracle(gpu):
     cond = config1(end=20)
     sim = capi.Sim(cond)
     ora = L.OracleSim(ocfg.parse(cond))
+    ora64 = L.OracleSim(ocfg.parse(cond), real64=True)
     _sync_initial(sim, ora)
-    probes_g, probes_o, ee_g, ee_o = [], [], [], []
+    ora64.load_initial()
+    ora64.reset_charge()
+    for s in range(2):
+        ora64.deposit(s)
+    ora64.solve_poisson(0.0)
+    probes = {"g": [], "o": [], "d": []}
+    ee = {"g": [], "o": [], "d": []}
     for cyc in range(20):
         sim.run(1)
         st_o, _ = ora.cycle(cyc + 1, faithful=False)
+        st_d, _ = ora64.cycle(cyc + 1, faithful=False)
         st = sim.last_solve()
         for s in range(2):
-            assert sim.count(s) == ora.pnum(s) == 128 * 128 * 64
-        probes_g.append(list(st.probe))
-        probes_o.append(list(st_o.probe))
-        ee_g.append(st.electric_energy)
-        ee_o.append(st_o.energy)
+            assert sim.count(s) == ora.pnum(s) == ora64.pnum(s) == 128 * 128 * 64
         assert st.error <= 1e-8
-    pg, po = np.array(probes_g), np.array(probes_o)
+        for k, v in (("g", st), ("o", st_o), ("d", st_d)):
+            probes[k].append(list(v.probe))
+        ee["g"].append(st.electric_energy)
+        ee["o"].append(st_o.energy)
+        ee["d"].append(st_d.energy)
+    p = {k: np.array(v) for k, v in probes.items()}
     for c in range(3):
-        scale = np.max(np.abs(po[:, c]))
-        err = np.max(np.abs(pg[:, c] - po[:, c])) / scale
-        print(f"config1 probe {c}: max error {err:.2e} of its range")
-        assert err < 1e-4, ("probe", c, err)
-    ee_g, ee_o = np.array(ee_g), np.array(ee_o)
-    assert np.max(np.abs(ee_g - ee_o) / ee_o) < 1e-4
+        scale = np.max(np.abs(p["d"][:, c]))
+        e_g = np.max(np.abs(p["g"][:, c] - p["d"][:, c])) / scale
+        e_o = np.max(np.abs(p["o"][:, c] - p["d"][:, c])) / scale
+        _within_fp32_spread(f"config1 probe {c}", e_g, e_o)
+        assert e_g < 1e-3
+    e = {k: np.array(v) for k, v in ee.items()}
+    _within_fp32_spread("config1 field energy", np.max(np.abs(e["g"] / e["d"] - 1)), np.max(np.abs(e["o"] / e["d"] - 1)))
     # fields of the last solve
     for name in ("Ex", "Ey", "phi"):
-        assert rel_inf(sim.field(name), ora.field(name)) < 1e-4, name
+        _within_fp32_spread(f"config1 {name}", rel_inf(sim.field(name), ora64.field(name)),
+                            rel_inf(ora.field(name), ora64.field(name)))
     # the whole particle multiset, matched one to one
     for s in range(2):
-        g, o = sim.particles(s), ora.particles(s, f32=True)
+        g, o, d = sim.particles(s), ora.particles(s, f32=True), ora64.particles(s)
         assert np.all(g["piflag"] == 0)
-        vth = _vth(o)
-        dmax, bijective = multiset_match(g, o, (1.0, 1.0, vth, vth, vth), (128.0, 128.0))
-        print(f"config1 species {s}: largest matched distance {dmax:.2e} (cells / v_th), bijective {bijective}")
-        assert bijective, s
-        assert dmax < 1e-4, (s, dmax)
+        vth = _vth(d)
+        sc = (1.0, 1.0, vth, vth, vth)
+        dg, bij_g = multiset_match(g, d, sc, (128.0, 128.0))
+        do, bij_o = multiset_match(o, d, sc, (128.0, 128.0))
+        assert bij_g and bij_o, s
+        _within_fp32_spread(f"config1 species {s} particles (cells / v_th)", dg, do)
+        assert dg < 1e-3
 
 
 @pytest.mark.slow
@@ -137,7 +158,6 @@ def test_config2_push_and_fused_deposit_at_64ppc_match_oracle(gpu):
         sim.set_field(name, ora.field(name).astype(np.float32))
     dt = cond["ParamForTimeIntegration"]["TimeStep"]
     ngx = ngy = 512
-    ora64 = L.OracleSim(ocfg.parse(cond), real64=True)
     for s in range(2):
         o = ora.particles(s, f32=True)
         perm = _tile_order(o["x"], o["y"])
@@ -167,11 +187,19 @@ def test_config2_push_and_fused_deposit_at_64ppc_match_oracle(gpu):
                 dg = (dg - dr + period / 2) % period - period / 2 + dr
             ulp = np.spacing((np.abs(r[c][live]) + (period or 0)).astype(np.float32)).astype(np.float64)
             assert np.all(np.abs(dg - dr) <= 4 * ulp + 1e-5 * (np.abs(dr) + vth * cst[k])), c
-        # the fused deposit of the pushed particles against the FP64 oracle
-        ora64.set_particles(s, g["x"][live], g["y"][live], g["vx"][live], g["vy"][live], g["vz"][live])
-        ora64.reset_charge()
-        ora64.deposit(s)
-        assert rel_inf(sim.field("rho"), ora64.field("rho")) < 2e-7, s
+        # The fused deposit of the pushed particles against an exact deposit of
+        # the same states. The states must be taken as cell + offset: a float
+        # position near x = 512 carries 3e-5 cells of rounding, which would
+        # move the reference sum by more than the deposit's own error.
+        raw = sim.particles_raw(s)
+        ok = raw["cell"] >= 0
+        ix = (raw["cell"][ok] & 0xFFFF).astype(np.int32)
+        iy = (raw["cell"][ok] >> 16).astype(np.int32)
+        acc = L.det_deposit_rho(3, ngx, ngy, 1, ix, iy, raw["ox"][ok], raw["oy"][ok])  # 2^-40 fixed point
+        exact = acc.astype(np.float64) * (np.float64(np.float32(cst["scale"])) * 2.0 ** -40)
+        err = rel_inf(sim.field("rho"), exact)
+        print(f"config2 64 ppc species {s}: fused deposit error {err:.2e} of the peak charge")
+        assert err < 2e-7, s
 
 
 def _flux_maxwellian_moments(p, vth, label):
@@ -224,10 +252,16 @@ def test_config2_cycles_with_resort_compaction_reflux_match_oracle(gpu):
                 for c in ("x", "y"):
                     np.testing.assert_allclose(g[c], o[c], rtol=2e-6, atol=1e-5)
                 injected[s].append(g)
-        # the CSV probe (phi, Ex, Ey at one node) against the field's own scale
+        # The CSV probe (phi, Ex, Ey at one node) against the field's own
+        # scale. The first cycle solves the charge of the load, where every
+        # ion sits on an electron: rho is rounding noise on both sides, so
+        # the comparison starts with the second cycle.
         for c, name in enumerate(("phi", "Ex", "Ey")):
             scale = np.max(np.abs(ora.field(name)))
-            assert abs(st.probe[c] - st_o.probe[c]) <= 1e-4 * scale, (cyc, name, st.probe[c], st_o.probe[c])
+            err = abs(st.probe[c] - st_o.probe[c]) / scale
+            print(f"config2 cycle {cyc} probe {name}: error {err:.2e} of the field's peak")
+            if cyc > 0:
+                assert err <= 1e-4, (cyc, name, st.probe[c], st_o.probe[c])
     # electrons only: the cold ions (Ti = 0.1 eV) hardly reach a wall in four steps
     _flux_maxwellian_moments(np.concatenate(injected[0]), vth_src[0], "electrons")
     # the 512 x 512 multigrid: residual on the oracle's CSR system and E
