@@ -361,7 +361,9 @@ __device__ __forceinline__ float cubic_coef(int tap, int m) {
 }
 
 // Coefficients of one polynomial from its 4 x 4 taps F[i + 4 j] (i: column
-// tap, j: row tap), stored as four float4 rows c[n] = (C[n][0], ..., C[n][3]).
+// tap, j: row tap), stored by power of h: c[m] = (C[0][m], C[1][m], C[2][m],
+// C[3][m]), so that one 16-byte load holds the coefficient of h^m of all four
+// powers of k and the four Horner chains in h run as two packed pairs.
 __device__ __forceinline__ void tab_build(const float (&F)[16], float4* c) {
   float T[4][4];  // T[i][n] = sum_j F(i, j) A[j][n]
 #pragma unroll
@@ -374,27 +376,33 @@ __device__ __forceinline__ void tab_build(const float (&F)[16], float4* c) {
       T[i][n] = t;
     }
 #pragma unroll
-  for (int n = 0; n < 4; ++n) {
+  for (int m = 0; m < 4; ++m) {
     float r[4];
 #pragma unroll
-    for (int m = 0; m < 4; ++m) {
+    for (int n = 0; n < 4; ++n) {
       float t = 0.0f;
 #pragma unroll
       for (int i = 0; i < 4; ++i) t = fmaf(cubic_coef(i, m), T[i][n], t);
-      r[m] = t;
+      r[n] = t;
     }
-    c[n] = make_float4(r[0], r[1], r[2], r[3]);
+    c[m] = make_float4(r[0], r[1], r[2], r[3]);
   }
 }
 
-// sum_n k^n sum_m C[n][m] h^m
+// sum_n k^n sum_m C[n][m] h^m: p_n = ((C[n][3] h + C[n][2]) h + C[n][1]) h +
+// C[n][0] for n = 0, 1 and n = 2, 3 as packed FP32 pairs (sm_100 FFMA2; each
+// half rounds exactly like the scalar fused multiply-add), then Horner in k.
 __device__ __forceinline__ float tab_eval(const float4* c, float h, float k) {
   const float4 c0 = c[0], c1 = c[1], c2 = c[2], c3 = c[3];
-  const float p0 = fmaf(fmaf(fmaf(c0.w, h, c0.z), h, c0.y), h, c0.x);
-  const float p1 = fmaf(fmaf(fmaf(c1.w, h, c1.z), h, c1.y), h, c1.x);
-  const float p2 = fmaf(fmaf(fmaf(c2.w, h, c2.z), h, c2.y), h, c2.x);
-  const float p3 = fmaf(fmaf(fmaf(c3.w, h, c3.z), h, c3.y), h, c3.x);
-  return fmaf(fmaf(fmaf(p3, k, p2), k, p1), k, p0);
+  const float2 hh = make_float2(h, h);
+  float2 p01 = make_float2(c3.x, c3.y), p23 = make_float2(c3.z, c3.w);
+  p01 = __ffma2_rn(p01, hh, make_float2(c2.x, c2.y));
+  p23 = __ffma2_rn(p23, hh, make_float2(c2.z, c2.w));
+  p01 = __ffma2_rn(p01, hh, make_float2(c1.x, c1.y));
+  p23 = __ffma2_rn(p23, hh, make_float2(c1.z, c1.w));
+  p01 = __ffma2_rn(p01, hh, make_float2(c0.x, c0.y));
+  p23 = __ffma2_rn(p23, hh, make_float2(c0.z, c0.w));
+  return fmaf(fmaf(fmaf(p23.y, k, p23.x), k, p01.y), k, p01.x);
 }
 
 // Gather Ex, Ey (and Bz) for one particle (src/Particle.mm:142-154).
@@ -961,6 +969,76 @@ __global__ void __launch_bounds__(kThreads, ORDER == 5 ? 2 : (PUSH && (!BZU || !
   if constexpr (PUSH) flush_tallies(tally, ke, c, cnt, lane);
 }
 
+// Node-centred weights of a particle at offsets h = (hx, hy) for both axes at
+// once: shape<ORDER> evaluated on packed FP32 pairs (each half rounds exactly
+// like the scalar intrinsics), with the x weights scaled by sx, a power of
+// two folded into the constants (scaling by 2^q commutes with every rounding
+// step, so wx[t] == sx * shape<ORDER>(hx)[t] and wy[t] == shape<ORDER>(hy)[t]
+// bit for bit).
+template <int ORDER>
+__device__ __forceinline__ void shape2(float2 h, float sx, float (&wx)[ORDER + 1], float (&wy)[ORDER + 1]) {
+  auto cp = [sx](float v) { return make_float2(v * sx, v); };
+  auto c1 = [](float v) { return make_float2(v, v); };
+  if constexpr (ORDER == 1) {
+    const float2 u = __ffma2_rn(h, cp(-1.0f), cp(1.0f));  // sx (1 - h), 1 - h
+    const float2 v = __fmul2_rn(h, cp(1.0f));
+    wx[0] = u.x, wy[0] = u.y, wx[1] = v.x, wy[1] = v.y;
+  } else if constexpr (ORDER == 3) {
+    constexpr float c6 = 1.0f / 6.0f, c23 = 2.0f / 3.0f;
+    const float2 u = __ffma2_rn(h, c1(-1.0f), c1(1.0f));
+    const float2 h2 = __fmul2_rn(h, h), u2 = __fmul2_rn(u, u);
+    const float2 w0 = __fmul2_rn(__fmul2_rn(u2, u), cp(c6));
+    const float2 w1 = __ffma2_rn(h2, __ffma2_rn(h, cp(0.5f), cp(-1.0f)), cp(c23));
+    const float2 w2 = __ffma2_rn(u2, __ffma2_rn(u, cp(0.5f), cp(-1.0f)), cp(c23));
+    const float2 w3 = __fmul2_rn(__fmul2_rn(h2, h), cp(c6));
+    wx[0] = w0.x, wy[0] = w0.y, wx[1] = w1.x, wy[1] = w1.y;
+    wx[2] = w2.x, wy[2] = w2.y, wx[3] = w3.x, wy[3] = w3.y;
+  } else {
+    constexpr float c120 = 1.0f / 120.0f;
+    constexpr float a0 = 26.0f / 120.0f, a1 = -50.0f / 120.0f, a2 = 20.0f / 120.0f, a3 = 20.0f / 120.0f,
+                    a4 = -20.0f / 120.0f, a5 = 5.0f / 120.0f;
+    constexpr float b0 = 11.0f / 20.0f, b2 = -0.5f, b4 = 0.25f, b5 = -1.0f / 12.0f;
+    const float2 u = __ffma2_rn(h, c1(-1.0f), c1(1.0f));
+    const float2 h2 = __fmul2_rn(h, h), u2 = __fmul2_rn(u, u);
+    const float2 w0 = __fmul2_rn(__fmul2_rn(__fmul2_rn(u2, u2), u), cp(c120));
+    const float2 w5 = __fmul2_rn(__fmul2_rn(__fmul2_rn(h2, h2), h), cp(c120));
+    const float2 w1 = __ffma2_rn(
+        h, __ffma2_rn(h, __ffma2_rn(h, __ffma2_rn(h, __ffma2_rn(h, cp(a5), cp(a4)), cp(a3)), cp(a2)), cp(a1)), cp(a0));
+    const float2 w4 = __ffma2_rn(
+        u, __ffma2_rn(u, __ffma2_rn(u, __ffma2_rn(u, __ffma2_rn(u, cp(a5), cp(a4)), cp(a3)), cp(a2)), cp(a1)), cp(a0));
+    const float2 w2 = __ffma2_rn(h2, __ffma2_rn(h2, __ffma2_rn(h, cp(b5), cp(b4)), cp(b2)), cp(b0));
+    const float2 w3 = __ffma2_rn(u2, __ffma2_rn(u2, __ffma2_rn(u, cp(b5), cp(b4)), cp(b2)), cp(b0));
+    wx[0] = w0.x, wy[0] = w0.y, wx[1] = w1.x, wy[1] = w1.y, wx[2] = w2.x, wy[2] = w2.y;
+    wx[3] = w3.x, wy[3] = w3.y, wx[4] = w4.x, wy[4] = w4.y, wx[5] = w5.x, wy[5] = w5.y;
+  }
+}
+
+// Lane-private single-word windows of the lean push: each contribution is
+// quantised to 2^-kPrivQ of a unit weight with one rounding by
+// fma(wx 2^kPrivQ, wy, 2^23), whose bit pattern is 0x4B000000 + q for
+// 0 <= q < 2^23. The window word of a copy thus accumulates c * 0x4B000000 +
+// sum(q) with c the copy's contributions to the node; c * 0x4B000000 has its
+// low 24 bits clear, so the sum is the low 24 bits as long as it stays below
+// 2^24: a copy takes at most kPer contributions per node (its lane's
+// particles), each at most the largest stencil weight.
+template <int ORDER>
+struct PrivQ {
+  static constexpr int kBits = ORDER == 1 ? 20 : (ORDER == 3 ? 22 : 21);
+  static constexpr double kMaxW = ORDER == 1 ? 1.0 : (ORDER == 3 ? 0.4445 : 0.3026);
+  static_assert(double(kPer) * kMaxW * double(1 << kBits) < 16777216.0, "lane-private window sum exceeds 24 bits");
+  static_assert(kMaxW * double(1 << kBits) < 8388608.0, "contribution outside the exact-integer range of the fma");
+};
+
+template <int N, int K = 0>
+__device__ __forceinline__ void priv_add_fma(uint32_t a0, const float (&rx)[N], const float (&ry)[N]) {
+  if constexpr (K < N * N) {
+    asm volatile("red.shared.add.u32 [%0+%1], %2;" ::"r"(a0), "n"(4 * (K % N + (K / N) * kPW)),
+                 "r"(__float_as_uint(__fmaf_rn(rx[K % N], ry[K / N], 8388608.0f)))
+                 : "memory");
+    priv_add_fma<N, K + 1>(a0, rx, ry);
+  }
+}
+
 // Push + fused deposit for the atomic mode without currents in a uniform Bz
 // (the 512 x 512 benchmark workload and most ensemble members). Phases A, B
 // and D are k_pic's; phase C evaluates the same expressions in the same order
@@ -1016,10 +1094,9 @@ __global__ void __launch_bounds__(kThreads, ORDER == 5 ? 2 : 4)
   // pbase + 4 (col + row kPW) with col = ix (x node index of the stencil base)
   const uint32_t pbase = static_cast<uint32_t>(__cvta_generic_to_shared(sDep)) + 4u * uint32_t(lane * w.ps) -
                          4u * uint32_t((ngb + w.dx0) + (ngb + w.dy0) * kPW);
-  constexpr float kUnit = float(1 << DL::kQBits);
 
   uint32_t tally = 0;
-  double ke = 0.0;
+  float ke = 0.0f;  // sum of |v|^2 over this thread's pushed particles (at most kPer)
   int32_t q_cell = -1;
   float q_ox = 0.0f, q_oy = 0.0f, q_vx = 0.0f, q_vy = 0.0f, q_vz = 0.0f;
   auto fetch = [&](uint32_t k) {
@@ -1117,18 +1194,16 @@ __global__ void __launch_bounds__(kThreads, ORDER == 5 ? 2 : 4)
           p.ox[k] = ox;
           p.oy[k] = oy;
           const float vv = __fadd_rn(__fadd_rn(__fmul_rn(vx, vx), __fmul_rn(vy, vy)), __fmul_rn(vz, vz));
-          ke += double(vv);
+          ke += vv;
           // deposit of the new position (node-centred weights, base = cell)
-          float wxn[N], wyn[N];
-          shape<ORDER>(ox, wxn);
-          shape<ORDER>(oy, wyn);
           const bool in_win = use && uint32_t(ix - wx0) <= ww && uint32_t(iy - wy0) <= wh;
           if (priv && in_win) {
-            float rx[N];
-#pragma unroll
-            for (int t = 0; t < N; ++t) rx[t] = __fmul_rn(wxn[t], kUnit);
-            priv_add<N>(pbase + 4u * uint32_t(ix + iy * kPW), rx, wyn);
+            float rx[N], ry[N];
+            shape2<ORDER>(make_float2(ox, oy), float(1 << PrivQ<ORDER>::kBits), rx, ry);
+            priv_add_fma<N>(pbase + 4u * uint32_t(ix + iy * kPW), rx, ry);
           } else {
+            float wxn[N], wyn[N];
+            shape2<ORDER>(make_float2(ox, oy), 1.0f, wxn, wyn);
             const Stagger nsx = stagger(ix, ox), nsy = stagger(iy, oy);
             float unused[N];
             if (in_win)
@@ -1151,8 +1226,23 @@ __global__ void __launch_bounds__(kThreads, ORDER == 5 ? 2 : 4)
 
   // ---- phase D
   __syncthreads();
-  chunk_flush<ORDER, false, false>(g, c, d, sDep, w, tid);
-  flush_tallies(tally, ke, c, cnt, lane);
+  if (priv) {  // 32 lane-private copies, 24-bit fields (PrivQ)
+    const int nx = g.nx, ny = g.ny;
+    const double fr = double(c.scale) / double(1 << PrivQ<ORDER>::kBits);
+    const uint32_t* sd = reinterpret_cast<const uint32_t*>(sDep);
+    for (int e = tid; e < kPW * w.dh; e += kThreads) {
+      const int cc = e % kPW;
+      if (cc >= w.dw) continue;
+      const int col = w.dx0 + cc, row = w.dy0 + e / kPW;
+      uint32_t r = 0;  // at most 32 * 2^24
+#pragma unroll 8
+      for (int q = 0; q < 32; ++q) r += sd[q * w.ps + e] & 0xFFFFFFu;
+      if (r != 0 && in_box(col, row, nx + 1, ny + 1)) atomicAdd(d.f64_rho + col + row * (nx + 1), double(r) * fr);
+    }
+  } else {
+    chunk_flush<ORDER, false, false>(g, c, d, sDep, w, tid);
+  }
+  flush_tallies(tally, double(ke), c, cnt, lane);
 }
 
 template <int ORDER>
