@@ -188,4 +188,4 @@ def multiset_match(a, b, scales, periods):
     box = [periods[i] / scales[i] if i < 2 and periods[i] is not None else 4 * big for i in range(5)]
     tree = cKDTree(pts(b), boxsize=box)
     d, idx = tree.query(pts(a), k=1)
-    return float(np.max(d)) if len(d) else 0.0, bool(np.unique(idx).size == len(idx) == len(b))
+    return float(np.max(d)) if len(d) else 0.0, bool(np.unique(idx).size == len(idx) == len(b["x"]))
