@@ -182,8 +182,10 @@ struct DepositLayout {
   static constexpr double kMaxW = ORDER == 1 ? 1.0 : (ORDER == 3 ? 0.4445 : 0.3026);
   static_assert(!kSingle || double(kChunk / kCopies) * kMaxW * double(1 << kQBits) < 2147483647.0,
                 "single-word deposit window could overflow");
-  static_assert(!kSingle || 32.0 * kPer * kMaxW * double(1 << kQBits) < 2147483647.0,
-                "sum of the 32 lane-private windows could overflow");
+  // lane-private windows: copy L takes lane L of every warp, kPer particles
+  // each, so at most kPer * (kThreads / 32) contributions per node and word
+  static_assert(!kSingle || double(kPer) * (kThreads / 32) * kMaxW * double(1 << kQBits) < 2147483647.0,
+                "a lane-private window word could overflow");
 };
 
 // This lane's copy of the window arrays: shared-memory byte address of its rho
@@ -312,7 +314,8 @@ __device__ __forceinline__ void deposit_one(const GridDims& g, const Window& w, 
 // fit, lane L adds into its own copy at L * ps words (ps odd, so lanes adding
 // to the same node of their copies hit 32 distinct banks). No stencil
 // rotation is needed, and every node offset is a compile-time immediate of
-// the row stride kPW. A copy receives at most kPer contributions per node.
+// the row stride kPW. Lane L of every warp shares copy L, so a copy receives
+// at most kPer * (kThreads / 32) contributions per node.
 // The products rn(wx * 2^kQBits * wy) are those of the shared layout, so the
 // integer window sums are the same.
 template <int N, int K = 0>
@@ -683,7 +686,9 @@ __device__ __forceinline__ void chunk_flush(const GridDims& g, const PushConsts&
       const int cc = e % kPW;
       if (cc >= w.dw) continue;
       const int col = w.dx0 + cc, row = w.dy0 + e / kPW;
-      int r = 0;  // at most 32 * kPer contributions: no overflow (DepositLayout)
+      // each copy word stays below 2^31 (DepositLayout); the 32 together may
+      // not, so they are summed in 64 bits
+      long long r = 0;
 #pragma unroll 8
       for (int q = 0; q < 32; ++q) r += sDep[q * w.ps + e];
       if (r != 0 && in_box(col, row, nx + 1, ny + 1)) atomicAdd(d.f64_rho + col + row * (nx + 1), double(r) * fr);
@@ -1013,32 +1018,6 @@ __device__ __forceinline__ void shape2(float2 h, float sx, float (&wx)[ORDER + 1
   }
 }
 
-// Lane-private single-word windows of the lean push: each contribution is
-// quantised to 2^-kPrivQ of a unit weight with one rounding by
-// fma(wx 2^kPrivQ, wy, 2^23), whose bit pattern is 0x4B000000 + q for
-// 0 <= q < 2^23. The window word of a copy thus accumulates c * 0x4B000000 +
-// sum(q) with c the copy's contributions to the node; c * 0x4B000000 has its
-// low 24 bits clear, so the sum is the low 24 bits as long as it stays below
-// 2^24: a copy takes at most kPer contributions per node (its lane's
-// particles), each at most the largest stencil weight.
-template <int ORDER>
-struct PrivQ {
-  static constexpr int kBits = ORDER == 1 ? 20 : (ORDER == 3 ? 22 : 21);
-  static constexpr double kMaxW = ORDER == 1 ? 1.0 : (ORDER == 3 ? 0.4445 : 0.3026);
-  static_assert(double(kPer) * kMaxW * double(1 << kBits) < 16777216.0, "lane-private window sum exceeds 24 bits");
-  static_assert(kMaxW * double(1 << kBits) < 8388608.0, "contribution outside the exact-integer range of the fma");
-};
-
-template <int N, int K = 0>
-__device__ __forceinline__ void priv_add_fma(uint32_t a0, const float (&rx)[N], const float (&ry)[N]) {
-  if constexpr (K < N * N) {
-    asm volatile("red.shared.add.u32 [%0+%1], %2;" ::"r"(a0), "n"(4 * (K % N + (K / N) * kPW)),
-                 "r"(__float_as_uint(__fmaf_rn(rx[K % N], ry[K / N], 8388608.0f)))
-                 : "memory");
-    priv_add_fma<N, K + 1>(a0, rx, ry);
-  }
-}
-
 // Push + fused deposit for the atomic mode without currents in a uniform Bz
 // (the 512 x 512 benchmark workload and most ensemble members). Phases A, B
 // and D are k_pic's; phase C evaluates the same expressions in the same order
@@ -1198,9 +1177,9 @@ __global__ void __launch_bounds__(kThreads, ORDER == 5 ? 2 : 4)
           // deposit of the new position (node-centred weights, base = cell)
           const bool in_win = use && uint32_t(ix - wx0) <= ww && uint32_t(iy - wy0) <= wh;
           if (priv && in_win) {
-            float rx[N], ry[N];
-            shape2<ORDER>(make_float2(ox, oy), float(1 << PrivQ<ORDER>::kBits), rx, ry);
-            priv_add_fma<N>(pbase + 4u * uint32_t(ix + iy * kPW), rx, ry);
+            float rx[N], ry[N];  // x weights pre-scaled by the window's fixed-point unit
+            shape2<ORDER>(make_float2(ox, oy), float(1 << DL::kQBits), rx, ry);
+            priv_add<N>(pbase + 4u * uint32_t(ix + iy * kPW), rx, ry);
           } else {
             float wxn[N], wyn[N];
             shape2<ORDER>(make_float2(ox, oy), 1.0f, wxn, wyn);
@@ -1226,22 +1205,7 @@ __global__ void __launch_bounds__(kThreads, ORDER == 5 ? 2 : 4)
 
   // ---- phase D
   __syncthreads();
-  if (priv) {  // 32 lane-private copies, 24-bit fields (PrivQ)
-    const int nx = g.nx, ny = g.ny;
-    const double fr = double(c.scale) / double(1 << PrivQ<ORDER>::kBits);
-    const uint32_t* sd = reinterpret_cast<const uint32_t*>(sDep);
-    for (int e = tid; e < kPW * w.dh; e += kThreads) {
-      const int cc = e % kPW;
-      if (cc >= w.dw) continue;
-      const int col = w.dx0 + cc, row = w.dy0 + e / kPW;
-      uint32_t r = 0;  // at most 32 * 2^24
-#pragma unroll 8
-      for (int q = 0; q < 32; ++q) r += sd[q * w.ps + e] & 0xFFFFFFu;
-      if (r != 0 && in_box(col, row, nx + 1, ny + 1)) atomicAdd(d.f64_rho + col + row * (nx + 1), double(r) * fr);
-    }
-  } else {
-    chunk_flush<ORDER, false, false>(g, c, d, sDep, w, tid);
-  }
+  chunk_flush<ORDER, false, false>(g, c, d, sDep, w, tid);
   flush_tallies(tally, double(ke), c, cnt, lane);
 }
 

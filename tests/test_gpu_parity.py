@@ -239,6 +239,64 @@ def test_fused_deposit_dense_cells_matches_fp64(gpu, order):
     assert rel_inf(sim.field("rho"), ora.field("rho")) < 2e-7
 
 
+def _exact_rho(sim, s, order, ngx, ngy, scale):
+    """Deposit of species s's current device states, taken as cell + offset,
+    with 2^-40 fixed-point weights summed exactly (the oracle's restatement
+    of the deterministic deposit): the reference value for the atomic mode."""
+    raw = sim.particles_raw(s)
+    ok = raw["cell"] >= 0
+    ix = (raw["cell"][ok] & 0xFFFF).astype(np.int32)
+    iy = (raw["cell"][ok] >> 16).astype(np.int32)
+    acc = L.det_deposit_rho(order, ngx, ngy, order // 2, ix, iy, raw["ox"][ok], raw["oy"][ok])
+    return acc.astype(np.float64) * (np.float64(np.float32(scale)) * 2.0 ** -40)
+
+
+@pytest.mark.parametrize("order", [1, 3, 5])
+@pytest.mark.parametrize("ppc", [256, 512])
+def test_fused_deposit_tile_sorted_lane_private_windows(gpu, order, ppc):
+    """Particles in cell-tile order, as the sort leaves them: a 2048-particle
+    chunk covers 4-8 cells, so the fused push + deposit of the atomic mode
+    accumulates in the 32 lane-private windows (lane L of all eight warps
+    sharing copy L). The charge matches an exact deposit of the same pushed
+    states to 2e-7 of its peak."""
+    ngx = ngy = 16
+    cond = condition(ngx=ngx, ngy=ngy, order=order, ppc=ppc, xbc="periodic", ybc="periodic", te=10.0,
+                     bz_tesla=0.02, dt=1e-11)
+    sim, ora = pair(cond)
+    ora.load_initial()
+    for s in range(2):
+        o = ora.particles(s, f32=True)
+        ix, iy = np.floor(o["x"]).astype(np.int64), np.floor(o["y"]).astype(np.int64)
+        perm = np.lexsort((ix % 8, iy % 8, ix // 8, iy // 8))
+        sim.set_particles(s, to_aos(*(o[c][perm] for c in ("x", "y", "vx", "vy", "vz"))))
+        sim.reset_charge()
+        sim.update(s, cond["ParamForTimeIntegration"]["TimeStep"], fused_deposit=True)
+        want = _exact_rho(sim, s, order, ngx, ngy, ora.species_consts(s)["scale"])
+        assert rel_inf(sim.field("rho"), want) < 2e-7, s
+
+
+def test_fused_deposit_hot_spot_sums_beyond_32_bits(gpu):
+    """4096 particles of one species on one node (CIC, offsets below 1e-3):
+    each lane-private window copy takes 64 near-unit contributions and the
+    32 copies of that node sum to about 2^34 fixed-point units, beyond a
+    32-bit word; the flush sums them in 64 bits."""
+    ngx = ngy = 16
+    cond = condition(ngx=ngx, ngy=ngy, order=1, ppc=16, xbc="periodic", ybc="periodic", te=1e-4, ti=1e-4,
+                     dt=1e-12)
+    sim, ora = pair(cond)
+    rng = np.random.default_rng(5)
+    n = 4096
+    x = (5.0 + rng.uniform(0, 1e-3, n)).astype(np.float32)
+    y = (7.0 + rng.uniform(0, 1e-3, n)).astype(np.float32)
+    v = np.zeros(n, np.float32)
+    sim.set_particles(0, to_aos(x, y, v, v, v))
+    sim.reset_charge()
+    sim.update(0, 1e-12, fused_deposit=True)
+    want = _exact_rho(sim, 0, 1, ngx, ngy, ora.species_consts(0)["scale"])
+    assert abs(np.max(np.abs(want)) / abs(np.float32(ora.species_consts(0)["scale"])) - n) < 8  # ~n on one node
+    assert rel_inf(sim.field("rho"), want) < 2e-7
+
+
 def combine_fixed(accs, scales, extra=1.0):
     v = np.zeros(accs[0].shape, np.float64)
     for a, s in zip(accs, scales):
