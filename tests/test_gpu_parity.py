@@ -258,7 +258,9 @@ def test_fused_deposit_tile_sorted_lane_private_windows(gpu, order, ppc):
     chunk covers 4-8 cells, so the fused push + deposit of the atomic mode
     accumulates in the 32 lane-private windows (lane L of all eight warps
     sharing copy L). The charge matches an exact deposit of the same pushed
-    states to 2e-7 of its peak."""
+    states to 2e-7 of its peak for orders 1 and 3 (contributions rounded to
+    2^-22 of a unit weight) and 4e-7 for order 5 (2^-21): a random walk of
+    thousands of roundings per node, far inside the 1e-6 of the atomic mode."""
     ngx = ngy = 16
     cond = condition(ngx=ngx, ngy=ngy, order=order, ppc=ppc, xbc="periodic", ybc="periodic", te=10.0,
                      bz_tesla=0.02, dt=1e-11)
@@ -272,7 +274,7 @@ def test_fused_deposit_tile_sorted_lane_private_windows(gpu, order, ppc):
         sim.reset_charge()
         sim.update(s, cond["ParamForTimeIntegration"]["TimeStep"], fused_deposit=True)
         want = _exact_rho(sim, s, order, ngx, ngy, ora.species_consts(s)["scale"])
-        assert rel_inf(sim.field("rho"), want) < 2e-7, s
+        assert rel_inf(sim.field("rho"), want) < (4e-7 if order == 5 else 2e-7), s
 
 
 def test_fused_deposit_hot_spot_sums_beyond_32_bits(gpu):
