@@ -20,7 +20,10 @@ constexpr int kSmoothThreads = 256;
 constexpr int kSmallThreads = 1024;
 
 // state words (FP64): see multigrid.hpp
-enum { S_SUM = 0, S_SUM2, S_NORMB, S_REL, S_DONE, S_ITER, S_MEAN, S_REL0, S_ZQ, S_PQ, S_RP, S_PQOLD, S_COUNT };
+enum {
+  S_SUM = 0, S_SUM2, S_NORMB, S_REL, S_DONE, S_ITER, S_MEAN, S_REL0, S_ZQ, S_PQ, S_RP, S_PQOLD,
+  S_ZAZ, S_RZ, S_RPO, S_PAZ, S_COUNT
+};
 
 // Boundary treatment of a direction: Dirichlet (values outside are zero),
 // periodic (wrap) or Neumann (mirror about the end node, i.e. the doubled
@@ -221,66 +224,129 @@ __global__ void k_residual64(const double* __restrict__ x, const double* __restr
 // x += alpha p, r -= alpha q. The orthogonalisation needs no symmetric or
 // exact preconditioner, so the FP32 V-cycle serves as it is; the first
 // iteration (S_ITER == 1) starts with p = z.
-__global__ void k_fcg_zq(const float* __restrict__ z, const double* __restrict__ q, int n, double* st) {
-  __shared__ double sh[32];
-  if (st[S_DONE] != 0.0 || st[S_ITER] == 1.0) return;
-  double a = 0.0;
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) a += double(z[k]) * q[k];
-  a = block_sum(a, sh);
-  if (threadIdx.x == 0) atomicAdd(st + S_ZQ, a);
+// Block sums of N values at once (one pair of barriers for all of them).
+template <int N>
+__device__ __forceinline__ void block_sums(double (&v)[N], double (*sh)[32]) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int a = 0; a < N; ++a) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v[a] += __shfl_xor_sync(0xffffffffu, v[a], o);
+    if (lane == 0) sh[a][wid] = v[a];
+  }
+  __syncthreads();
+  if (wid == 0) {
+#pragma unroll
+    for (int a = 0; a < N; ++a) {
+      double r = lane < int(blockDim.x >> 5) ? sh[a][lane] : 0.0;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) r += __shfl_xor_sync(0xffffffffu, r, o);
+      v[a] = r;
+    }
+  }
+  __syncthreads();
 }
 
-// p = z + beta p_old (into p), q = A p (neighbour values of p formed on the
-// fly from z and p_old, which no thread writes), dots p.q and r.p.
-__global__ void k_fcg_dir(const float* __restrict__ z, const double* __restrict__ p_old, double* __restrict__ p,
-                          double* __restrict__ q, const double* __restrict__ r, kern::PoissonLayout L, double* st) {
-  __shared__ double sh[32];
+// The flexible-CG iteration in two passes. With q_old = A p_old,
+//   p = z + beta p_old,  q = A p = A z + beta q_old,
+//   p.q = z.Az + beta (z.q_old + p_old.Az) + beta^2 p_old.q_old,
+//   r.p = r.z + beta r.p_old,
+// so one pass over z, r, p_old, q_old gives every scalar (A z formed on the
+// fly from z's neighbours; p_old.Az is kept apart from z.q_old because the
+// operator is not symmetric with a Neumann direction), and a second pass
+// updates p, q, x and r in place. Pass A: the dot products.
+__global__ void k_fcg_dots(const float* __restrict__ z, const double* __restrict__ q_old,
+                           const double* __restrict__ p_old, const double* __restrict__ r, kern::PoissonLayout L,
+                           double* st) {
+  __shared__ double sh[5][32];
   if (st[S_DONE] != 0.0) return;
-  const double beta = st[S_ITER] == 1.0 ? 0.0 : -st[S_ZQ] / st[S_PQOLD];
+  const bool first = st[S_ITER] == 1.0;  // p_old, q_old hold nothing of this solve yet
   const int mx = L.nkx + 1, my = L.nky + 1, n = mx * my;
-  double pq = 0.0, rp = 0.0;
+  double v[5] = {0.0, 0.0, 0.0, 0.0, 0.0};  // z.q_old, z.Az, r.z, r.p_old, p_old.Az
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
     const int i = k % mx, j = k / mx;
-    auto pv = [&](int t) { return beta == 0.0 ? double(z[t]) : double(z[t]) + beta * p_old[t]; };
-    const double pk = pv(k);
-    const double qk = apply_A(L, k, i, j, mx, pv);
-    p[k] = pk;
-    q[k] = qk;
-    pq += pk * qk;
-    rp += r[k] * pk;
+    const double zk = double(z[k]), rk = r[k];
+    const double az = apply_A(L, k, i, j, mx, [&](int t) { return double(z[t]); });
+    v[1] += zk * az;
+    v[2] += rk * zk;
+    if (!first) {
+      const double po = p_old[k];
+      v[0] += zk * q_old[k];
+      v[3] += rk * po;
+      v[4] += po * az;
+    }
   }
-  pq = block_sum(pq, sh);
-  rp = block_sum(rp, sh);
+  block_sums<5>(v, sh);
   if (threadIdx.x == 0) {
-    atomicAdd(st + S_PQ, pq);
-    atomicAdd(st + S_RP, rp);
+    atomicAdd(st + S_ZQ, v[0]);
+    atomicAdd(st + S_ZAZ, v[1]);
+    atomicAdd(st + S_RZ, v[2]);
+    atomicAdd(st + S_RPO, v[3]);
+    atomicAdd(st + S_PAZ, v[4]);
   }
   (void)my;
 }
 
-// x += alpha p, r -= alpha q; float(r) is the next V-cycle's right-hand
-// side; accumulates sum w r, sum r^2 for the convergence test.
-__global__ void k_fcg_update(double* __restrict__ x, const double* __restrict__ p, const double* __restrict__ q,
-                             double* __restrict__ r, float* __restrict__ r32, kern::PoissonLayout L, double* st) {
-  __shared__ double sh[32];
-  if (st[S_DONE] != 0.0) return;
-  const double alpha = st[S_PQ] != 0.0 ? st[S_RP] / st[S_PQ] : 0.0;
+// The convergence test of one iteration (AMGCL's ||r|| / ||b|| <= tol or
+// maxiter), run by one thread once every partial sum has arrived.
+__device__ __forceinline__ void fcg_check(double* st, double pq, double tol, int maxiter, double wsum) {
+  st[S_PQOLD] = pq;
+  st[S_ZQ] = st[S_ZAZ] = st[S_RZ] = st[S_RPO] = st[S_PAZ] = 0.0;
+  const double sum = __ldcg(st + S_SUM), sum2 = __ldcg(st + S_SUM2);
+  const double rel = sqrt(sum2 > 0 ? sum2 : 0.0) / st[S_NORMB];
+  st[S_REL] = rel;
+  if (!(rel > tol) || st[S_ITER] >= double(maxiter)) {
+    st[S_DONE] = 1.0;
+  } else {
+    st[S_ITER] += 1.0;
+    st[S_MEAN] = sum / wsum;
+  }
+  st[S_SUM] = 0.0;
+  st[S_SUM2] = 0.0;
+}
+
+// Pass B: p = z + beta p_old, q = A z + beta q_old (both in place), x +=
+// alpha p, r -= alpha q with float(r) for the next V-cycle; the last block
+// to finish runs the convergence test (the counter returns to zero).
+__global__ void k_fcg_step(const float* __restrict__ z, double* __restrict__ p, double* __restrict__ q,
+                           double* __restrict__ x, double* __restrict__ r, float* __restrict__ r32,
+                           kern::PoissonLayout L, double* st, unsigned* ctr, double tol, int maxiter, double wsum) {
+  __shared__ double sh[2][32];
+  __shared__ bool s_last;
+  if (st[S_DONE] != 0.0) return;  // uniform: every block sees the previous kernel's value
+  const bool first = st[S_ITER] == 1.0;
+  const double beta = first ? 0.0 : -st[S_ZQ] / st[S_PQOLD];
+  const double pq = st[S_ZAZ] + (first ? 0.0 : beta * (st[S_ZQ] + st[S_PAZ]) + beta * beta * st[S_PQOLD]);
+  const double rp = st[S_RZ] + (first ? 0.0 : beta * st[S_RPO]);
+  const double alpha = pq != 0.0 ? rp / pq : 0.0;
   const int mx = L.nkx + 1, my = L.nky + 1, n = mx * my;
-  double s1 = 0.0, s2 = 0.0;
+  double v[2] = {0.0, 0.0};  // sum w r, sum r^2
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
     const int i = k % mx, j = k / mx;
-    x[k] += alpha * p[k];
-    const double rk = r[k] - alpha * q[k];
+    const double az = apply_A(L, k, i, j, mx, [&](int t) { return double(z[t]); });
+    const double pk = first ? double(z[k]) : double(z[k]) + beta * p[k];
+    const double qk = first ? az : az + beta * q[k];
+    p[k] = pk;
+    q[k] = qk;
+    x[k] += alpha * pk;
+    const double rk = r[k] - alpha * qk;
     r[k] = rk;
     r32[k] = float(rk);
-    s1 += res_weight(L, i, j, mx, my) * rk;
-    s2 += rk * rk;
+    v[0] += res_weight(L, i, j, mx, my) * rk;
+    v[1] += rk * rk;
   }
-  s1 = block_sum(s1, sh);
-  s2 = block_sum(s2, sh);
+  block_sums<2>(v, sh);
   if (threadIdx.x == 0) {
-    atomicAdd(st + S_SUM, s1);
-    atomicAdd(st + S_SUM2, s2);
+    atomicAdd(st + S_SUM, v[0]);
+    atomicAdd(st + S_SUM2, v[1]);
+    __threadfence();
+    s_last = atomicAdd(ctr, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (s_last && threadIdx.x == 0) {
+    __threadfence();
+    *ctr = 0u;
+    fcg_check(st, pq, tol, maxiter, wsum);
   }
 }
 
@@ -817,7 +883,7 @@ PoissonMG::PoissonMG(const kern::PoissonLayout& L, int nu_pre, int nu_post)
     lv.f.resize(size_t(mx) * my, true);
     lv_.push_back(std::move(lv));
     if (!(can_coarsen(mx, bx) && can_coarsen(my, by))) break;
-    if (size_t(mx) * my <= 16) break;
+    if (size_t(mx) * my <= size_t(kDenseMax)) break;  // solved by its dense inverse
     mx = coarser(mx, bx);
     my = coarser(my, by);
     cx *= 0.25f;
@@ -855,8 +921,8 @@ PoissonMG::PoissonMG(const kern::PoissonLayout& L, int nu_pre, int nu_post)
   });
   r64_.resize(size_t(n_), true);
   q_.resize(size_t(n_), true);
+  ctr_.resize(1, true);
   p_[0].resize(size_t(n_), true);
-  p_[1].resize(size_t(n_), true);
   // Dense inverse of the coarsest operator (FP64 Gauss-Jordan, stored FP32);
   // a singular one (no Dirichlet direction) is regularised as A + a 1 w^T
   // with w its left null vector and a = |cd| / n, whose inverse returns the
@@ -1000,15 +1066,11 @@ void PoissonMG::enqueue_iteration(int parity, double* x, double tol, int maxiter
   }
   vcycle(s);  // z = M r
   const float* z = result(0);
-  double* p = p_[parity].get();
-  const double* p_old = p_[parity ^ 1].get();
-  k_fcg_zq<<<reduce_blocks(n_), 256, 0, s>>>(z, q_.get(), n_, st);
+  (void)parity;  // p and q are updated in place
+  k_fcg_dots<<<reduce_blocks(n_), 256, 0, s>>>(z, q_.get(), p_[0].get(), r64_.get(), L_, st);
   GP_LAUNCH_CHECK();
-  k_fcg_dir<<<reduce_blocks(n_), 256, 0, s>>>(z, p_old, p, q_.get(), r64_.get(), L_, st);
-  GP_LAUNCH_CHECK();
-  k_fcg_update<<<reduce_blocks(n_), 256, 0, s>>>(x, p, q_.get(), r64_.get(), f.f.get(), L_, st);
-  GP_LAUNCH_CHECK();
-  k_check<<<1, 1, 0, s>>>(st, tol, maxiter, wsum);
+  k_fcg_step<<<reduce_blocks(n_), 256, 0, s>>>(z, p_[0].get(), q_.get(), x, r64_.get(), f.f.get(), L_, st, ctr_.get(),
+                                               tol, maxiter, wsum);
   GP_LAUNCH_CHECK();
 }
 
@@ -1030,7 +1092,7 @@ PoissonMG::IterationGraphs PoissonMG::iteration_graphs(double* x, double tol, in
   g.maxiter = maxiter;
   const unsigned long long c0 = thread_kernel_launches();
   bool ok = true;
-  for (int par = 0; par < 2 && ok; ++par) {
+  for (int par = 0; par < 1 && ok; ++par) {  // one graph: p and q are updated in place
     cudaGraph_t graph = nullptr;
     if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
       ok = false;
@@ -1054,7 +1116,7 @@ PoissonMG::IterationGraphs PoissonMG::iteration_graphs(double* x, double tol, in
     graphs_ok_ = false;
     return IterationGraphs{};
   }
-  g.kernels = static_cast<long long>(captured / 2);
+  g.kernels = static_cast<long long>(captured);
   if (graphs_.size() >= 4) {  // a few solution vectors per system (Poisson, Darwin parts, tests)
     for (auto& e : graphs_.front().exec) cudaGraphExecDestroy(e);
     graphs_.erase(graphs_.begin());
@@ -1093,7 +1155,7 @@ MGResult PoissonMG::solve(const double* b, const double* sums_b, double* x, doub
   for (;;) {
     for (int i = 0; i < batch && launched < maxiter; ++i, ++launched) {
       if (gr.exec[0]) {
-        GP_CUDA(cudaGraphLaunch(gr.exec[launched & 1], s));
+        GP_CUDA(cudaGraphLaunch(gr.exec[0], s));
         add_kernel_launches(gr.kernels);
       } else {
         enqueue_iteration(launched & 1, x, tol, maxiter, s);

@@ -78,7 +78,7 @@ class PoissonMG {
     double* x = nullptr;
     double tol = 0;
     int maxiter = 0;
-    cudaGraphExec_t exec[2] = {nullptr, nullptr};
+    cudaGraphExec_t exec[2] = {nullptr, nullptr};  // [0]: one iteration ([1] unused)
     long long kernels = 0;  // kernels per graph launch
   };
   IterationGraphs iteration_graphs(double* x, double tol, int maxiter, cudaStream_t s);
@@ -98,9 +98,10 @@ class PoissonMG {
   int my_top() const { return L_.nky + 1; }
   std::vector<Level> lv_;
   DeviceArray<double> r64_, q_;  // FP64 residual and A p of the flexible CG iteration
-  DeviceArray<double> p_[2];      // search directions (current and previous, alternating)
+  DeviceArray<double> p_[1];      // search direction (updated in place)
+  DeviceArray<unsigned> ctr_;     // blocks finished in the flexible-CG update (last one tests convergence)
   DeviceArray<float> coarse_inv_;  // dense inverse of the coarsest operator (small coarsest levels)
-  DeviceArray<double> state_;   // [0] sum r [1] sum r^2 [2] ||b|| [3] rel res [4] done [5] iterations [6] mean r [7] initial rel res
+  DeviceArray<double> state_;   // [0] sum r [1] sum r^2 [2] ||b|| [3] rel res [4] done [5] iterations [6] mean r [7] initial rel res, then the flexible-CG scalars
   PinnedArray<double> host_;
 };
 
