@@ -280,6 +280,36 @@ def ensemble_leg(members, steps, threads, seed=0):
             "wall_s": el, "timing": "host wall clock around the batched run (all members synchronised)"}
 
 
+def steady_state_leg(sim, warm, steps):
+    """The same run continued well past the initial cell sort: `warm` more
+    cycles (absorption and re-injection settle, the electrons drift and the
+    re-sort cadence sets in), then `steps` cycles timed with CUDA events on
+    the library's stream, one call per cycle so that the cycles with a
+    re-sort can be counted."""
+    from gample_b200 import capi
+    sim.run(warm)
+    n0 = sim.count(0) + sim.count(1)
+    l0 = capi.kernel_launches()
+    ms, pulled, sorts = [], [], 0
+    sim.set_profiling(True)
+    prev = sim.phase_times()["sort"]
+    for _ in range(steps):
+        ms.append(sim.time_cycles(1))
+        pulled.append(sim.last_flow(0).pulled + sim.last_flow(1).pulled)
+        t = sim.phase_times()["sort"]
+        sorts += t > prev
+        prev = t
+    sim.set_profiling(False)
+    launches = capi.kernel_launches() - l0
+    n1 = sim.count(0) + sim.count(1)
+    total = sum(ms)
+    return {"cycles_before_timing": warm, "steps": steps, "ms_per_step": total / steps,
+            "pushes_per_s": 0.5 * (n0 + n1) * steps / (total / 1e3),
+            "ms_per_step_min": min(ms), "ms_per_step_max": max(ms), "sorts": int(sorts),
+            "absorbed_per_cycle": sum(pulled) / steps, "gpu_launches_per_step": launches / steps,
+            "timing": "CUDA events per cycle on the library's stream (per-phase events on: ~1 % overhead)"}
+
+
 def dist_setup():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -412,6 +442,7 @@ def run_b200(args):
                 "traffic": traffic, "peak_kind": peak_kind, "kernel": "k_push (gather+Boris+BC+fused deposit)",
                 "algorithmic_bytes_per_particle": BYTES_PER_PUSH,
                 "phase_ms_per_step": {k: v / prof_cycles for k, v in ph.items()}}
+    steady = steady_state_leg(sim, args.steady_warm, args.steady_steps) if args.steady_steps > 0 else None
     sim.close()
     del sim
 
@@ -483,6 +514,7 @@ def run_b200(args):
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
                 "gpu_launches": launches, "gpu_launches_per_step": launches / args.steps,
                 "poisson": poisson_block(iters_last, unknowns, roofline["phase_ms_per_step"]["solve"], peak),
+                "steady_state": steady,
                 "learned_warm_start": learned,
                 "ensemble": ensemble}
         print(json.dumps(line), flush=True)
@@ -508,6 +540,8 @@ def main():
     ap.add_argument("--ensemble", type=int, default=64, help="members of the batched-ensemble leg (0: skip)")
     ap.add_argument("--ensemble-steps", type=int, default=10)
     ap.add_argument("--ensemble-threads", type=int, default=16)
+    ap.add_argument("--steady-warm", type=int, default=200, help="cycles run before the steady-state leg")
+    ap.add_argument("--steady-steps", type=int, default=50, help="cycles timed in the steady-state leg (0: skip)")
     ap.add_argument("--quick", action="store_true", help="timed cycles only (for profiler runs)")
     args = ap.parse_args()
     if args.impl == "reference":

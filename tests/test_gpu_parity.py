@@ -449,6 +449,38 @@ def test_product_reproduces_reference_trace(gpu, name, reference_order, tmp_path
         assert np.all(err <= 2e-4 * np.abs(ref[:, col]) + 3e-4 * scale), (col, err)
 
 
+def test_product_follows_the_recorded_org_3rd_run(gpu, tmp_path):
+    """data/org_3rd.json (500 x 200, order 3, Dirichlet 200 V / 0 V walls,
+    periodic y, Bz from tools/makeBfld.py, 80 particles per cell, an
+    XsinusoidalIonization source and a hollow cathode): the first logged
+    points of the reference's recorded run, every 20 cycles. The code
+    version of that run is unknown, so this is a plausibility check of the
+    early trace (the probe's phi and Ex within a few per cent), not a pin."""
+    import json
+    with open(os.path.join(GOLDEN, "org_3rd.json")) as f:
+        cond = json.load(f)
+    for c in ("x", "y", "z"):
+        cond["ParamForField"]["FilePathOf" + "B" + c] = os.path.join(GOLDEN, f"B{c}_3rd.bin")
+    cond["ParamForTimeIntegration"]["LogOutput"] = 20
+    _, ref = read_trace(os.path.join(GOLDEN, "org_3rd_head_timeseries.csv"))
+    rows = 10
+    log = str(tmp_path / "org3")
+    sim = capi.Sim(cond, log_name=log)
+    sim.initialize()
+    sim.run(20 * rows)
+    sim.close()
+    _, got = read_trace(log + "_timeseries.csv")
+    got, ref = got[:rows], ref[:rows]
+    np.testing.assert_array_equal(got[:, 0], ref[:, 0])
+    np.testing.assert_allclose(got[:, 1], ref[:, 1], rtol=1e-6)
+    for col, name in ((2, "phi"), (3, "Ex"), (4, "Ey")):
+        rel = np.abs(got[:, col] - ref[:, col]) / np.max(np.abs(ref[:, 2 if col == 2 else 3]))
+        print(f"org_3rd {name}: errors over the first {rows} rows (of the phi / Ex scale):",
+              " ".join(f"{e:.3f}" for e in rel))
+    assert np.all(np.abs(got[:, 2] - ref[:, 2]) <= 0.05 * np.abs(ref[:, 2]))
+    assert np.all(np.abs(got[:, 3] - ref[:, 3]) <= 0.10 * np.max(np.abs(ref[:, 3])))
+
+
 def test_fused_order_equals_reference_order(gpu):
     cond = condition(ngx=32, ngy=24, order=3, ppc=16, xbc="Dirichlet", ybc="periodic", deposit_mode=1,
                      bz_tesla=0.02, phi_xmin=20.0, end=5, dt=1e-11)
