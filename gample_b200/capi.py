@@ -94,6 +94,9 @@ EXPORTS = {
     "gp_sim_load_progress": (C.c_int, [C.c_void_p, C.c_int]),
     "gp_field_learned": (C.c_int, [C.c_void_p, C.c_int, C.c_float, C.c_uint64]),
     "gp_field_learned_stats": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "gp_field_learned_bank": (C.c_int, [C.c_void_p, C.c_int]),
+    "gp_field_learned_train": (C.c_int, [C.c_void_p, C.c_int, C.c_float, C.c_uint64, C.c_void_p]),
+    "gp_sim_reload": (C.c_int, [C.c_void_p, C.c_uint64]),
     "gp_ensemble_create": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
     "gp_ensemble_free": (None, [C.c_void_p]),
     "gp_ensemble_initialize": (C.c_int, [C.c_void_p]),
@@ -241,6 +244,18 @@ class Sim:
 
     LEARNED_KEYS = ("loss", "iters_learned", "iters_plain", "ms_learned", "ms_plain", "ms_net", "rel0_learned",
                     "rel0_plain", "trained_steps")
+
+    def reload(self, seed):
+        """The initial load again from master seed `seed` (initialize() follows)."""
+        check(lib().gp_sim_reload(self.h, seed))
+
+    def learned_bank(self, capacity):
+        check(lib().gp_field_learned_bank(self.h, capacity))
+
+    def learned_train(self, steps, lr=1e-3, seed=0):
+        out = (C.c_double * 3)()
+        check(lib().gp_field_learned_train(self.h, steps, lr, seed, out))
+        return {"loss_first": out[0], "loss_last": out[1], "samples": int(out[2])}
 
     def set_learned(self, mode, lr=1e-3, seed=0):
         check(lib().gp_field_learned(self.h, mode, lr, seed))

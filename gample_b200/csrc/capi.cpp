@@ -436,6 +436,12 @@ gp_status gp_ensemble_member(gp_ensemble* e, int i, gp_sim** out) {
     return GP_OK;
   });
 }
+gp_status gp_sim_reload(gp_sim* sim, uint64_t seed) {
+  return guarded([&] {
+    S(sim).reload(seed);
+    return GP_OK;
+  });
+}
 gp_status gp_sim_initialize(gp_sim* sim) {
   return guarded([&] {
     S(sim).initialize();
@@ -547,8 +553,21 @@ gp_status gp_field_solve_darwin(gp_sim* sim, double dt, int iterations[3], doubl
 }
 gp_status gp_field_learned(gp_sim* sim, int mode, float lr, uint64_t seed) {
   return guarded([&] {
-    if (mode < 0 || mode > 7 || !(lr >= 0)) throw std::invalid_argument("learned mode must be 0..7 and lr >= 0");
+    if (mode < 0 || mode > 31 || !(lr >= 0)) throw std::invalid_argument("learned mode must be 0..31 and lr >= 0");
     S(sim).field->setLearned(mode, lr, seed);
+    return GP_OK;
+  });
+}
+gp_status gp_field_learned_bank(gp_sim* sim, int capacity) {
+  return guarded([&] {
+    S(sim).field->setLearnedBank(capacity);
+    return GP_OK;
+  });
+}
+gp_status gp_field_learned_train(gp_sim* sim, int steps, float lr, uint64_t seed, double out[3]) {
+  return guarded([&] {
+    if (steps < 1 || !(lr > 0) || !out) throw std::invalid_argument("steps >= 1, lr > 0 and an output are needed");
+    S(sim).field->trainLearned(steps, lr, seed, out);
     return GP_OK;
   });
 }

@@ -154,6 +154,7 @@ Init Init::parseString(const std::string& text) {
     c.tolerance = float(s.f("ToleranceForPoisson", 1e-7));
     c.depositMode = int(s.i("DepositMode", 0));
     c.sortInterval = int(s.i("SortInterval", 0));
+    c.masterSeed = uint64_t(s.i("MasterSeed", 0));
   }
   {  // ParamForField: src/Init.mm:109-146
     Section s{&require_object(root, "ParamForField")};

@@ -60,6 +60,7 @@ struct ParamForComputing {  // src/Init.h:27-36
   // to the reference's behaviour).
   int depositMode = 0;  // "DepositMode": 0 = FP32 atomics, 1 = deterministic fixed point
   int sortInterval = 0; // "SortInterval": cell-sort period in cycles (0 = automatic)
+  uint64_t masterSeed = 0;  // "MasterSeed": seed of the splitmix64 -> PCG32 streams (the reference fixes 0)
 };
 
 struct ParamForParticle {  // src/Init.h:38-52

@@ -201,15 +201,20 @@ __global__ void k_weights(const float* w, int cout, int cout_p, int kpad, __nv_b
 
 }  // namespace
 
-WarmStartNet::WarmStartNet(int h, int w, uint64_t seed, cudaStream_t s) : stream(s), h_(h), w_(w) {
+WarmStartNet::WarmStartNet(int h, int w, uint64_t seed, cudaStream_t s, int cin0, const int (&c)[4])
+    : stream(s), h_(h), w_(w), cin0_(cin0) {
   if (h % 8 || w % 8 || h < 8 || w < 8) throw std::invalid_argument("network grid must be a multiple of 8");
+  if (cin0 < 1 || c[0] < 1 || c[1] < 1 || c[2] < 1 || c[3] < 1) throw std::invalid_argument("network widths");
   struct Spec {
     int cin, cout;
     bool relu;
   };
-  const Spec specs[12] = {{2, 32, true},    {32, 32, true},   {32, 64, true},   {64, 64, true},
-                          {64, 128, true},  {128, 128, true}, {128, 256, true}, {256, 256, true},
-                          {384, 128, true}, {192, 64, true},  {96, 32, true},   {32, 1, false}};
+  // encoder: two convolutions per level (widths c0..c3); decoder: one per
+  // level on the upsampled coarser output concatenated with the skip
+  const Spec specs[12] = {{cin0, c[0], true},        {c[0], c[0], true},        {c[0], c[1], true},
+                          {c[1], c[1], true},        {c[1], c[2], true},        {c[2], c[2], true},
+                          {c[2], c[3], true},        {c[3], c[3], true},        {c[3] + c[2], c[2], true},
+                          {c[2] + c[1], c[1], true}, {c[1] + c[0], c[0], true}, {c[0], 1, false}};
   std::mt19937_64 rng(seed);
   size_t max_col = 0, max_gcol = 0, max_gy = 0;
   const int level_of[12] = {0, 0, 1, 1, 2, 2, 3, 3, 2, 1, 0, 0};
@@ -247,7 +252,8 @@ WarmStartNet::WarmStartNet(int h, int w, uint64_t seed, cudaStream_t s) : stream
     layers_.push_back(std::move(L));
   }
   // activations (see the forward pass for their roles)
-  const int chans[19] = {2, 32, 32, 32, 64, 64, 64, 128, 128, 128, 256, 256, 384, 128, 192, 64, 96, 32, 1};
+  const int chans[19] = {cin0, c[0], c[0], c[0], c[1], c[1], c[1], c[2], c[2], c[2], c[3], c[3], c[3] + c[2],
+                         c[2], c[2] + c[1], c[1], c[1] + c[0], c[0], 1};
   const int lev[19] = {0, 0, 0, 1, 1, 1, 2, 2, 2, 3, 3, 3, 2, 2, 1, 1, 0, 0, 0};
   for (int i = 0; i < 19; ++i) {
     Act a;
@@ -364,7 +370,7 @@ void WarmStartNet::conv_backward(ConvLayer& L, const Act& x, Act& y, Act* dx, co
 
 void WarmStartNet::forward(const float* in, float* out) {
   auto& A = acts_;
-  const size_t n0 = size_t(h_) * w_ * 2;
+  const size_t n0 = size_t(h_) * w_ * cin0_;
   k_f32_to_bf16<<<grid_for(n0), kT, 0, stream>>>(in, n0, A[0].y.get());
   GP_LAUNCH_CHECK();
   auto pool = [&](int a, int b) {
@@ -397,12 +403,42 @@ void WarmStartNet::forward(const float* in, float* out) {
 }
 
 float WarmStartNet::loss_and_grad(const float* in, const float* target) {
-  auto& A = acts_;
   forward(in, out_.get());
   const int n = h_ * w_;
   GP_CUDA(cudaMemsetAsync(loss_.get(), 0, 4, stream));
   k_mse<<<std::min(grid_for(size_t(n)), 1184), kT, 0, stream>>>(out_.get(), target, n, gout_.get(), loss_.get());
   GP_LAUNCH_CHECK();
+  backward(gout_.get());
+  float loss = 0;
+  int err = 0;
+  GP_CUDA(cudaMemcpyAsync(&loss, loss_.get(), 4, cudaMemcpyDeviceToHost, stream));
+  GP_CUDA(cudaMemcpyAsync(&err, err_.get(), 4, cudaMemcpyDeviceToHost, stream));
+  GP_CUDA(cudaStreamSynchronize(stream));
+  if (err) throw std::runtime_error("tensor-core GEMM: MMA completion wait timed out");
+  return loss;
+}
+
+float WarmStartNet::loss_and_grad_residual(const float* in, const kern::PoissonLayout& L) {
+  if (cin0_ != 1) throw std::invalid_argument("the residual loss needs a one-channel network");
+  forward(in, out_.get());
+  if (!res_.size()) {
+    res_.resize(size_t(h_) * w_, true);
+    lossd_.resize(1, true);
+  }
+  GP_CUDA(cudaMemsetAsync(lossd_.get(), 0, sizeof(double), stream));
+  residual_loss_grad(out_.get(), in, L, h_, w_, res_.get(), gout_.get(), lossd_.get(), stream);
+  backward(gout_.get());
+  double loss = 0;
+  int err = 0;
+  GP_CUDA(cudaMemcpyAsync(&loss, lossd_.get(), sizeof(double), cudaMemcpyDeviceToHost, stream));
+  GP_CUDA(cudaMemcpyAsync(&err, err_.get(), 4, cudaMemcpyDeviceToHost, stream));
+  GP_CUDA(cudaStreamSynchronize(stream));
+  if (err) throw std::runtime_error("tensor-core GEMM: MMA completion wait timed out");
+  return float(loss);
+}
+
+void WarmStartNet::backward(const float* gout) {
+  auto& A = acts_;
   for (auto& a : A) GP_CUDA(cudaMemsetAsync(a.g.get(), 0, a.g.bytes(), stream));
   auto pool_back = [&](int b, int a) {
     k_pool_back<<<grid_for(A[a].g.size()), kT, 0, stream>>>(A[b].g.get(), A[a].h, A[a].w, A[a].c, A[a].g.get());
@@ -413,7 +449,7 @@ float WarmStartNet::loss_and_grad(const float* in, const float* target) {
                                                                   A[x].g.get(), A[sk].g.get());
     GP_LAUNCH_CHECK();
   };
-  conv_backward(layers_[11], A[17], A[18], &A[17], gout_.get());
+  conv_backward(layers_[11], A[17], A[18], &A[17], gout);
   conv_backward(layers_[10], A[16], A[17], &A[16]);
   up_back(16, 15, 2);
   conv_backward(layers_[9], A[14], A[15], &A[14]);
@@ -431,17 +467,21 @@ float WarmStartNet::loss_and_grad(const float* in, const float* target) {
   pool_back(3, 2);
   conv_backward(layers_[1], A[1], A[2], &A[1]);
   conv_backward(layers_[0], A[0], A[1], nullptr);
-  float loss = 0;
-  int err = 0;
-  GP_CUDA(cudaMemcpyAsync(&loss, loss_.get(), 4, cudaMemcpyDeviceToHost, stream));
-  GP_CUDA(cudaMemcpyAsync(&err, err_.get(), 4, cudaMemcpyDeviceToHost, stream));
-  GP_CUDA(cudaStreamSynchronize(stream));
-  if (err) throw std::runtime_error("tensor-core GEMM: MMA completion wait timed out");
-  return loss;
 }
 
 float WarmStartNet::train_step(const float* in, const float* target, float lr) {
   const float loss = loss_and_grad(in, target);
+  adam(lr);
+  return loss;
+}
+
+float WarmStartNet::train_step_residual(const float* in, const kern::PoissonLayout& L, float lr) {
+  const float loss = loss_and_grad_residual(in, L);
+  adam(lr);
+  return loss;
+}
+
+void WarmStartNet::adam(float lr) {
   ++step_;
   const float b1 = 0.9f, b2 = 0.999f;
   const float c1 = 1.0f - std::pow(b1, float(step_)), c2 = 1.0f - std::pow(b2, float(step_));
@@ -454,7 +494,6 @@ float WarmStartNet::train_step(const float* in, const float* target, float lr) {
     GP_LAUNCH_CHECK();
   }
   sync_weights();
-  return loss;
 }
 
 }  // namespace nn

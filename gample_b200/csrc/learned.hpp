@@ -20,6 +20,7 @@
 #include <vector>
 
 #include "device.hpp"
+#include "kernels.hpp"
 
 namespace gample {
 namespace nn {
@@ -60,6 +61,19 @@ void apply_correction(const float* out, const double* prev, int mx, int my, int 
 void make_target(const double* x, const double* prev, const double* b, int mx, int my, int h, int w,
                  const float* inv, float* target, double* sums, cudaStream_t s);
 
+// Residual formulation of the warm start: in = (b - A phi) / s on the padded
+// grid with s its RMS over the unknowns (scale[0] = s, sum2: one device
+// double of scratch); x = prev + out * s / |Cd|; the loss of a correction
+// out is mean((in - (A / |Cd|) out)^2) over the unknowns, whose gradient
+// with respect to out is written to g (res: scratch of h * w floats, loss:
+// one device double, accumulated).
+void residual_input(const double* b, const double* phi, const kern::PoissonLayout& L, int h, int w, float* in,
+                    double* sum2, float* scale, cudaStream_t s);
+void apply_residual_correction(const float* out, const double* prev, const kern::PoissonLayout& L, int w,
+                               const float* scale, double* x, cudaStream_t s);
+void residual_loss_grad(const float* out, const float* in, const kern::PoissonLayout& L, int h, int w, float* res,
+                        float* g, double* loss, cudaStream_t s);
+
 struct ConvLayer {
   int cin, cout;           // channels
   int kpad;                // 9 * cin rounded up to a multiple of 32
@@ -74,13 +88,21 @@ struct ConvLayer {
 
 class WarmStartNet {
  public:
-  // h, w: grid (multiples of 8); the levels run at h, h/2, h/4, h/8.
-  WarmStartNet(int h, int w, uint64_t seed, cudaStream_t s);
-  // in: NHWC input [h][w][2] FP32 (normalised); out: [h][w] FP32
+  // h, w: grid (multiples of 8); the levels run at h, h/2, h/4, h/8 with
+  // widths c[0..3]; cin0 input channels.
+  WarmStartNet(int h, int w, uint64_t seed, cudaStream_t s, int cin0 = 2, const int (&c)[4] = kWideWidths);
+  static constexpr int kWideWidths[4] = {32, 64, 128, 256};
+  // in: NHWC input [h][w][cin0] FP32 (normalised); out: [h][w] FP32
   void forward(const float* in, float* out);
+  int input_channels() const { return cin0_; }
   // One Adam step on the mean-squared error against target [h][w]; returns
   // the loss of the forward pass (synchronous read of one float).
   float train_step(const float* in, const float* target, float lr);
+  // The same on the residual loss of a one-channel network (input: a
+  // normalised residual, residual_input): the mean square of the residual
+  // left by the correction the network predicts.
+  float train_step_residual(const float* in, const kern::PoissonLayout& L, float lr);
+  float loss_and_grad_residual(const float* in, const kern::PoissonLayout& L);
   // Parameter access for the gradient check (FP32 masters, layer by layer).
   int num_layers() const { return int(layers_.size()); }
   ConvLayer& layer(int i) { return layers_[i]; }
@@ -101,11 +123,14 @@ class WarmStartNet {
   void conv_forward(ConvLayer& L, const Act& x, Act& y, float* out_f32 = nullptr);
   void conv_backward(ConvLayer& L, const Act& x, Act& y, Act* dx, const float* gy_override = nullptr);
   void im2col(const Act& x, int kpad, int rows);  // into col_
-  int h_, w_;
+  void backward(const float* gout);  // gradients of every layer from the output gradient
+  void adam(float lr);               // one Adam step on the gradients, then the BF16 copies
+  int h_, w_, cin0_;
   std::vector<ConvLayer> layers_;
   std::vector<Act> acts_;
   DeviceArray<__nv_bfloat16> col_, colT_, gyT_, gyb_;
-  DeviceArray<float> gcol_, out_, gout_, loss_;
+  DeviceArray<float> gcol_, out_, gout_, loss_, res_;
+  DeviceArray<double> lossd_;
   DeviceArray<int> err_;
   int step_ = 0;
 };

@@ -79,7 +79,12 @@ class EMField {
   // Learned warm start of the Poisson solve (build addition). mode bits:
   // 1 start the multigrid from previous phi + the network's correction,
   // 2 train the network on (rhs, previous phi) -> (phi - previous phi) after
-  // each solve, 4 also solve from the plain warm start for comparison.
+  // each solve, 4 also solve from the plain warm start for comparison,
+  // 8 store each solve's normalised residual in the sample bank, 16 (when
+  // the network is created) the residual formulation: a one-channel network
+  // (widths 16/32/64/64) maps the residual r = b - A (previous phi), divided
+  // by its RMS, to a correction, trained on the mean square of the residual
+  // the correction leaves (2 then trains on each solve's sample).
   struct LearnedStats {
     double loss = 0;
     int iters_learned = 0, iters_plain = 0;
@@ -88,6 +93,12 @@ class EMField {
     int trained_steps = 0;
   };
   void setLearned(int mode, float lr, uint64_t seed);
+  // Sample bank of the residual formulation (capacity samples on the device)
+  // and offline training on it: steps Adam steps on samples drawn at random
+  // (seed); out[0], out[1]: mean loss of the first and of the last ten steps,
+  // out[2]: samples in the bank.
+  void setLearnedBank(int capacity);
+  void trainLearned(int steps, float lr, uint64_t seed, double out[3]);
   int learned_mode = 0;
   float learned_lr = 1e-3f;
   std::unique_ptr<nn::WarmStartNet> net;
@@ -143,6 +154,12 @@ class EMField {
  private:
   PinnedArray<double> host_diag_;
   MGResult poissonSolve(double* d);  // plain or learned warm start
+  MGResult residualSolve(double* d);  // learned warm start, residual formulation
+  bool learned_residual_ = false;
+  DeviceArray<float> bank_;           // normalised residual samples [cap][h][w]
+  int bank_cap_ = 0, bank_n_ = 0, bank_next_ = 0;
+  DeviceArray<double> nn_sum2_;
+  DeviceArray<float> nn_scale_;
   DeviceArray<float> nn_in_, nn_out_, nn_target_, nn_inv_;
   DeviceArray<double> sol_prev_, sol_cmp_, nn_sums_;
   float h_inv_[3] = {0, 0, 0};
@@ -233,6 +250,9 @@ class Collision {
   // particles of every species (overwriting them) from the splitmix64/PCG32
   // stream.
   Collision(const Init& init, std::vector<Particle*>& ptcls, cudaStream_t stream);
+  // Build addition: the initial load again from another master seed (the
+  // sources keep their set-up).
+  void reload(uint64_t seed, std::vector<Particle*>& ptcls);
   int artificialIonization(double dt, std::vector<Particle*>& ptcls, XmlLogger* logger);  // :464-566
   int hollowCathode(double dt, std::vector<Particle*>& ptcls, XmlLogger* logger);         // :568-678
   // Build addition: re-inject absorbed particles at Xmin (GenerateType
@@ -248,6 +268,7 @@ class Collision {
 
  private:
   void ensure_states(uint32_t n);
+  void loadInitial(std::vector<Particle*>& ptcls);
   const Init& init_;
   uint64_t minstd_ = 1;
   bool existAI_ = false, existHC_ = false;

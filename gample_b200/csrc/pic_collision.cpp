@@ -52,10 +52,12 @@ void Collision::ensure_states(uint32_t n) {
   initialized = n;
 }
 
-Collision::Collision(const Init& init, std::vector<Particle*>& ptcls, cudaStream_t st) : stream(st), init_(init) {
-  const ParamForField& fp = init.paramForField;
-  const auto& pp = init.paramForParticle;
-  if (pp.empty()) throw ConfigError("no particle species");
+// The initial load (src/Collision.mm:189-336): species 0's count of
+// electron + ion pairs from the splitmix64/PCG32 streams of master_seed,
+// overwriting both species.
+void Collision::loadInitial(std::vector<Particle*>& ptcls) {
+  const ParamForField& fp = init_.paramForField;
+  const auto& pp = init_.paramForParticle;
   Particle* ele = find(ptcls, "electron");
   Particle* ion = nullptr;
   for (auto* p : ptcls)
@@ -90,6 +92,21 @@ Collision::Collision(const Init& init, std::vector<Particle*>& ptcls, cudaStream
   GP_CUDA(cudaStreamSynchronize(stream));
   ele->n_bound = addn;
   ion->n_bound = addn;
+}
+
+void Collision::reload(uint64_t seed, std::vector<Particle*>& ptcls) {
+  master_seed = seed;
+  initialized = 0;  // every stream restarts from the new master seed
+  minstd_ = 1;
+  loadInitial(ptcls);
+}
+
+Collision::Collision(const Init& init, std::vector<Particle*>& ptcls, cudaStream_t st) : stream(st), init_(init) {
+  master_seed = init.paramForComputing.masterSeed;  // 0 in the reference (src/Collision.mm:283-294)
+  const ParamForField& fp = init.paramForField;
+  const auto& pp = init.paramForParticle;
+  if (pp.empty()) throw ConfigError("no particle species");
+  loadInitial(ptcls);
 
   // Sources: src/Collision.mm:365-458 (one artificial-ionization and one
   // hollow-cathode source; with several, the last one of each kind is used).

@@ -164,6 +164,19 @@ void Simulation::initialize() {
   GP_CUDA(cudaStreamSynchronize(stream));
 }
 
+void Simulation::reload(uint64_t seed) {
+  collision->reload(seed, ptrs);
+  for (auto* p : ptrs) {
+    p->needs_sort = true;
+    p->random_order = true;
+    p->cycles_since_sort = 0;
+  }
+  cycle_no = init.paramForTimeIntegration.Start;
+  comp = 0;
+  time = cycle_no * init.paramForTimeIntegration.TimeStep;
+  GP_CUDA(cudaStreamSynchronize(stream));
+}
+
 void Simulation::cycle() {
   const auto& T = init.paramForTimeIntegration;
   const double dt = T.TimeStep;

@@ -30,6 +30,10 @@ class Simulation {
   Simulation(const Init& init, const std::string& log_name, bool fused);
   ~Simulation();
   void initialize();  // src/main.mm:114-147 (initial deposit and solve)
+  // Build addition: the initial load again from another master seed and the
+  // cycle counter back at Start (initialize() follows); fields, solver state
+  // and the warm-start network are kept.
+  void reload(uint64_t seed);
   void cycle();       // one cycle of src/main.mm:155-253
   void run(int ncycles);
   // Binary outputs under bin/ (src/FileIO.mm) are written only when a log

@@ -98,6 +98,11 @@ gp_status gp_sim_create(const gp_init* init, const char* log_name, int flags, gp
 void gp_sim_free(gp_sim* sim);
 /* Initial deposit and field solve: src/main.mm:136-141. */
 gp_status gp_sim_initialize(gp_sim* sim);
+/* The initial load again from master seed `seed` (ParamForComputing
+ * MasterSeed; the reference fixes 0) with the cycle counter back at Start;
+ * gp_sim_initialize follows. Fields, solver state and any warm-start network
+ * are kept. Build addition, no reference counterpart. */
+gp_status gp_sim_reload(gp_sim* sim, uint64_t seed);
 /* ncycles cycles of the time loop: src/main.mm:155-253. */
 gp_status gp_sim_run(gp_sim* sim, int ncycles);
 gp_status gp_sim_cycle_number(const gp_sim* sim, int* cycle, double* time);
@@ -209,8 +214,20 @@ gp_status gp_deposit_charge_noalloc(int weighting_order, int ngx, int ngy, const
 /* Attach the network to a run's Poisson solve. mode bits: 1 start the
  * multigrid from previous phi + network correction, 2 train after each solve
  * on (rhs, previous phi) -> (phi - previous phi), 4 also time a solve from the
- * plain warm start; the multigrid always reaches ToleranceForPoisson. */
+ * plain warm start, 8 keep each solve's sample in the sample bank, 16 (when
+ * the network is first attached) the residual formulation: a one-channel
+ * network (widths 16/32/64/64) maps the residual b - A (previous phi),
+ * divided by its RMS, to a correction of previous phi and learns from the
+ * mean square of the residual that correction leaves (Dirichlet and periodic
+ * field boundaries); the multigrid always reaches ToleranceForPoisson. */
 gp_status gp_field_learned(gp_sim* sim, int mode, float lr, uint64_t seed);
+/* Sample bank of the residual formulation: room for `capacity` samples on
+ * the device, filled by the solves while mode bit 8 is set. */
+gp_status gp_field_learned_bank(gp_sim* sim, int capacity);
+/* Offline training on the bank: `steps` Adam steps (learning rate lr) on
+ * samples drawn at random (seed); out[0], out[1]: mean loss of the first and
+ * of the last ten steps, out[2]: samples in the bank. */
+gp_status gp_field_learned_train(gp_sim* sim, int steps, float lr, uint64_t seed, double out[3]);
 /* last solve: loss, V-cycles (learned, plain), ms (learned incl. network,
  * plain, network alone), starting relative residual (learned, plain),
  * training steps so far */

@@ -140,7 +140,9 @@ def parse(path_or_dict):
                    "integrationChunkSize": _int(m["IntegrationChunkSize"]),
                    "aggrThreshold": _f32(_dbl(m["AggregationThreshold"])), "chebDegree": _int(m["ChebyshevDegree"]),
                    "amgCycleType": _int(m["AMGCycleType"]), "maxiter": _int(m["MaxiterForPoisson"]),
-                   "tolerance": _f32(_dbl(m["ToleranceForPoisson"]))}
+                   "tolerance": _f32(_dbl(m["ToleranceForPoisson"])),
+                   # build addition: master seed of the RNG streams (the reference fixes 0)
+                   "masterSeed": int(c.get("MasterSeed", 0))}
 
     fd = root.get("ParamForField")
     if not isinstance(fd, dict):
@@ -276,6 +278,7 @@ def to_struct(cfg, lib_module):
     C.pnum_max = cfg["comp"]["pNumMax"]
     C.maxiter = cfg["comp"]["maxiter"]
     C.tol = cfg["comp"]["tolerance"]
+    C.master_seed = cfg["comp"].get("masterSeed", 0)
     C.ngx, C.ngy, C.ngb, C.dx, C.dy = f["ngx"], f["ngy"], f["ngb"], f["dx"], f["dy"]
     C.ampE[:] = _pad(f["ampE"], 3, 0.0)
     C.ampB[:] = _pad(f["ampB"], 3, 0.0)

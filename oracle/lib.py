@@ -40,7 +40,7 @@ class OrConfig(C.Structure):
                 ("initE_uniform", C.c_int), ("initB_uniform", C.c_int), ("weight_order", C.c_int),
                 ("boris_order", C.c_int), ("cur_dens", C.c_int), ("fbc", C.c_int * 4), ("fbc_val", C.c_double * 4),
                 ("cathode_pos", C.c_double), ("pbc", C.c_int * 4), ("sp", OrSpecies * OR_MAX_SPECIES),
-                ("n_sources", C.c_int), ("src", OrSource * OR_MAX_SOURCES)]
+                ("n_sources", C.c_int), ("src", OrSource * OR_MAX_SOURCES), ("master_seed", C.c_uint64)]
 
 
 class OrSolveStats(C.Structure):

@@ -52,6 +52,7 @@ typedef struct {
   or_species sp[OR_MAX_SPECIES];
   int n_sources;
   or_source src[OR_MAX_SOURCES];
+  uint64_t master_seed; /* build addition: seed of the RNG streams (the reference fixes 0) */
 } or_config;
 
 typedef struct {

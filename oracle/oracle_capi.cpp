@@ -47,6 +47,7 @@ struct Sim : SimBase {
   int ele = -1, ion = -1;
 
   explicit Sim(const or_config& c) : cfg(c) {
+    master = c.master_seed;
     g.ngx = c.ngx;
     g.ngy = c.ngy;
     g.ngb = c.ngb;

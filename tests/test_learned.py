@@ -97,31 +97,52 @@ def test_training_reduces_the_loss(gpu):
 
 
 @pytest.mark.gpu
-def test_learned_warm_start_trains_online_and_keeps_the_tolerance(gpu):
-    """The network trained on the run's own (rhs, previous phi) pairs: the
-    solve from its warm start reaches the same tolerance, and the gain over
-    the plain warm start (V-cycles, starting residual) is measured."""
+def test_learned_warm_start_gain_over_the_plain_warm_start(gpu):
+    """The residual formulation trained offline on samples the simulator
+    generates from four master seeds (3rd order, Dirichlet x / periodic y,
+    128 x 128, 64 particles per cell): on a held-out seed, the multigrid runs
+    to the same 1e-8 from the plain warm start (previous phi) and from
+    previous phi plus the network's correction. The network lowers the
+    starting residual by more than 5x; it does not lower the V-cycle count
+    (the residual it leaves is the smooth part, which the V-cycles reduce at
+    the same rate), and its forward pass costs more time than it saves. The
+    test asserts the residual gain and the unchanged answer, and reports the
+    V-cycle and time ratios."""
     from gample_b200 import capi
     from tests.helpers import condition
-    cond = condition(ngx=64, ngy=64, order=3, ppc=32, xbc="Dirichlet", ybc="periodic", bz_tesla=0.02, end=100)
+    cond = condition(ngx=128, ngy=128, order=3, ppc=64, xbc="Dirichlet", ybc="periodic", bz_tesla=0.02, end=1000,
+                     dx=5.2567e-3, dt=3.96e-12)
     sim = capi.Sim(cond)
+    sim.set_learned(16, 1e-3, 0)
+    seeds, samples = 4, 25
+    sim.learned_bank(seeds * samples)
+    for seed in range(seeds):
+        sim.reload(seed)
+        sim.initialize()
+        sim.set_learned(16, 1e-3)
+        sim.run(5)
+        sim.set_learned(16 | 8, 1e-3)
+        sim.run(samples)
+    tr = sim.learned_train(600, 1e-3, 1)
+    assert tr["samples"] == seeds * samples
+    assert tr["loss_last"] < 0.1 * tr["loss_first"], tr
+    sim.reload(seeds)
     sim.initialize()
-    sim.run(2)
-    sim.set_learned(4, 1e-3, 7)
-    sim.run(1)
-    sim.set_learned(2 | 4, 1e-3)
-    losses = []
-    for _ in range(40):
-        sim.run(1)
-        losses.append(sim.learned_stats()["loss"])
-    assert np.mean(losses[-10:]) < np.mean(losses[:10])
-    sim.set_learned(1 | 4, 1e-3)
+    sim.set_learned(16, 1e-3)
+    sim.run(5)
+    sim.set_learned(16 | 1 | 4, 1e-3)
     st = []
-    for _ in range(5):
+    for _ in range(10):
         sim.run(1)
-        s = sim.learned_stats()
-        st.append(s)
+        st.append(sim.learned_stats())
         assert sim.last_solve().error <= 1e-8
-    gain = np.mean([s["iters_plain"] for s in st]) / np.mean([s["iters_learned"] for s in st])
-    assert 0.5 < gain < 4.0  # measured, either way; the solve never depends on it
+    m = lambda k: float(np.mean([s[k] for s in st]))
+    residual_gain = m("rel0_plain") / m("rel0_learned")
+    vcycle_gain = m("iters_plain") / m("iters_learned")
+    print(f"learned warm start: starting residual {m('rel0_plain'):.3e} -> {m('rel0_learned'):.3e} "
+          f"({residual_gain:.1f}x), V-cycles {m('iters_plain'):.1f} -> {m('iters_learned'):.1f} "
+          f"({vcycle_gain:.2f}x), solve {m('ms_plain'):.3f} -> {m('ms_learned'):.3f} ms incl. network "
+          f"{m('ms_net'):.3f} ms")
+    assert residual_gain > 5.0, residual_gain
+    assert m("iters_learned") <= m("iters_plain")
     sim.close()
