@@ -52,6 +52,27 @@ def test_loader_matches_oracle(gpu, order, ppc):
         assert np.all(g["piflag"] == 0)
 
 
+@pytest.mark.parametrize("seed", [7, 19])
+def test_loader_with_master_seed_matches_oracle(gpu, seed):
+    """ParamForComputing MasterSeed (build addition; the reference fixes 0)
+    selects the splitmix64 -> PCG32 streams on both sides, and gp_sim_reload
+    reloads a run from another seed."""
+    cond = condition(ngx=40, ngy=24, order=3, ppc=9, xbc="Dirichlet", ybc="periodic")
+    cond["ParamForComputing"]["MasterSeed"] = seed
+    sim, ora = pair(cond)
+    ora.load_initial()
+    base = condition(ngx=40, ngy=24, order=3, ppc=9, xbc="Dirichlet", ybc="periodic")
+    sim0 = capi.Sim(base)
+    sim0.reload(seed)
+    for s in range(2):
+        g, g0, o = sim.particles(s), sim0.particles(s), ora.particles(s, f32=True)
+        np.testing.assert_array_equal(g["x"], o["x"])
+        np.testing.assert_array_equal(g["y"], o["y"])
+        np.testing.assert_array_equal(g0["x"], g["x"])
+        np.testing.assert_array_equal(g0["vz"], g["vz"])
+    sim0.close()
+
+
 # ---------------------------------------------------------------- push
 def random_fields(ora, rng, emag, bz=None):
     for name in ("Ex", "Ey"):
