@@ -20,6 +20,7 @@
 #include <climits>
 #include <cstdio>
 #include <mutex>
+#include <type_traits>
 
 #include "device.hpp"
 #include "kernels.hpp"
@@ -186,6 +187,8 @@ struct DepositLayout {
   // each, so at most kPer * (kThreads / 32) contributions per node and word
   static_assert(!kSingle || double(kPer) * (kThreads / 32) * kMaxW * double(1 << kQBits) < 2147483647.0,
                 "a lane-private window word could overflow");
+  // the flush's sum of the 32 lane-private copies fits 32 unsigned bits
+  static constexpr bool kPrivSum32 = 32.0 * kPer * (kThreads / 32) * kMaxW * double(1 << kQBits) < 4294967295.0;
 };
 
 // This lane's copy of the window arrays: shared-memory byte address of its rho
@@ -686,11 +689,13 @@ __device__ __forceinline__ void chunk_flush(const GridDims& g, const PushConsts&
       const int cc = e % kPW;
       if (cc >= w.dw) continue;
       const int col = w.dx0 + cc, row = w.dy0 + e / kPW;
-      // each copy word stays below 2^31 (DepositLayout); the 32 together may
-      // not, so they are summed in 64 bits
-      long long r = 0;
+      // each copy word stays below 2^31 (DepositLayout); the 32 together
+      // fit 32 unsigned bits for orders 3 and 5, not for order 1 (weights up
+      // to 1), which sums in 64 bits
+      using Sum = std::conditional_t<DL::kPrivSum32, uint32_t, unsigned long long>;
+      Sum r = 0;
 #pragma unroll 8
-      for (int q = 0; q < 32; ++q) r += sDep[q * w.ps + e];
+      for (int q = 0; q < 32; ++q) r += Sum(uint32_t(sDep[q * w.ps + e]));
       if (r != 0 && in_box(col, row, nx + 1, ny + 1)) atomicAdd(d.f64_rho + col + row * (nx + 1), double(r) * fr);
     }
   } else if (w.use) {
@@ -1096,19 +1101,139 @@ __global__ void __launch_bounds__(kThreads, ORDER == 5 ? 2 : 4)
     float ox = q_ox, oy = q_oy, vx = q_vx, vy = q_vy, vz = q_vz;
     if (i + 1 < kPer) fetch(k + uint32_t(kThreads));
     int fl = 0;
-    if (k < n) {
+    // The gather of a particle in the chunk's box: per-cell polynomial
+    // tables (order 3) or the staged windows.
+    auto gather_box = [&](int ix, int iy, float ox, float oy, float& Epx, float& Epy) {
+      if (tab) {
+        const int ux = ox >= 0.5f ? 1 : 0, uy = oy >= 0.5f ? 1 : 0;
+        const float hx = ux ? __fsub_rn(ox, 0.5f) : __fadd_rn(ox, 0.5f);
+        const float hy = uy ? __fsub_rn(oy, 0.5f) : __fadd_rn(oy, 0.5f);
+        Epx = tab_eval(tbx + iy * xrs + kTabEntry * (ix + ux), hx, oy);
+        Epy = tab_eval(tby + (iy + uy) * yrs + kTabEntry * ix, ox, hy);
+      } else {
+        const Stagger sx = stagger(ix, ox), sy = stagger(iy, oy);
+        float wxn[N], wxh[N], wyn[N], wyh[N];
+        shape<ORDER>(sx.hnode, wxn);
+        shape<ORDER>(sx.hhalf, wxh);
+        shape<ORDER>(sy.hnode, wyn);
+        shape<ORDER>(sy.hhalf, wyh);
+        float Bpz = 0.0f;
+        gather<ORDER, true, true, false>(g, f, w, sx, sy, wxn, wxh, wyn, wyh, sEx, sEy, nullptr, Epx, Epy, Bpz);
+      }
+    };
+    // Boris push (src/Particle.mm:157-209) with the launch's Bz factors
+    auto boris = [&](float Epx, float Epy, float& vx, float& vy, float& vz) {
+      const float etx = __fmul_rn(bz.fe, Epx), ety = __fmul_rn(bz.fe, Epy);
+      const float umx = vx + etx, umy = vy + ety, umz = vz;
+      const float v0x = umx + umy * bz.btz;
+      const float v0y = umy - umx * bz.btz;
+      const float upx = umx + v0y * bz.ssz;
+      const float upy = umy - v0x * bz.ssz;
+      vx = upx + c.constE * Epx;
+      vy = upy + c.constE * Epy;
+      vz = umz;
+    };
+    // Store, kinetic energy and deposit of a particle that is live, interior
+    // and inside the deposit window after the move.
+    auto store_deposit_win = [&](int ix, int iy, float ox, float oy, float vx, float vy, float vz) {
+      p.vx[k] = vx;
+      p.vy[k] = vy;
+      p.vz[k] = vz;
+      p.cell[k] = pack_cell(ix, iy);
+      p.ox[k] = ox;
+      p.oy[k] = oy;
+      ke += __fadd_rn(__fadd_rn(__fmul_rn(vx, vx), __fmul_rn(vy, vy)), __fmul_rn(vz, vz));
+      if (priv) {
+        float rx[N], ry[N];  // x weights pre-scaled by the window's fixed-point unit
+        shape2<ORDER>(make_float2(ox, oy), float(1 << DL::kQBits), rx, ry);
+        priv_add<N>(pbase + 4u * uint32_t(ix + iy * kPW), rx, ry);
+      } else {
+        float wxn[N], wyn[N], unused[N];
+        shape2<ORDER>(make_float2(ox, oy), 1.0f, wxn, wyn);
+        deposit_one<ORDER, false, false, true, false>(g, w, lane, stagger(ix, ox), stagger(iy, oy), wxn, unused, wyn,
+                                                      unused, c.scale, vx, vy, d, sw);
+      }
+    };
+    // Boundary conditions, store and deposit of any moved particle
+    // (src/Particle.mm:212-269); returns the flag.
+    auto finish = [&](int ix, int iy, float ox, float oy, float vx, float vy, float vz, bool okx, bool oky) {
+      int f = 0;
+      if (!(okx && oky) || !isfinite(vz)) {
+        f = 5;
+      } else if (!interior(g, ix, iy)) {
+        if (c.bc[0] == 0) ix = wrap_periodic(ix, ngb, g.ngx);
+        if (c.bc[2] == 0) iy = wrap_periodic(iy, ngb, g.ngy);
+        if (c.bc[0] == 1 && ix < ngb) f = 1;
+        if (c.bc[1] == 1 && ix >= ngb + g.ngx) f = 2;
+        if (c.bc[2] == 1 && iy < ngb) f = 3;
+        if (c.bc[3] == 1 && iy >= ngb + g.ngy) f = 4;
+        if (c.bc[0] == 2 && ix < ngb) {
+          reflect(ix, ox, ngb);
+          vx = -vx;
+        }
+        if (c.bc[1] == 2 && ix >= ngb + g.ngx) {
+          reflect(ix, ox, ngb + g.ngx);
+          vx = -vx;
+        }
+        if (c.bc[2] == 2 && iy < ngb) {
+          reflect(iy, oy, ngb);
+          vy = -vy;
+        }
+        if (c.bc[3] == 2 && iy >= ngb + g.ngy) {
+          reflect(iy, oy, ngb + g.ngy);
+          vy = -vy;
+        }
+        if (f == 0 && !interior(g, ix, iy)) f = 5;
+      }
+      if (f != 0) {
+        p.vx[k] = vx;
+        p.vy[k] = vy;
+        p.vz[k] = vz;
+        p.cell[k] = -f;
+        return f;
+      }
+      const bool in_win = use && uint32_t(ix - wx0) <= ww && uint32_t(iy - wy0) <= wh;
+      if (in_win) {
+        store_deposit_win(ix, iy, ox, oy, vx, vy, vz);
+      } else {
+        p.vx[k] = vx;
+        p.vy[k] = vy;
+        p.vz[k] = vz;
+        p.cell[k] = pack_cell(ix, iy);
+        p.ox[k] = ox;
+        p.oy[k] = oy;
+        ke += __fadd_rn(__fadd_rn(__fmul_rn(vx, vx), __fmul_rn(vy, vy)), __fmul_rn(vz, vz));
+        float wxn[N], wyn[N], unused[N];
+        shape2<ORDER>(make_float2(ox, oy), 1.0f, wxn, wyn);
+        deposit_one<ORDER, false, false, false, false>(g, w, lane, stagger(ix, ox), stagger(iy, oy), wxn, unused, wyn,
+                                                       unused, c.scale, vx, vy, d, sw);
+      }
+      return 0;
+    };
+    int ix = cell_ix(cell), iy = cell_iy(cell);
+    const bool inb = use && uint32_t(ix - mnx) <= bw && uint32_t(iy - mny) <= bh;
+    // Warps whose 32 particles are all live and inside the staged box take a
+    // branch-free path (the usual case for cell-sorted particles); the
+    // decisions are warp-uniform, so no lane waits on another's branch.
+    if (__all_sync(0xffffffffu, k < n && cell >= 0 && inb)) {
+      float Epx, Epy;
+      gather_box(ix, iy, ox, oy, Epx, Epy);
+      boris(Epx, Epy, vx, vy, vz);
+      const bool okx = advance(ix, ox, vx, c.constX);
+      const bool oky = advance(iy, oy, vy, c.constY);
+      const bool plain = okx && oky && isfinite(vz) && interior(g, ix, iy) && uint32_t(ix - wx0) <= ww &&
+                         uint32_t(iy - wy0) <= wh;
+      if (__all_sync(0xffffffffu, plain))
+        store_deposit_win(ix, iy, ox, oy, vx, vy, vz);
+      else
+        fl = finish(ix, iy, ox, oy, vx, vy, vz, okx, oky);
+    } else if (k < n) {
       if (cell < 0) {
         fl = -cell;  // flagged before this push and not yet compacted: keep the flag
       } else {
-        int ix = cell_ix(cell), iy = cell_iy(cell);
-        const bool inb = use && uint32_t(ix - mnx) <= bw && uint32_t(iy - mny) <= bh;
         float Epx = 0.0f, Epy = 0.0f;
-        if (tab && inb) {
-          const int ux = ox >= 0.5f ? 1 : 0, uy = oy >= 0.5f ? 1 : 0;
-          const float hx = ux ? __fsub_rn(ox, 0.5f) : __fadd_rn(ox, 0.5f);
-          const float hy = uy ? __fsub_rn(oy, 0.5f) : __fadd_rn(oy, 0.5f);
-          Epx = tab_eval(tbx + iy * xrs + kTabEntry * (ix + ux), hx, oy);
-          Epy = tab_eval(tby + (iy + uy) * yrs + kTabEntry * ix, ox, hy);
+        if (inb) {
+          gather_box(ix, iy, ox, oy, Epx, Epy);
         } else {
           const Stagger sx = stagger(ix, ox), sy = stagger(iy, oy);
           float wxn[N], wxh[N], wyn[N], wyh[N];
@@ -1117,87 +1242,19 @@ __global__ void __launch_bounds__(kThreads, ORDER == 5 ? 2 : 4)
           shape<ORDER>(sy.hnode, wyn);
           shape<ORDER>(sy.hhalf, wyh);
           float Bpz = 0.0f;
-          if (inb)
-            gather<ORDER, true, true, false>(g, f, w, sx, sy, wxn, wxh, wyn, wyh, sEx, sEy, nullptr, Epx, Epy, Bpz);
-          else if (interior(g, ix, iy))
+          if (interior(g, ix, iy))
             gather<ORDER, true, false, false>(g, f, w, sx, sy, wxn, wxh, wyn, wyh, sEx, sEy, nullptr, Epx, Epy, Bpz);
           else
             gather<ORDER, true, false, true>(g, f, w, sx, sy, wxn, wxh, wyn, wyh, sEx, sEy, nullptr, Epx, Epy, Bpz);
-          if (!inb) tally += 1u << 24;
+          tally += 1u << 24;
         }
-        // Boris push (src/Particle.mm:157-209) with the launch's Bz factors
-        const float etx = __fmul_rn(bz.fe, Epx), ety = __fmul_rn(bz.fe, Epy);
-        const float umx = vx + etx, umy = vy + ety, umz = vz;
-        const float v0x = umx + umy * bz.btz;
-        const float v0y = umy - umx * bz.btz;
-        const float upx = umx + v0y * bz.ssz;
-        const float upy = umy - v0x * bz.ssz;
-        vx = upx + c.constE * Epx;
-        vy = upy + c.constE * Epy;
-        vz = umz;
-        // position update and boundary conditions (src/Particle.mm:212-269)
+        boris(Epx, Epy, vx, vy, vz);
         const bool okx = advance(ix, ox, vx, c.constX);
         const bool oky = advance(iy, oy, vy, c.constY);
-        if (!(okx && oky) || !isfinite(vz)) {
-          fl = 5;
-        } else if (!interior(g, ix, iy)) {
-          if (c.bc[0] == 0) ix = wrap_periodic(ix, ngb, g.ngx);
-          if (c.bc[2] == 0) iy = wrap_periodic(iy, ngb, g.ngy);
-          if (c.bc[0] == 1 && ix < ngb) fl = 1;
-          if (c.bc[1] == 1 && ix >= ngb + g.ngx) fl = 2;
-          if (c.bc[2] == 1 && iy < ngb) fl = 3;
-          if (c.bc[3] == 1 && iy >= ngb + g.ngy) fl = 4;
-          if (c.bc[0] == 2 && ix < ngb) {
-            reflect(ix, ox, ngb);
-            vx = -vx;
-          }
-          if (c.bc[1] == 2 && ix >= ngb + g.ngx) {
-            reflect(ix, ox, ngb + g.ngx);
-            vx = -vx;
-          }
-          if (c.bc[2] == 2 && iy < ngb) {
-            reflect(iy, oy, ngb);
-            vy = -vy;
-          }
-          if (c.bc[3] == 2 && iy >= ngb + g.ngy) {
-            reflect(iy, oy, ngb + g.ngy);
-            vy = -vy;
-          }
-          if (fl == 0 && !interior(g, ix, iy)) fl = 5;
-        }
-        p.vx[k] = vx;
-        p.vy[k] = vy;
-        p.vz[k] = vz;
-        if (fl == 0) {
-          p.cell[k] = pack_cell(ix, iy);
-          p.ox[k] = ox;
-          p.oy[k] = oy;
-          const float vv = __fadd_rn(__fadd_rn(__fmul_rn(vx, vx), __fmul_rn(vy, vy)), __fmul_rn(vz, vz));
-          ke += vv;
-          // deposit of the new position (node-centred weights, base = cell)
-          const bool in_win = use && uint32_t(ix - wx0) <= ww && uint32_t(iy - wy0) <= wh;
-          if (priv && in_win) {
-            float rx[N], ry[N];  // x weights pre-scaled by the window's fixed-point unit
-            shape2<ORDER>(make_float2(ox, oy), float(1 << DL::kQBits), rx, ry);
-            priv_add<N>(pbase + 4u * uint32_t(ix + iy * kPW), rx, ry);
-          } else {
-            float wxn[N], wyn[N];
-            shape2<ORDER>(make_float2(ox, oy), 1.0f, wxn, wyn);
-            const Stagger nsx = stagger(ix, ox), nsy = stagger(iy, oy);
-            float unused[N];
-            if (in_win)
-              deposit_one<ORDER, false, false, true, false>(g, w, lane, nsx, nsy, wxn, unused, wyn, unused, c.scale,
-                                                            vx, vy, d, sw);
-            else
-              deposit_one<ORDER, false, false, false, false>(g, w, lane, nsx, nsy, wxn, unused, wyn, unused, c.scale,
-                                                             vx, vy, d, sw);
-          }
-        } else {
-          p.cell[k] = -fl;
-        }
+        fl = finish(ix, iy, ox, oy, vx, vy, vz, okx, oky);
       }
-      if (fl) tally += 1u + (fl <= 4 ? 1u << (4 * fl) : 1u << 20);
     }
+    if (fl) tally += 1u + (fl <= 4 ? 1u << (4 * fl) : 1u << 20);
     const uint32_t wbase = base + uint32_t(i * kThreads + wid * 32);
     const uint32_t bits = __ballot_sync(0xffffffffu, fl != 0);
     if (lane == 0 && wbase < n) dead_bits[wbase >> 5] = bits;
