@@ -1102,7 +1102,8 @@ __global__ void __launch_bounds__(kThreads, ORDER == 5 ? 2 : 4)
     if (i + 1 < kPer) fetch(k + uint32_t(kThreads));
     int fl = 0;
     // The gather of a particle in the chunk's box: per-cell polynomial
-    // tables (order 3) or the staged windows.
+    // tables (order 3) or the staged windows (which add into Epx, Epy: the
+    // caller starts them at zero).
     auto gather_box = [&](int ix, int iy, float ox, float oy, float& Epx, float& Epy) {
       if (tab) {
         const int ux = ox >= 0.5f ? 1 : 0, uy = oy >= 0.5f ? 1 : 0;
@@ -1216,7 +1217,7 @@ __global__ void __launch_bounds__(kThreads, ORDER == 5 ? 2 : 4)
     // branch-free path (the usual case for cell-sorted particles); the
     // decisions are warp-uniform, so no lane waits on another's branch.
     if (__all_sync(0xffffffffu, k < n && cell >= 0 && inb)) {
-      float Epx, Epy;
+      float Epx = 0.0f, Epy = 0.0f;  // the window gather accumulates into them
       gather_box(ix, iy, ox, oy, Epx, Epy);
       boris(Epx, Epy, vx, vy, vz);
       const bool okx = advance(ix, ox, vx, c.constX);
