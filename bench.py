@@ -189,7 +189,7 @@ def poisson_block(vcycles, unknowns, solve_ms, peak):
     return {"vcycles_last_step": vcycles, "tolerance": 1e-8, "solve_ms_per_step": solve_ms,
             "ms_per_vcycle_incl_cg": ms_cycle, "algorithmic_bytes_per_vcycle": per_cycle,
             "achieved_gbs": achieved, "frac_of_hbm": achieved / peak if achieved else None,
-            "note": "latency-bound: ~13 dependent launches per CG iteration (one CUDA graph), "
+            "note": "latency-bound: 9 dependent launches per CG iteration at 512^2 (one CUDA graph), "
                     "levels <= 4096 points in one CTA"}
 
 
