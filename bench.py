@@ -420,6 +420,10 @@ def run_b200(args):
         sim.run(args.warmup)
     n0 = sim.count(0) + sim.count(1)
     clocks = ClockSampler(local)
+    # per-phase CUDA events on the library's stream inside the timed region
+    # (the push kernel's launch time for the roofline); not in profiler runs
+    if not args.quick:
+        sim.set_profiling(True)
     barrier()
     clocks.start()
     l0 = capi.kernel_launches()
@@ -427,6 +431,8 @@ def run_b200(args):
     launches = capi.kernel_launches() - l0
     barrier()
     clk = clocks.stop()
+    ph = sim.phase_times() if not args.quick else None
+    sim.set_profiling(False)
     n1 = sim.count(0) + sim.count(1)
     if args.quick:  # profiling runs: the timed cycles only
         if rank == 0:
@@ -440,16 +446,11 @@ def run_b200(args):
     pushes_rank = 0.5 * (n0 + n1) * args.steps
     ms_max, _, value = aggregate_ranks(ms, pushes_rank, pg)
 
-    # Roofline of the dominant kernel (push + fused deposit): a few more
-    # cycles with per-phase CUDA events on the library's stream.
-    sim.set_profiling(True)
-    prof_cycles = max(2, min(5, args.steps))
-    sim.run(prof_cycles)
-    ph = sim.phase_times()
-    sim.set_profiling(False)
-    n_prof = sim.count(0) + sim.count(1)
+    # Roofline of the dominant kernel (push + fused deposit), from the phase
+    # events of the timed cycles: two launches (species) per cycle.
+    prof_cycles = args.steps
     push_ms_per_launch = ph["push"] / (2 * prof_cycles)
-    particles_per_launch = n_prof / 2
+    particles_per_launch = 0.25 * (n0 + n1)
     peak, peak_kind = load_peaks()
     achieved = BYTES_PER_PUSH * particles_per_launch / (push_ms_per_launch / 1e3) / 1e9
     tr = load_traffic()
@@ -530,6 +531,8 @@ def run_b200(args):
                 "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
                 "gpu_launches": launches, "gpu_launches_per_step": launches / args.steps,
+                "timing": "CUDA events around the K cycles on the library's stream, per-phase events inside "
+                          "(roofline and poisson blocks); max over ranks",
                 "poisson": poisson_block(iters_last, unknowns, roofline["phase_ms_per_step"]["solve"], peak),
                 "steady_state": steady,
                 "learned_warm_start": learned,

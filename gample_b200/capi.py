@@ -79,6 +79,7 @@ EXPORTS = {
     "gp_particle_reduce": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(GpFlowStats)]),
     "gp_particle_integrate_charge": (C.c_int, [C.c_void_p, C.c_int]),
     "gp_particle_count": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_uint32)]),
+    "gp_particle_push_stats": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_uint32)]),
     "gp_particle_download": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_uint32, C.POINTER(C.c_uint32)]),
     "gp_particle_upload": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_uint32]),
     "gp_particle_download_raw": (C.c_int, [C.c_void_p, C.c_int] + [C.c_void_p] * 6 +
@@ -309,6 +310,13 @@ class Sim:
         n = C.c_uint32()
         check(lib().gp_particle_count(self.h, s, C.byref(n)))
         return n.value
+
+    def push_stats(self, s):
+        """(particles pushed without a window, chunks staged by bulk tensor
+        copies, staging waits that timed out) of the last push."""
+        out = (C.c_uint32 * 3)()
+        check(lib().gp_particle_push_stats(self.h, s, out))
+        return tuple(out)
 
     def particles(self, s):
         n = self.count(s)

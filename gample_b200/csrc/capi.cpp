@@ -605,6 +605,7 @@ gp_status gp_field_upload(gp_sim* sim, int which, const void* host, size_t bytes
     GP_CUDA(cudaMemcpyAsync(fb.dev, host, bytes, cudaMemcpyHostToDevice, s.stream));
     GP_CUDA(cudaStreamSynchronize(s.stream));
     if (which == GP_FIELD_BZ) s.field->bz_uniform = false;  // arbitrary Bz: gather it
+    s.field->e_pitched_stale = true;
     return GP_OK;
   });
 }
@@ -641,6 +642,16 @@ gp_status gp_particle_count(gp_sim* sim, int s, uint32_t* n) {
   return guarded([&] {
     if (!n) throw std::invalid_argument("null output");
     *n = species(sim, s)->pNum();
+    return GP_OK;
+  });
+}
+gp_status gp_particle_push_stats(gp_sim* sim, int s, uint32_t out[3]) {
+  return guarded([&] {
+    if (!out) throw std::invalid_argument("null output");
+    const auto c = species(sim, s)->counters();
+    out[0] = c.n_slow;
+    out[1] = c.n_tma;
+    out[2] = c.err;
     return GP_OK;
   });
 }

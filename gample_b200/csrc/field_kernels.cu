@@ -233,7 +233,7 @@ __global__ void k_phi_fill(const double* sol, GridDims g, PoissonLayout L, float
 }
 
 __global__ void k_gradient(const double* phi, GridDims g, float dx, float dy, float* Ex, float* Ey, const float* jx,
-                           const float* jy, double* sums) {
+                           const float* jy, double* sums, float* Exp, float* Eyp, int pitch) {
   __shared__ double sh[32];
   const int nx = g.nx, ny = g.ny;
   const int nEx = (nx + 2) * (ny + 1), nEy = (nx + 1) * (ny + 2);
@@ -244,6 +244,7 @@ __global__ void k_gradient(const double* phi, GridDims g, float dx, float dy, fl
       const double d = phi[i + 1 + (j + 1) * (nx + 3)] - phi[i + (j + 1) * (nx + 3)];
       const float v = __double2float_rn(-d / double(dx));
       Ex[k] = v;
+      if (Exp) Exp[i + j * pitch] = v;
       e2 += double(v) * double(v);
       ej += double(v) * double(jx[k]);
     } else {
@@ -252,6 +253,7 @@ __global__ void k_gradient(const double* phi, GridDims g, float dx, float dy, fl
       const double d = phi[i + 1 + (j + 1) * (nx + 3)] - phi[i + 1 + j * (nx + 3)];
       const float v = __double2float_rn(-d / double(dy));
       Ey[kk] = v;
+      if (Eyp) Eyp[i + j * pitch] = v;
       e2 += double(v) * double(v);
       ej += double(v) * double(jy[kk]);
     }
@@ -354,10 +356,10 @@ void phi_fill(const double* sol, GridDims g, PoissonLayout L, float dx, double c
 }
 
 void gradient_energy(const double* phi, GridDims g, float dx, float dy, float* Ex, float* Ey, const float* jx,
-                     const float* jy, double* sums, cudaStream_t s) {
+                     const float* jy, double* sums, cudaStream_t s, float* Exp, float* Eyp) {
   const size_t n = size_t(g.nx + 2) * (g.ny + 1) + size_t(g.nx + 1) * (g.ny + 2);
   GP_CUDA(cudaMemsetAsync(sums, 0, 2 * sizeof(double), s));
-  k_gradient<<<grid1d(n), 256, 0, s>>>(phi, g, dx, dy, Ex, Ey, jx, jy, sums);
+  k_gradient<<<grid1d(n), 256, 0, s>>>(phi, g, dx, dy, Ex, Ey, jx, jy, sums, Exp, Eyp, field_pitch(g));
   GP_LAUNCH_CHECK();
 }
 

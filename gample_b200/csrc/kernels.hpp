@@ -13,8 +13,12 @@
 //  * fields: the reference's staggered arrays with its extents and strides
 //    (rho (nx+1)(ny+1), Ex (nx+2)(ny+1), Ey (nx+1)(ny+2), Bz (nx+2)(ny+2),
 //    phi double (nx+3)(ny+3); src/EMField.mm:127-144).
+//  * pitched copies of Ex and Ey for the push kernels' TMA staging: the same
+//    rows with a row pitch rounded up to 4 floats (a tensor map's row stride
+//    must be a multiple of 16 bytes), written with E.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -49,6 +53,8 @@ struct SpeciesCounters {
   uint32_t n_injected;
   uint32_t n_pulled; // removed by the last compaction (which consumes n_dead)
   uint32_t n_slow;   // pushed without a shared-memory window (chunk too spread out)
+  uint32_t err;      // chunks whose field staging did not complete in time (staged by loads instead)
+  uint32_t n_tma;    // chunks whose Ex / Ey tiles were staged by bulk tensor copies
   double ke;         // sum of 0.5 m v^2 w over particles still live (erg)
 };
 
@@ -79,6 +85,27 @@ struct FieldPtrs {
   const float* Bz;
 };
 
+// Tensor maps of the pitched Ex and Ey copies for the push kernels' field
+// staging (cp.async.bulk.tensor.2d into shared memory, out-of-range elements
+// filled with zero): one map per box size kFieldBoxW[b] x kFieldBoxH[b]
+// (columns x rows), so that a chunk copies the smallest box covering its
+// window. valid = 0: no maps, the kernels stage with per-thread loads.
+constexpr int kFieldBoxes = 3;
+constexpr int kFieldBoxW[kFieldBoxes] = {20, 24, 40};
+constexpr int kFieldBoxH[kFieldBoxes] = {8, 16, 40};
+struct FieldMaps {
+  CUtensorMap ex[kFieldBoxes];
+  CUtensorMap ey[kFieldBoxes];
+  int valid;
+};
+// Row pitch (floats) of the pitched copies.
+inline int field_pitch(const GridDims& g) { return (g.nx + 2 + 3) & ~3; }
+// Encode the maps for pitched copies Exp ((ny+1) rows) and Eyp ((ny+2) rows).
+// Returns false (maps->valid = 0) when the driver offers no tensor maps.
+bool make_field_maps(const float* Exp, const float* Eyp, GridDims g, FieldMaps* maps);
+// Ex, Ey -> their pitched copies.
+void pitch_fields(const float* Ex, const float* Ey, GridDims g, float* Exp, float* Eyp, cudaStream_t s);
+
 // ------------------------------------------------------------- particles
 // Gather + Boris + move + boundary conditions for particles [0, n) where n
 // is read from counters->n; optionally deposits the new positions (live
@@ -90,7 +117,7 @@ struct FieldPtrs {
 // chunks are compact in space because the particles are cell-sorted.
 void push(int order, int boris_order, bool deposit, bool det, bool current, bool bz_uniform, GridDims g,
           ParticleArrays p, FieldPtrs f, PushConsts c, DepositTargets d, SpeciesCounters* counters,
-          uint32_t* dead_bits, uint32_t n_bound, cudaStream_t s);
+          uint32_t* dead_bits, uint32_t n_bound, cudaStream_t s, const FieldMaps* maps = nullptr);
 
 // Deposit particles [0, counters->n) (src/Particle.mm:281-389), or with
 // injected_only the particles appended since the last push,
@@ -189,8 +216,9 @@ void phi_fill(const double* sol, GridDims g, PoissonLayout L, float dx, double c
               double* phi, cudaStream_t s);
 // Ex, Ey = -grad phi (src/EMField.mm:1080-1094) and the energy / Joule
 // sums (src/EMField.mm:1096-1111) into sums[0] (sum E^2), sums[1] (sum E.j).
+// Exp, Eyp (optional): the pitched copies, written alongside.
 void gradient_energy(const double* phi, GridDims g, float dx, float dy, float* Ex, float* Ey, const float* jx,
-                     const float* jy, double* sums, cudaStream_t s);
+                     const float* jy, double* sums, cudaStream_t s, float* Exp = nullptr, float* Eyp = nullptr);
 // Probe values for the timeseries CSV (src/EMField.mm:1130-1134).
 void probe(const double* phi, const float* Ex, const float* Ey, GridDims g, double* out3, cudaStream_t s);
 

@@ -15,8 +15,11 @@
 // deterministic mode). Chunks whose box does not fit (unsorted or drifted
 // particles) fall back to direct global gathers/atomics, per chunk; particles
 // not strictly inside the grid use bounds-checked stencils.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <climits>
 #include <cstdio>
 #include <mutex>
@@ -58,6 +61,52 @@ __device__ __forceinline__ double warp_sum(double v) {
   return v;
 }
 __device__ __forceinline__ bool in_box(int i, int j, int w, int h) { return i >= 0 && j >= 0 && i < w && j < h; }
+
+// ---- field staging by bulk tensor copies (TMA). One mbarrier per CTA, used
+// once (phase 0): thread 0 arms it with the byte count and issues the copies
+// of the Ex and Ey tiles; every thread waits on it, with a bounded number of
+// polls, before reading the tiles.
+static_assert(kFieldBoxes == 3 && kFieldBoxW[0] == 20 && kFieldBoxH[0] == 8 && kFieldBoxW[1] == 24 &&
+                  kFieldBoxH[1] == 16 && kFieldBoxW[2] == 40 && kFieldBoxH[2] == 40,
+              "box table of field_box()");
+// Smallest box that covers need_w x need_h, or -1.
+__device__ __forceinline__ int field_box(int need_w, int need_h) {
+  if (need_w <= 20 && need_h <= 8) return 0;
+  if (need_w <= 24 && need_h <= 16) return 1;
+  if (need_w <= 40 && need_h <= 40) return 2;
+  return -1;
+}
+__device__ __forceinline__ int field_box_w(int b) { return b == 0 ? 20 : (b == 1 ? 24 : 40); }
+__device__ __forceinline__ int field_box_h(int b) { return b == 0 ? 8 : (b == 1 ? 16 : 40); }
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return static_cast<uint32_t>(__cvta_generic_to_shared(p)); }
+__device__ __forceinline__ void mbar_init1(uint32_t bar) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+// Tile (x, y) .. (x + box w - 1, y + box h - 1) of a 2D tensor map into
+// shared memory at dst (row stride = box width); x is a multiple of 4
+// elements (16 bytes), dst 128-byte aligned.
+__device__ __forceinline__ void tma_tile(uint32_t dst, const CUtensorMap* map, int x, int y, uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+      ::"r"(dst), "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar)
+      : "memory");
+}
+__device__ __forceinline__ bool mbar_wait0(uint32_t bar) {
+  for (int i = 0; i < (1 << 20); ++i) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(bar)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
 
 template <bool DET>
 struct AccT {
@@ -104,6 +153,12 @@ struct Window {  // shared-memory windows of one CTA (array-index coordinates)
   int tab;               // 1: gather table of the box's cells instead of the field windows
   int tbw, tbh;          // box size in cells
   int xrs, yrs, yoff;    // Ex / Ey table row strides and the Ey table's start (float4)
+  // staged Ex / Ey tiles: origin, row stride and rows (gather windows: the
+  // window itself, or the TMA box that covers it; tables: the box the table
+  // build reads); tma: 1 when a bulk tensor copy stages them, into sEx / sEy
+  // (windows) or at byte soff of sEx, Ey one box further (tables)
+  int sx0, sy0, sstr, shh;
+  int tma, sbox, soff;
 };
 
 // r[t] = w[(t + sh) mod N] for a per-lane shift sh in [0, N).
@@ -429,17 +484,17 @@ __device__ __forceinline__ void gather(const GridDims& g, const FieldPtrs& f, co
   const int nr = sy.node - ngb, hr = sy.half - ngb + 1;   // Ex and Ey/Bz row bases
   // tap (i, j) of each component
   auto ex = [&](int i, int j) -> float {
-    if constexpr (WIN) return sEx[(hc + i - w.gx0) + (nr + j - w.gy0) * w.gw];
+    if constexpr (WIN) return sEx[(hc + i - w.sx0) + (nr + j - w.sy0) * w.sstr];
     if (CHECKED && !in_box(hc + i, nr + j, nx + 2, ny + 1)) return 0.0f;
     return __ldg(f.Ex + (hc + i) + (nr + j) * (nx + 2));
   };
   auto ey = [&](int i, int j) -> float {
-    if constexpr (WIN) return sEy[(nc + i - w.gx0) + (hr + j - w.gy0) * w.gw];
+    if constexpr (WIN) return sEy[(nc + i - w.sx0) + (hr + j - w.sy0) * w.sstr];
     if (CHECKED && !in_box(nc + i, hr + j, nx + 1, ny + 2)) return 0.0f;
     return __ldg(f.Ey + (nc + i) + (hr + j) * (nx + 1));
   };
   auto bz = [&](int i, int j) -> float {
-    if constexpr (WIN) return sBz[(hc + i - w.gx0) + (hr + j - w.gy0) * w.gw];
+    if constexpr (WIN) return sBz[(hc + i - w.sx0) + (hr + j - w.sy0) * w.sstr];
     if (CHECKED && !in_box(hc + i, hr + j, nx + 2, ny + 2)) return 0.0f;
     return __ldg(f.Bz + (hc + i) + (hr + j) * (nx + 2));
   };
@@ -538,11 +593,18 @@ __host__ __device__ constexpr size_t smem_bytes() {
 // Phases A and B of a chunk (shared by the push / deposit kernels): the box
 // of the chunk's cells, the shared-memory field window or gather table
 // covering it, and the cleared deposit window. Returns the window (also in s_w).
-template <int ORDER, bool PUSH, bool DEP, bool DET, bool CUR, bool BZU>
+// TMA: the Ex / Ey tiles are staged by bulk tensor copies from the pitched
+// copies (tm, when valid; bar: the CTA's initialised mbarrier), which fill
+// elements outside the arrays with zero as the per-thread loads do; a copy
+// that does not complete within the wait's bound makes the threads load the
+// tiles per thread instead (same values); staged chunks are
+// counted in cnt->n_tma, time-outs in cnt->err.
+template <int ORDER, bool PUSH, bool DEP, bool DET, bool CUR, bool BZU, bool TMA = false>
 __device__ __forceinline__ Window chunk_setup(const GridDims& g, const ParticleArrays& p, const FieldPtrs& f,
                                             uint32_t n, uint32_t base, int tid, int lane, int wid, float* sEx,
                                             float* sEy, float* sBz, int* sDep, int (*s_red)[kThreads / 32],
-                                            Window& s_w, int32_t& s_ref) {
+                                            Window& s_w, int32_t& s_ref, const FieldMaps* tm = nullptr,
+                                            uint32_t bar = 0, SpeciesCounters* cnt = nullptr) {
   using DL = DepositLayout<ORDER, CUR, DET>;
   constexpr bool kTab = PUSH && BZU && ORDER == 3 && !DET && !CUR;
   const int ngb = g.ngb;
@@ -601,6 +663,9 @@ __device__ __forceinline__ Window chunk_setup(const GridDims& g, const ParticleA
     w.tab = 0;
     w.tbw = w.tbh = 1;
     w.xrs = w.yrs = w.yoff = 0;
+    w.tma = w.sbox = w.soff = 0;
+    w.sx0 = w.sy0 = 0;
+    w.sstr = w.shh = 1;
     if (w.mnx != INT_MAX) {
       w.gx0 = w.mnx - ngb;
       w.gy0 = w.mny - ngb;
@@ -622,11 +687,59 @@ __device__ __forceinline__ Window chunk_setup(const GridDims& g, const ParticleA
       w.yrs = tab_row_stride(w.tbw);
       w.yoff = w.tbh * w.xrs;
       w.tab = (kTab && w.use && w.yoff + (w.tbh + 1) * w.yrs <= kTabFloat4) ? 1 : 0;
+      w.sx0 = w.gx0;
+      w.sy0 = w.gy0;
+      w.sstr = w.gw;
+      w.shh = w.gh;
+      if constexpr (TMA && PUSH) {
+        // gx0 = mnx - ngb >= 0 (box cells are interior); the copy starts at
+        // the multiple of 4 columns at or below it
+        const int x0 = w.gx0 & ~3, y0 = w.gy0;
+        if (w.use && tm->valid && (smem_u32(sEx) & 127u) == 0) {
+          if (w.tab) {
+            // taps read by the table build: Ex columns gx0 .. gx0 + tbw + 3,
+            // rows gy0 .. gy0 + tbh + 2; Ey columns gx0 .. gx0 + tbw + 2,
+            // rows gy0 .. gy0 + tbh + 3; both tiles after the tables
+            const int b = field_box(w.gx0 - x0 + w.tbw + 4, w.tbh + 4);
+            const int off = ((w.yoff + (w.tbh + 1) * w.yrs) * 16 + 127) & ~127;
+            if (b >= 0 && off + 8 * field_box_w(b) * field_box_h(b) <= 2 * kWin * int(sizeof(float))) {
+              w.tma = 1;
+              w.sbox = b;
+              w.soff = off;
+            }
+          } else {
+            const int b = field_box(w.gx0 - x0 + w.gw, w.gh);
+            if (b >= 0) {
+              w.tma = 1;
+              w.sbox = b;
+            }
+          }
+          if (w.tma) {
+            w.sx0 = x0;
+            w.sstr = field_box_w(w.sbox);
+            w.shh = field_box_h(w.sbox);
+            const uint32_t fb = 4u * uint32_t(w.sstr * w.shh);  // bytes per tile, a multiple of 128
+            const uint32_t dx = smem_u32(sEx) + uint32_t(w.soff);
+            const uint32_t dy = w.tab ? dx + fb : smem_u32(sEy);
+            mbar_expect_tx(bar, 2 * fb);
+            tma_tile(dx, &tm->ex[w.sbox], x0, y0, bar);
+            tma_tile(dy, &tm->ey[w.sbox], x0, y0, bar);
+          }
+        }
+      }
     }
     s_w = w;
   }
   __syncthreads();
   const Window w = s_w;
+  bool staged = false;  // the bulk copies have landed
+  if constexpr (TMA && PUSH) {
+    if (w.tma) {
+      staged = mbar_wait0(bar);
+      if (!staged) atomicAdd(&cnt->err, 1u);
+      if (tid == 0) atomicAdd(&cnt->n_tma, 1u);
+    }
+  }
 
   // ---- phase B: stage the field window, clear the deposit window
   if (w.use) {
@@ -642,20 +755,29 @@ __device__ __forceinline__ Window chunk_setup(const GridDims& g, const ParticleA
         const int t = ex ? e : e - nxe;
         const int rw = ex ? w.tbw + 1 : w.tbw;  // entries per table row
         const int col = t % rw, row = t / rw;
-        const float* src = ex ? f.Ex : f.Ey;
-        const int stride = ex ? nx + 2 : nx + 1;
         const int c0 = w.mnx - ngb + col, r0 = w.mny - ngb + row;  // taps c0..c0+3, r0..r0+3
         float F[16];
+        if (staged) {
+          const float* src = reinterpret_cast<const float*>(reinterpret_cast<const unsigned char*>(sEx) + w.soff) +
+                             (ex ? 0 : w.sstr * w.shh) + (c0 - w.sx0) + (r0 - w.sy0) * w.sstr;
 #pragma unroll
-        for (int j = 0; j < 4; ++j)
+          for (int j = 0; j < 4; ++j)
 #pragma unroll
-          for (int i = 0; i < 4; ++i) F[i + 4 * j] = __ldg(src + (c0 + i) + (r0 + j) * stride);
+            for (int i = 0; i < 4; ++i) F[i + 4 * j] = src[i + j * w.sstr];
+        } else {
+          const float* src = ex ? f.Ex : f.Ey;
+          const int stride = ex ? nx + 2 : nx + 1;
+#pragma unroll
+          for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int i = 0; i < 4; ++i) F[i + 4 * j] = __ldg(src + (c0 + i) + (r0 + j) * stride);
+        }
         tab_build(F, tb + (ex ? row * w.xrs : w.yoff + row * w.yrs) + kTabEntry * col);
       }
     } else if constexpr (PUSH) {
       const int nx = g.nx, ny = g.ny;
-      for (int e = tid; e < w.gw * w.gh; e += kThreads) {
-        const int col = w.gx0 + e % w.gw, row = w.gy0 + e / w.gw;
+      for (int e = tid; !staged && e < w.sstr * w.shh; e += kThreads) {
+        const int col = w.sx0 + e % w.sstr, row = w.sy0 + e / w.sstr;
         sEx[e] = in_box(col, row, nx + 2, ny + 1) ? __ldg(f.Ex + col + row * (nx + 2)) : 0.0f;
         sEy[e] = in_box(col, row, nx + 1, ny + 2) ? __ldg(f.Ey + col + row * (nx + 1)) : 0.0f;
         if constexpr (!BZU) sBz[e] = in_box(col, row, nx + 2, ny + 2) ? __ldg(f.Bz + col + row * (nx + 2)) : 0.0f;
@@ -774,7 +896,7 @@ __global__ void __launch_bounds__(kThreads, ORDER == 5 ? 2 : (PUSH && (!BZU || !
   // pushes without deposit) keeps the stencil sum everywhere.
   // (not with currents: the two paths together exceed the 64 registers of order 3)
   constexpr bool kTab = PUSH && BZU && ORDER == 3 && !DET && !CUR;
-  extern __shared__ __align__(16) unsigned char smem[];
+  extern __shared__ __align__(128) unsigned char smem[];
   float* sEx = reinterpret_cast<float*>(smem);
   float* sEy = sEx + (PUSH ? kWin : 0);
   float* sBz = sEy + (PUSH ? kWin : 0);
@@ -1037,25 +1159,28 @@ __device__ __forceinline__ void shape2(float2 h, float sx, float (&wx)[ORDER + 1
 template <int ORDER>
 __global__ void __launch_bounds__(kThreads, ORDER == 5 ? 2 : 4)
     k_push_fast(GridDims g, ParticleArrays p, FieldPtrs f, PushConsts c, int boris_order, DepositTargets d,
-                SpeciesCounters* cnt, uint32_t* dead_bits) {
+                SpeciesCounters* cnt, uint32_t* dead_bits, const __grid_constant__ FieldMaps tm) {
   using DL = DepositLayout<ORDER, false, false>;
   constexpr int N = ORDER + 1;
   constexpr bool kTab = ORDER == 3;
-  extern __shared__ __align__(16) unsigned char smem[];
+  extern __shared__ __align__(128) unsigned char smem[];
   float* sEx = reinterpret_cast<float*>(smem);
   float* sEy = sEx + kWin;
   int* sDep = reinterpret_cast<int*>(smem + 2 * size_t(kWin) * sizeof(float));
   __shared__ int s_red[4][kThreads / 32];
   __shared__ Window s_w;
   __shared__ int32_t s_ref;
+  __shared__ __align__(8) uint64_t s_bar;  // field staging (one use)
 
   const uint32_t n = cnt->n;
   const uint32_t base = blockIdx.x * uint32_t(kChunk);
   if (base >= n) return;  // uniform over the block
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   const int ngb = g.ngb;
-  const Window w = chunk_setup<ORDER, true, true, false, false, true>(g, p, f, n, base, tid, lane, wid, sEx, sEy,
-                                                                      nullptr, sDep, s_red, s_w, s_ref);
+  const uint32_t bar = smem_u32(&s_bar);
+  if (tid == 0) mbar_init1(bar);  // ordered before the copies by phase A's barriers
+  const Window w = chunk_setup<ORDER, true, true, false, false, true, true>(
+      g, p, f, n, base, tid, lane, wid, sEx, sEy, nullptr, sDep, s_red, s_w, s_ref, &tm, bar, cnt);
   WinPtrs sw;
   sw.rho = static_cast<uint32_t>(__cvta_generic_to_shared(sDep + ((lane / DL::kN2) % DL::kCopies) * DL::kStride));
 
@@ -1265,16 +1390,18 @@ __global__ void __launch_bounds__(kThreads, ORDER == 5 ? 2 : 4)
   __syncthreads();
   chunk_flush<ORDER, false, false>(g, c, d, sDep, w, tid);
   flush_tallies(tally, double(ke), c, cnt, lane);
+  // a copy whose wait timed out must not land after the CTA has left
+  if (tid == 0 && w.tma) (void)mbar_wait0(bar);
 }
 
 template <int ORDER>
 void launch_push_fast(uint32_t nblocks, cudaStream_t s, GridDims g, ParticleArrays p, FieldPtrs f, PushConsts c,
-                      int boris, DepositTargets d, SpeciesCounters* cnt, uint32_t* bits) {
+                      int boris, DepositTargets d, SpeciesCounters* cnt, uint32_t* bits, const FieldMaps& tm) {
   auto kern = k_push_fast<ORDER>;
   constexpr size_t bytes = smem_bytes<ORDER, true, true, false, false, true>();
   static std::once_flag once;
   std::call_once(once, [&] { GP_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes))); });
-  kern<<<nblocks, kThreads, bytes, s>>>(g, p, f, c, boris, d, cnt, bits);
+  kern<<<nblocks, kThreads, bytes, s>>>(g, p, f, c, boris, d, cnt, bits, tm);
 }
 
 template <int ORDER, bool PUSH, bool DEP, bool DET, bool CUR, bool BZU>
@@ -1324,16 +1451,18 @@ void dispatch_pic(bool dep, bool det, bool cur, bool bzu, uint32_t nblocks, cuda
 
 void push(int order, int boris_order, bool dep, bool det, bool cur, bool bzu, GridDims g, ParticleArrays p,
           FieldPtrs f, PushConsts c, DepositTargets d, SpeciesCounters* cnt, uint32_t* dead_bits, uint32_t n_bound,
-          cudaStream_t s) {
+          cudaStream_t s, const FieldMaps* maps) {
   // Zero the per-push counters (everything after n).
   GP_CUDA(cudaMemsetAsync(&cnt->n_dead, 0, sizeof(SpeciesCounters) - offsetof(SpeciesCounters, n_dead), s));
   if (n_bound == 0) return;
   const uint32_t nblocks = (n_bound + kChunk - 1) / kChunk;
   if (dep && !det && !cur && bzu) {  // the lean kernel of the common configuration
+    static const FieldMaps none{};     // valid = 0: per-thread staging
+    const FieldMaps& tm = maps ? *maps : none;
     switch (order) {
-      case 1: launch_push_fast<1>(nblocks, s, g, p, f, c, boris_order, d, cnt, dead_bits); break;
-      case 3: launch_push_fast<3>(nblocks, s, g, p, f, c, boris_order, d, cnt, dead_bits); break;
-      case 5: launch_push_fast<5>(nblocks, s, g, p, f, c, boris_order, d, cnt, dead_bits); break;
+      case 1: launch_push_fast<1>(nblocks, s, g, p, f, c, boris_order, d, cnt, dead_bits, tm); break;
+      case 3: launch_push_fast<3>(nblocks, s, g, p, f, c, boris_order, d, cnt, dead_bits, tm); break;
+      case 5: launch_push_fast<5>(nblocks, s, g, p, f, c, boris_order, d, cnt, dead_bits, tm); break;
       default: throw std::invalid_argument("WeightingOrder must be 1, 3 or 5");
     }
     GP_LAUNCH_CHECK();
@@ -1346,6 +1475,57 @@ void push(int order, int boris_order, bool dep, bool det, bool cur, bool bzu, Gr
     default: throw std::invalid_argument("WeightingOrder must be 1, 3 or 5");
   }
   GP_LAUNCH_CHECK();
+}
+
+namespace {
+__global__ void k_pitch_fields(const float* __restrict__ Ex, const float* __restrict__ Ey, GridDims g,
+                               float* __restrict__ Exp, float* __restrict__ Eyp, int pitch) {
+  const int nx = g.nx, ny = g.ny;
+  const int nEx = (nx + 2) * (ny + 1), nEy = (nx + 1) * (ny + 2);
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nEx + nEy; k += gridDim.x * blockDim.x) {
+    if (k < nEx)
+      Exp[k % (nx + 2) + (k / (nx + 2)) * pitch] = Ex[k];
+    else
+      Eyp[(k - nEx) % (nx + 1) + ((k - nEx) / (nx + 1)) * pitch] = Ey[k - nEx];
+  }
+}
+}  // namespace
+
+void pitch_fields(const float* Ex, const float* Ey, GridDims g, float* Exp, float* Eyp, cudaStream_t s) {
+  const int n = (g.nx + 2) * (g.ny + 1) + (g.nx + 1) * (g.ny + 2);
+  k_pitch_fields<<<std::min((n + 255) / 256, 1184), 256, 0, s>>>(Ex, Ey, g, Exp, Eyp, field_pitch(g));
+  GP_LAUNCH_CHECK();
+}
+
+bool make_field_maps(const float* Exp, const float* Eyp, GridDims g, FieldMaps* maps) {
+  *maps = FieldMaps{};
+  if ((reinterpret_cast<uintptr_t>(Exp) | reinterpret_cast<uintptr_t>(Eyp)) & 15u) return false;
+  void* fn = nullptr;
+  cudaDriverEntryPointQueryResult q{};
+  if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &fn, 12000, cudaEnableDefault, &q) != cudaSuccess ||
+      q != cudaDriverEntryPointSuccess || !fn) {
+    cudaGetLastError();
+    return false;
+  }
+  auto encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+  const cuuint64_t stride[1] = {cuuint64_t(field_pitch(g)) * sizeof(float)};  // a multiple of 16 bytes
+  const cuuint32_t estr[2] = {1, 1};
+  for (int b = 0; b < kFieldBoxes; ++b) {
+    const cuuint32_t box[2] = {cuuint32_t(kFieldBoxW[b]), cuuint32_t(kFieldBoxH[b])};
+    const cuuint64_t dx[2] = {cuuint64_t(g.nx + 2), cuuint64_t(g.ny + 1)};  // Ex: columns, rows
+    const cuuint64_t dy[2] = {cuuint64_t(g.nx + 1), cuuint64_t(g.ny + 2)};  // Ey
+    if (encode(&maps->ex[b], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(Exp), dx, stride, box, estr,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS ||
+        encode(&maps->ey[b], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(Eyp), dy, stride, box, estr,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS) {
+      *maps = FieldMaps{};
+      return false;
+    }
+  }
+  maps->valid = 1;
+  return true;
 }
 
 void deposit(int order, bool det, bool cur, GridDims g, ParticleArrays p, float scale, DepositTargets d,

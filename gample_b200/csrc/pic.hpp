@@ -133,6 +133,14 @@ class EMField {
 
   DeviceArray<float> rho, jx, jy, Ex, Ey, Ez, Bx, By, Bz;
   DeviceArray<float> delEx, delEy, delBz;  // Darwin corrections (zero in the electrostatic model)
+  // Pitched copies of Ex and Ey and their tensor maps, for the field staging
+  // of the atomic-mode push in a uniform Bz (the only kernel that reads them).
+  // k_gradient writes them with E; any other write of E marks them stale.
+  DeviceArray<float> Exp, Eyp;
+  kern::FieldMaps maps{};
+  bool e_pitched_stale = true;
+  // The maps for the push (refreshing stale copies first), or nullptr.
+  const kern::FieldMaps* pushMaps();
   DeviceArray<double> phi, sol, b, diag;  // diag: [0..1] rhs sums [2..3] E sums [4] cathode mean [5..7] probe
   // per-species deposit accumulators: int64 fixed point (deterministic mode)
   // or FP64 (fast mode); combined into rho/jx/jy by finalizeCharge()

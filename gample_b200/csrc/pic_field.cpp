@@ -158,6 +158,15 @@ EMField::EMField(const Init& init, cudaStream_t s, int nspecies) : stream(s), ho
   sol.resize(size_t(mg->unknowns()), true);
   b.resize(size_t(mg->unknowns()), true);
   if (init.flagForEquation.EMField == 2) setupDarwin();
+  if (!det && !current && bz_uniform) {
+    const size_t pitch = size_t(kern::field_pitch(dims));
+    Exp.resize(pitch * (dims.ny + 1), true);
+    Eyp.resize(pitch * (dims.ny + 2), true);
+    if (!kern::make_field_maps(Exp.get(), Eyp.get(), dims, &maps)) {
+      Exp = DeviceArray<float>();
+      Eyp = DeviceArray<float>();
+    }
+  }
 
   acc_rho.resize(nspecies);
   acc_jx.resize(nspecies);
@@ -182,6 +191,15 @@ EMField::EMField(const Init& init, cudaStream_t s, int nspecies) : stream(s), ho
     }
   }
   GP_CUDA(cudaStreamSynchronize(s));
+}
+
+const kern::FieldMaps* EMField::pushMaps() {
+  if (!maps.valid) return nullptr;
+  if (e_pitched_stale) {
+    kern::pitch_fields(Ex.get(), Ey.get(), dims, Exp.get(), Eyp.get(), stream);
+    e_pitched_stale = false;
+  }
+  return &maps;
 }
 
 void EMField::load1dField(const std::string& path, std::vector<float>& out, size_t need) const {
@@ -279,7 +297,9 @@ SolveStats EMField::solvePoisson(double dt, XmlLogger* logger) {
   }
   last_mg = poissonSolve(d);
   kern::phi_fill(sol.get(), dims, layout, dx, cathodePos, d + 4, phi.get(), stream);
-  kern::gradient_energy(phi.get(), dims, dx, dy, Ex.get(), Ey.get(), jx.get(), jy.get(), d + 2, stream);
+  kern::gradient_energy(phi.get(), dims, dx, dy, Ex.get(), Ey.get(), jx.get(), jy.get(), d + 2, stream,
+                        maps.valid ? Exp.get() : nullptr, maps.valid ? Eyp.get() : nullptr);
+  e_pitched_stale = false;
   kern::probe(phi.get(), Ex.get(), Ey.get(), dims, d + 5, stream);
   GP_CUDA(cudaMemcpyAsync(host_diag_.get(), d, 8 * sizeof(double), cudaMemcpyDeviceToHost, stream));
   GP_CUDA(cudaStreamSynchronize(stream));

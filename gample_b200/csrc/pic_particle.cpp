@@ -206,13 +206,16 @@ void Particle::update(double dt, EMField& fld, bool fused_deposit) {
   last_dt = dt;
   kern::FieldPtrs f{fld.Ex.get(), fld.Ey.get(), fld.Bz.get()};
   kern::push(order, boris, fused_deposit, fld.det, fld.current, fld.bz_uniform, fld.dims, arrays(), f, c,
-             fld.targets(index), cnt.get(), dead_bits.get(), n_bound, stream);
+             fld.targets(index), cnt.get(), dead_bits.get(), n_bound, stream, fld.pushMaps());
   ++cycles_since_sort;
 }
 
 FlowStats Particle::reduce(XmlLogger* logger) {
   kern::compact(arrays(), cnt.get(), dead_bits.get(), scratch.get(), n_bound, stream);
   kern::SpeciesCounters c = counters();
+  if (c.err)
+    throw std::runtime_error("push: " + std::to_string(c.err) +
+                             " field-staging waits timed out (tiles were loaded per thread instead)");
   FlowStats fs;
   // src/Particle.mm:915: counts in units of the charge sign
   const int unit = int(q / float(phys::ec));

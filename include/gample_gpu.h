@@ -142,6 +142,10 @@ gp_status gp_particle_reduce(gp_sim* sim, int s, gp_flow_stats* out);
 gp_status gp_particle_integrate_charge(gp_sim* sim, int s);
 /* pNum (src/Particle.mm:451, paramsBuffer) */
 gp_status gp_particle_count(gp_sim* sim, int s, uint32_t* n);
+/* Diagnostics of the last push (build addition): out[0] particles pushed
+ * without a shared-memory window, out[1] chunks whose Ex / Ey tiles were
+ * staged by bulk tensor copies, out[2] staging waits that timed out. */
+gp_status gp_particle_push_stats(gp_sim* sim, int s, uint32_t out[3]);
 /* particleBuffer contents as 24-byte records (src/Particle.h:69-78) */
 gp_status gp_particle_download(gp_sim* sim, int s, gp_particle_state* host, uint32_t capacity, uint32_t* n);
 gp_status gp_particle_upload(gp_sim* sim, int s, const gp_particle_state* host, uint32_t n);

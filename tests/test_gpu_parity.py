@@ -147,11 +147,15 @@ def test_push_matches_oracle(gpu, order, boris, bcs):
 
 
 @pytest.mark.parametrize("order", [1, 3, 5])
-def test_push_dense_sorted_uniform_bz_matches_oracle(gpu, order):
+@pytest.mark.parametrize("fused", [False, True])
+def test_push_dense_sorted_uniform_bz_matches_oracle(gpu, order, fused):
     """256 particles per cell in tile order with a uniform Bz: chunks cover a
     few cells, so order 3 gathers through the per-cell polynomial tables and
     orders 1 and 5 through the staged windows; rough random Ex, Ey make every
-    tap matter. Same tolerances as the push test above."""
+    tap matter. fused: push with the fused deposit of the atomic mode, the
+    lean kernel, whose Ex / Ey tiles arrive by bulk tensor copies from the
+    pitched copies of the uploaded fields (refreshed after the upload). Same
+    tolerances as the push test above."""
     ngx = ngy = 16
     cond = condition(ngx=ngx, ngy=ngy, order=order, ppc=256, xbc="periodic", ybc="periodic", bz_tesla=0.05,
                      dt=2e-11)
@@ -169,7 +173,12 @@ def test_push_dense_sorted_uniform_bz_matches_oracle(gpu, order):
         ora.set_particles(s, o["x"], o["y"], o["vx"], o["vy"], o["vz"], f32=True)
         sim.set_particles(s, to_aos(o["x"], o["y"], o["vx"], o["vy"], o["vz"]))
         ora.push(s)
-        sim.update(s, cond["ParamForTimeIntegration"]["TimeStep"], fused_deposit=False)
+        if fused:
+            sim.reset_charge()
+        sim.update(s, cond["ParamForTimeIntegration"]["TimeStep"], fused_deposit=fused)
+        if fused:
+            slow, staged, timeouts = sim.push_stats(s)
+            assert staged > 0 and timeouts == 0, (slow, staged, timeouts)
         g, r = sim.particles(s), ora.particles(s, f32=True)
         assert np.array_equal(g["piflag"], r["piflag"])
         vth = np.sqrt(np.mean(r["vx"].astype(np.float64) ** 2))
