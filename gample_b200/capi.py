@@ -80,6 +80,7 @@ EXPORTS = {
     "gp_particle_integrate_charge": (C.c_int, [C.c_void_p, C.c_int]),
     "gp_particle_count": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_uint32)]),
     "gp_particle_push_stats": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_uint32)]),
+    "gp_particle_sort": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
     "gp_particle_download": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_uint32, C.POINTER(C.c_uint32)]),
     "gp_particle_upload": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_uint32]),
     "gp_particle_download_raw": (C.c_int, [C.c_void_p, C.c_int] + [C.c_void_p] * 6 +
@@ -102,6 +103,7 @@ EXPORTS = {
     "gp_ensemble_free": (None, [C.c_void_p]),
     "gp_ensemble_initialize": (C.c_int, [C.c_void_p]),
     "gp_ensemble_run": (C.c_int, [C.c_void_p, C.c_int]),
+    "gp_ensemble_time_cycles": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_float)]),
     "gp_ensemble_member": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_void_p)]),
     "gp_nn_create": (C.c_int, [C.c_int, C.c_int, C.c_uint64, C.POINTER(C.c_void_p)]),
     "gp_nn_free": (None, [C.c_void_p]),
@@ -311,10 +313,17 @@ class Sim:
         check(lib().gp_particle_count(self.h, s, C.byref(n)))
         return n.value
 
+    def sort(self, s, path=0):
+        """Sort species s by cell now (path 0 automatic, 1 block-local
+        re-sort, 2 staged record scatter)."""
+        check(lib().gp_particle_sort(self.h, s, path))
+
     def push_stats(self, s):
         """(particles pushed without a window, chunks staged by bulk tensor
-        copies, staging waits that timed out) of the last push."""
-        out = (C.c_uint32 * 3)()
+        copies, staging waits that timed out, chunks gathering through the
+        per-cell tables, chunks depositing into lane-private windows) of the
+        last push."""
+        out = (C.c_uint32 * 5)()
         check(lib().gp_particle_push_stats(self.h, s, out))
         return tuple(out)
 
@@ -455,6 +464,12 @@ class Ensemble:
 
     def run(self, n):
         check(lib().gp_ensemble_run(self.p, n))
+
+    def time_cycles(self, n):
+        """run(n) timed on the device (ms, CUDA events on the member streams)."""
+        ms = C.c_float()
+        check(lib().gp_ensemble_time_cycles(self.p, n, C.byref(ms)))
+        return ms.value
 
     def close(self):
         if getattr(self, "p", None):

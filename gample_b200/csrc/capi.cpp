@@ -428,6 +428,14 @@ gp_status gp_ensemble_run(gp_ensemble* e, int ncycles) {
     return GP_OK;
   });
 }
+gp_status gp_ensemble_time_cycles(gp_ensemble* e, int ncycles, float* ms) {
+  return guarded([&] {
+    if (!e || !e->ens || !ms) throw std::invalid_argument("null argument");
+    if (ncycles < 0) throw std::invalid_argument("negative cycle count");
+    *ms = e->ens->time_cycles(ncycles);
+    return GP_OK;
+  });
+}
 gp_status gp_ensemble_member(gp_ensemble* e, int i, gp_sim** out) {
   return guarded([&] {
     if (!e || !e->ens || !out) throw std::invalid_argument("null argument");
@@ -645,13 +653,25 @@ gp_status gp_particle_count(gp_sim* sim, int s, uint32_t* n) {
     return GP_OK;
   });
 }
-gp_status gp_particle_push_stats(gp_sim* sim, int s, uint32_t out[3]) {
+gp_status gp_particle_sort(gp_sim* sim, int s, int path) {
+  return guarded([&] {
+    if (path < 0 || path > 2) throw std::invalid_argument("path must be 0, 1 or 2");
+    auto* p = species(sim, s);
+    if (path) p->random_order = path == 2;
+    p->sort();
+    GP_CUDA(cudaStreamSynchronize(p->stream));
+    return GP_OK;
+  });
+}
+gp_status gp_particle_push_stats(gp_sim* sim, int s, uint32_t out[5]) {
   return guarded([&] {
     if (!out) throw std::invalid_argument("null output");
     const auto c = species(sim, s)->counters();
     out[0] = c.n_slow;
     out[1] = c.n_tma;
     out[2] = c.err;
+    out[3] = c.n_tab;
+    out[4] = c.n_priv;
     return GP_OK;
   });
 }

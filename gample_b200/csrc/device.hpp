@@ -45,6 +45,21 @@ unsigned long long thread_kernel_launches();  // launches issued by the calling 
 // the library's streams do not synchronise with the default stream.
 // release_cached_device_memory() returns the cached blocks to the driver.
 void* device_alloc(size_t bytes);
+
+// A CUDA event with timing, destroyed with its owner.
+class TimingEvent {
+ public:
+  TimingEvent() { GP_CUDA(cudaEventCreate(&e_)); }
+  ~TimingEvent() {
+    if (e_) cudaEventDestroy(e_);
+  }
+  TimingEvent(const TimingEvent&) = delete;
+  TimingEvent& operator=(const TimingEvent&) = delete;
+  cudaEvent_t get() const { return e_; }
+
+ private:
+  cudaEvent_t e_ = nullptr;
+};
 void device_free(void* p);
 void release_cached_device_memory();
 

@@ -38,7 +38,7 @@ void Ensemble::parallel(F&& f) {
     pool.emplace_back([&] {
       try {
         GP_CUDA(cudaSetDevice(dev));
-        for (size_t i = next++; i < order_.size(); i = next++) f(*members[order_[i]]);
+        for (size_t i = next++; i < order_.size(); i = next++) f(order_[i]);
       } catch (...) {
         std::lock_guard<std::mutex> lock(mu);
         if (!first) first = std::current_exception();
@@ -49,11 +49,33 @@ void Ensemble::parallel(F&& f) {
 }
 
 void Ensemble::initialize() {
-  parallel([](Simulation& s) { s.initialize(); });
+  parallel([this](size_t i) { members[i]->initialize(); });
 }
 
 void Ensemble::run(int ncycles) {
-  parallel([ncycles](Simulation& s) { s.run(ncycles); });
+  parallel([this, ncycles](size_t i) { members[i]->run(ncycles); });
+}
+
+float Ensemble::time_cycles(int ncycles) {
+  const size_t n = members.size();
+  std::vector<TimingEvent> t0(n), t1(n);
+  for (auto& m : members) GP_CUDA(cudaStreamSynchronize(m->stream));
+  parallel([&](size_t i) {
+    Simulation& s = *members[i];
+    GP_CUDA(cudaEventRecord(t0[i].get(), s.stream));
+    s.run(ncycles);
+    GP_CUDA(cudaEventRecord(t1[i].get(), s.stream));
+  });
+  float lo = 0, hi = 0;
+  for (size_t i = 0; i < n; ++i) {
+    GP_CUDA(cudaEventSynchronize(t1[i].get()));
+    float a = 0, b = 0;
+    GP_CUDA(cudaEventElapsedTime(&a, t0[0].get(), t0[i].get()));
+    GP_CUDA(cudaEventElapsedTime(&b, t0[0].get(), t1[i].get()));
+    lo = std::min(lo, a);
+    hi = std::max(hi, b);
+  }
+  return hi - lo;
 }
 
 }  // namespace gample

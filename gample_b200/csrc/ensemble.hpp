@@ -6,7 +6,7 @@
 // (diagnostics, counter reads) do not stall the others. The threads take
 // members from a shared queue, largest first (particle capacity times
 // species, then grid cells), so that one thread does not end up with several
-// large members while the others idle. Members share no state: each one's
+// large members while the others idle; f receives the member's index. Members share no state: each one's
 // results equal the same run alone.
 #pragma once
 
@@ -22,6 +22,9 @@ class Ensemble {
   Ensemble(const std::vector<Init>& inits, int threads);
   void initialize();
   void run(int ncycles);
+  // run(ncycles) timed on the device: from the earliest member's first
+  // kernel to the latest member's last (CUDA events on the member streams).
+  float time_cycles(int ncycles);
   size_t size() const { return members.size(); }
   std::vector<std::unique_ptr<Simulation>> members;
 

@@ -55,6 +55,8 @@ struct SpeciesCounters {
   uint32_t n_slow;   // pushed without a shared-memory window (chunk too spread out)
   uint32_t err;      // chunks whose field staging did not complete in time (staged by loads instead)
   uint32_t n_tma;    // chunks whose Ex / Ey tiles were staged by bulk tensor copies
+  uint32_t n_tab;    // chunks that gathered through the per-cell tables (order 3)
+  uint32_t n_priv;   // chunks that deposited into the 32 lane-private windows
   double ke;         // sum of 0.5 m v^2 w over particles still live (erg)
 };
 

@@ -739,6 +739,8 @@ __device__ __forceinline__ Window chunk_setup(const GridDims& g, const ParticleA
       if (!staged) atomicAdd(&cnt->err, 1u);
       if (tid == 0) atomicAdd(&cnt->n_tma, 1u);
     }
+    if (tid == 0 && w.tab) atomicAdd(&cnt->n_tab, 1u);
+    if (tid == 0 && w.priv) atomicAdd(&cnt->n_priv, 1u);
   }
 
   // ---- phase B: stage the field window, clear the deposit window

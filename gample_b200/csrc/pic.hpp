@@ -197,9 +197,24 @@ class Particle {
   void sort(Particle* lender = nullptr);
   bool needs_sort = true;
   bool random_order = true;  // particles not yet sorted since loading / upload
-  int sort_interval = 0;  // cycles between sorts; 0 = when too many chunks miss their window
+  int sort_interval = 0;  // cycles between sorts; 0 = adaptive (below)
   int cycles_since_sort = 0;
   uint32_t slow_after_sort = 0;  // particles pushed outside their window right after the last sort
+  // Adaptive re-sort of the atomic mode: the push of the first cycle after a
+  // sort sets the base time per particle; each later push adds its time above
+  // that base to excess_ms; the species sorts again once excess_ms reaches
+  // the time of its last periodic sort (for a push time that grows linearly
+  // with the cycles since the sort this is the interval of least total time).
+  // Until a periodic sort has been timed, and in the deterministic mode,
+  // whose cadence must not depend on timings, the species sorts once the
+  // particles pushed outside their chunk's window exceed those of the first
+  // push after the last sort by 2 % of the live count.
+  bool cost_policy = true;
+  bool sort_timed = false, sort_pending_timing = false;
+  float last_sort_ms = 0;
+  double base_ms_per_particle = 0, excess_ms = 0;
+  uint32_t n_pushed = 0;
+  TimingEvent ev_push[2], ev_sort[2];
 
   std::string pName;
   int index = 0;

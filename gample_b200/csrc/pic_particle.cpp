@@ -181,7 +181,10 @@ void Particle::sort(Particle* lender) {
   const uint32_t extra_cap = lender && lender->stream == stream ? lender->pNumMax : 0u;
   if (!(random_order && kern::sort_by_cell_staged(dims_, buf[cur].view(), buf[1 - cur].view(), pNumMax, extra,
                                                   extra_cap, cnt.get(), sort_scratch.get(), n_bound, stream))) {
+    GP_CUDA(cudaEventRecord(ev_sort[0].get(), stream));
     kern::sort_by_cell(dims_, buf[cur].view(), buf[1 - cur].view(), cnt.get(), sort_scratch.get(), n_bound, stream);
+    GP_CUDA(cudaEventRecord(ev_sort[1].get(), stream));
+    sort_pending_timing = !random_order;  // the periodic re-sort of nearly sorted particles
     cur = 1 - cur;
   }
   random_order = false;
@@ -205,8 +208,13 @@ void Particle::update(double dt, EMField& fld, bool fused_deposit) {
   if (fused_deposit) fld.charge_dirty = true;
   last_dt = dt;
   kern::FieldPtrs f{fld.Ex.get(), fld.Ey.get(), fld.Bz.get()};
+  const kern::FieldMaps* maps = fld.pushMaps();
+  GP_CUDA(cudaEventRecord(ev_push[0].get(), stream));
   kern::push(order, boris, fused_deposit, fld.det, fld.current, fld.bz_uniform, fld.dims, arrays(), f, c,
-             fld.targets(index), cnt.get(), dead_bits.get(), n_bound, stream, fld.pushMaps());
+             fld.targets(index), cnt.get(), dead_bits.get(), n_bound, stream, maps);
+  GP_CUDA(cudaEventRecord(ev_push[1].get(), stream));
+  n_pushed = n_bound;
+  cost_policy = !fld.det;
   ++cycles_since_sort;
 }
 
@@ -236,8 +244,27 @@ FlowStats Particle::reduce(XmlLogger* logger) {
   // injection) exceed those of the first push after the last sort by 2% of
   // the live count.
   if (cycles_since_sort == 1) slow_after_sort = c.n_slow;
+  // counters() synchronised the stream: this cycle's push (and a sort before
+  // it) have completed
+  if (sort_pending_timing) {
+    GP_CUDA(cudaEventElapsedTime(&last_sort_ms, ev_sort[0].get(), ev_sort[1].get()));
+    sort_timed = true;
+    sort_pending_timing = false;
+  }
+  if (cycles_since_sort >= 1 && n_pushed > 0) {
+    float push_ms = 0;
+    GP_CUDA(cudaEventElapsedTime(&push_ms, ev_push[0].get(), ev_push[1].get()));
+    if (cycles_since_sort == 1) {
+      base_ms_per_particle = double(push_ms) / double(n_pushed);
+      excess_ms = 0;
+    } else {
+      excess_ms += double(push_ms) - base_ms_per_particle * double(n_pushed);
+    }
+  }
   if (sort_interval > 0)
     needs_sort = needs_sort || cycles_since_sort >= sort_interval;
+  else if (cost_policy && sort_timed)
+    needs_sort = needs_sort || excess_ms >= double(last_sort_ms);
   else
     needs_sort = needs_sort || double(c.n_slow) > double(slow_after_sort) + 0.02 * double(c.n);
   if (logger && logger->on()) {

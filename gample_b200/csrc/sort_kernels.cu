@@ -16,10 +16,25 @@
 // records are padded to 32 bytes: each is then one whole, aligned sector,
 // which the L2 writes back without first reading the rest of the sector from
 // DRAM (a 24-byte record shares its sectors with records that arrive at
-// other times). Otherwise they are 24-byte records. Nearly sorted particles
-// (the periodic re-sort) keep the direct scatter, whose writes are already
-// coalesced.
+// other times). Otherwise they are 24-byte records.
+//
+// Nearly sorted particles (the periodic re-sort) take a block-local path:
+// a block of kRsBlock consecutive particles, which covers a few cells plus
+// the drift since the last sort, counts its particles per cell of a 32 x 32
+// box around its middle particle in shared memory and adds each nonzero
+// count to the global histogram once. Particles outside the box (strays:
+// compaction fills holes with particles from the end of the store,
+// re-injected particles) are counted with one global atomic each. In the
+// scatter the block reserves each box cell's slots with one global atomic,
+// orders its particles by box cell in shared memory and writes each cell's
+// particles as one run of consecutive slots. Written straight from their
+// source positions, a warp's 32 particles, spread over as many cells by the
+// drift, would each land in a different 32-byte sector (27 sectors per
+// store after 25 cycles at 64 particles per cell), and the L2 would read
+// the rest of the partly written sectors back from DRAM (3x the traffic).
 #include <cuda_runtime.h>
+
+#include <climits>
 
 #include "device.hpp"
 #include "kernels.hpp"
@@ -42,11 +57,188 @@ struct KeyGeom {
   uint32_t nkeys;
 };
 
-__device__ __forceinline__ uint32_t cell_key(int32_t cell, const KeyGeom& k) {
-  if (cell < 0) return k.nkeys;  // flagged particles (none after compaction) go last
-  const int ix = cell_ix(cell), iy = cell_iy(cell);
+__device__ __forceinline__ uint32_t xy_key(int ix, int iy, const KeyGeom& k) {
   const uint32_t tile = uint32_t((iy / kTile) * k.ntx + ix / kTile);
   return (tile * kTile + uint32_t(iy % kTile)) * kTile + uint32_t(ix % kTile);
+}
+__device__ __forceinline__ uint32_t cell_key(int32_t cell, const KeyGeom& k) {
+  if (cell < 0) return k.nkeys;  // flagged particles (none after compaction) go last
+  return xy_key(cell_ix(cell), cell_iy(cell), k);
+}
+
+// ---- block-local re-sort of nearly sorted particles
+constexpr int kRsPer = 8;                    // particles per thread
+constexpr int kRsBlock = kThreads * kRsPer;  // particles per block
+constexpr int kRsBox = 32;                   // box of kRsBox x kRsBox cells
+constexpr int kRsStray = -1, kRsNone = -2;   // bin of a particle outside the box / past the end
+
+// Box origin of a block: its middle particle's cell, 15 cells to the left
+// and below (a flagged middle particle leaves every particle a stray).
+__device__ __forceinline__ void rs_origin(const int32_t* cell, uint32_t n, uint32_t base, int2& org) {
+  const uint32_t rest = n - base;
+  const int32_t c = cell[base + (rest < uint32_t(kRsBlock) ? rest / 2 : uint32_t(kRsBlock / 2))];
+  org = c >= 0 ? make_int2(cell_ix(c) - (kRsBox / 2 - 1), cell_iy(c) - (kRsBox / 2 - 1))
+               : make_int2(INT_MIN / 2, INT_MIN / 2);
+}
+__device__ __forceinline__ int rs_bin(int32_t c, int2 org) {
+  if (c < 0) return kRsStray;
+  const unsigned dx = unsigned(cell_ix(c) - org.x), dy = unsigned(cell_iy(c) - org.y);
+  return dx < unsigned(kRsBox) && dy < unsigned(kRsBox) ? int(dy * kRsBox + dx) : kRsStray;
+}
+// Count the block's particles per box cell into bins (warp-aggregated
+// shared atomics); strays are added to the global counts when counts != 0.
+__device__ __forceinline__ void rs_count(const int32_t* __restrict__ cell, uint32_t n, uint32_t base, int2 org,
+                                         const KeyGeom& g, uint32_t* bins, uint32_t* counts) {
+  const int lane = threadIdx.x & 31;
+  int32_t c[kRsPer];  // all loads first, so that they are in flight together
+#pragma unroll
+  for (int i = 0; i < kRsPer; ++i) {
+    const uint32_t k = base + uint32_t(i * kThreads) + threadIdx.x;
+    c[i] = k < n ? __ldg(cell + k) : INT_MIN;
+  }
+#pragma unroll
+  for (int i = 0; i < kRsPer; ++i) {
+    const int bin = c[i] != INT_MIN ? rs_bin(c[i], org) : kRsNone;
+    const unsigned peers = __match_any_sync(0xffffffffu, bin);
+    if (bin >= 0 && lane == __ffs(peers) - 1) atomicAdd(&bins[bin], uint32_t(__popc(peers)));
+    if (counts && bin == kRsStray) atomicAdd(&counts[cell_key(c[i], g)], 1u);
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) k_rs_hist(const int32_t* cell, const SpeciesCounters* cnt, KeyGeom g,
+                                                      uint32_t* counts) {
+  __shared__ uint32_t bins[kRsBox * kRsBox];
+  __shared__ int2 s_org;
+  const uint32_t n = cnt->n, base = blockIdx.x * uint32_t(kRsBlock);
+  if (base >= n) return;  // uniform over the block
+  for (int b = threadIdx.x; b < kRsBox * kRsBox; b += kThreads) bins[b] = 0;
+  if (threadIdx.x == 0) rs_origin(cell, n, base, s_org);
+  __syncthreads();
+  const int2 org = s_org;
+  rs_count(cell, n, base, org, g, bins, counts);
+  __syncthreads();
+  for (int b = threadIdx.x; b < kRsBox * kRsBox; b += kThreads)
+    if (const uint32_t v = bins[b]) atomicAdd(&counts[xy_key(org.x + b % kRsBox, org.y + b / kRsBox, g)], v);
+}
+
+// Shared memory of k_rs_scatter: the staged particles (six words and the
+// destination slot each, in box-cell order, strays last) and, per box cell
+// and for the strays (entry kRsBins), the count / cursor, the first local
+// position and the first global slot.
+constexpr int kRsBins = kRsBox * kRsBox;
+constexpr size_t kRsSmem = (size_t(kRsBlock) * 7 + 3 * size_t(kRsBins + 1)) * sizeof(uint32_t);
+
+__global__ void __launch_bounds__(kThreads) k_rs_scatter(ParticleArrays src, ParticleArrays dst,
+                                                         const SpeciesCounters* cnt, KeyGeom g, uint32_t* offsets) {
+  extern __shared__ __align__(16) uint32_t rs_smem[];
+  uint32_t* st = rs_smem;                   // [7][kRsBlock]: cell, ox, oy, vx, vy, vz, slot
+  uint32_t* cur = st + 7 * kRsBlock;        // per bin: count, then cursor
+  uint32_t* lbase = cur + (kRsBins + 1);    // per bin: first local position
+  uint32_t* gbase = lbase + (kRsBins + 1);  // per box cell: first global slot
+  __shared__ int2 s_org;
+  __shared__ uint32_t s_warp[kThreads / 32];
+  const uint32_t n = cnt->n, base = blockIdx.x * uint32_t(kRsBlock);
+  if (base >= n) return;  // uniform over the block
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  for (int b = tid; b <= kRsBins; b += kThreads) cur[b] = 0;
+  if (tid == 0) rs_origin(src.cell, n, base, s_org);
+  __syncthreads();
+  const int2 org = s_org;
+  // this thread's particles, all loads first: cell, bin (strays: bin
+  // kRsBins) and the five state words
+  int32_t c[kRsPer];
+  int bin[kRsPer];
+  float w[5][kRsPer];
+#pragma unroll
+  for (int i = 0; i < kRsPer; ++i) {
+    const uint32_t k = base + uint32_t(i * kThreads + tid);
+    const bool in = k < n;
+    c[i] = in ? __ldg(src.cell + k) : -1;
+    w[0][i] = in ? __ldg(src.ox + k) : 0.0f;
+    w[1][i] = in ? __ldg(src.oy + k) : 0.0f;
+    w[2][i] = in ? __ldg(src.vx + k) : 0.0f;
+    w[3][i] = in ? __ldg(src.vy + k) : 0.0f;
+    w[4][i] = in ? __ldg(src.vz + k) : 0.0f;
+  }
+#pragma unroll
+  for (int i = 0; i < kRsPer; ++i) {
+    const uint32_t k = base + uint32_t(i * kThreads + tid);
+    const int b = k < n ? rs_bin(c[i], org) : kRsNone;
+    bin[i] = b == kRsStray ? kRsBins : b;
+  }
+#pragma unroll
+  for (int i = 0; i < kRsPer; ++i) {
+    const unsigned peers = __match_any_sync(0xffffffffu, bin[i]);
+    if (bin[i] >= 0 && lane == __ffs(peers) - 1) atomicAdd(&cur[bin[i]], uint32_t(__popc(peers)));
+  }
+  __syncthreads();
+  // exclusive scan of the counts into lbase (thread t: bins t*kEach ..),
+  // the box cells' global slots reserved, cursors back to zero
+  constexpr int kEach = (kRsBins + 1 + kThreads - 1) / kThreads;
+  uint32_t v[kEach], run = 0;
+#pragma unroll
+  for (int e = 0; e < kEach; ++e) {
+    const int b = tid * kEach + e;
+    v[e] = b <= kRsBins ? cur[b] : 0u;
+    run += v[e];
+  }
+  uint32_t incl = run;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += y;
+  }
+  if (lane == 31) s_warp[wid] = incl;
+  __syncthreads();
+  uint32_t off = incl - run;
+  for (int q = 0; q < wid; ++q) off += s_warp[q];
+  const uint32_t total = [&] {
+    uint32_t t = 0;
+    for (int q = 0; q < kThreads / 32; ++q) t += s_warp[q];
+    return t;
+  }();
+#pragma unroll
+  for (int e = 0; e < kEach; ++e) {
+    const int b = tid * kEach + e;
+    if (b <= kRsBins) {
+      lbase[b] = off;
+      cur[b] = 0;
+      if (b < kRsBins)
+        gbase[b] = v[e] ? atomicAdd(&offsets[xy_key(org.x + b % kRsBox, org.y + b / kRsBox, g)], v[e]) : 0u;
+    }
+    off += v[e];
+  }
+  __syncthreads();
+  // stage each particle at lbase[bin] + rank with its destination slot
+  const unsigned lt = (1u << lane) - 1u;
+#pragma unroll
+  for (int i = 0; i < kRsPer; ++i) {
+    const unsigned peers = __match_any_sync(0xffffffffu, bin[i]);
+    const int leader = __ffs(peers) - 1;
+    uint32_t r = 0;
+    if (bin[i] >= 0 && lane == leader) r = atomicAdd(&cur[bin[i]], uint32_t(__popc(peers)));
+    r = __shfl_sync(0xffffffffu, r, leader) + uint32_t(__popc(peers & lt));
+    if (bin[i] >= 0) {
+      const uint32_t lp = lbase[bin[i]] + r;
+      const uint32_t slot = bin[i] < kRsBins ? gbase[bin[i]] + r : atomicAdd(&offsets[cell_key(c[i], g)], 1u);
+      st[0 * kRsBlock + lp] = uint32_t(c[i]);
+#pragma unroll
+      for (int q = 0; q < 5; ++q) st[(q + 1) * kRsBlock + lp] = __float_as_uint(w[q][i]);
+      st[6 * kRsBlock + lp] = slot;
+    }
+  }
+  __syncthreads();
+  // write out: consecutive local positions of one box cell go to
+  // consecutive slots
+  for (uint32_t j = tid; j < total; j += kThreads) {
+    const uint32_t slot = st[6 * kRsBlock + j];
+    dst.cell[slot] = int32_t(st[j]);
+    dst.ox[slot] = __uint_as_float(st[1 * kRsBlock + j]);
+    dst.oy[slot] = __uint_as_float(st[2 * kRsBlock + j]);
+    dst.vx[slot] = __uint_as_float(st[3 * kRsBlock + j]);
+    dst.vy[slot] = __uint_as_float(st[4 * kRsBlock + j]);
+    dst.vz[slot] = __uint_as_float(st[5 * kRsBlock + j]);
+  }
 }
 
 __global__ void __launch_bounds__(kThreads) k_cs_hist(const int32_t* cell, const SpeciesCounters* cnt, KeyGeom g,
@@ -138,30 +330,6 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_sums(uint32_t* sums, uint
 __global__ void k_scan_add(uint32_t* out, const uint32_t* sums, uint32_t n) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) out[i] += sums[i / kScanChunk];
-}
-
-__global__ void __launch_bounds__(kThreads) k_cs_scatter(ParticleArrays src, ParticleArrays dst,
-                                                         const SpeciesCounters* cnt, KeyGeom g, uint32_t* offsets) {
-  const uint32_t n = cnt->n;
-  const int lane = threadIdx.x & 31;
-  const unsigned lt = (1u << lane) - 1u;
-  for (uint32_t base = (blockIdx.x * kThreads + threadIdx.x) & ~31u; base < n; base += gridDim.x * kThreads) {
-    const uint32_t k = base + lane;
-    const uint32_t key = k < n ? cell_key(src.cell[k], g) : kNoKey;
-    const unsigned peers = __match_any_sync(0xffffffffu, key);
-    const int leader = __ffs(peers) - 1;
-    uint32_t slot = 0;
-    if (key != kNoKey && lane == leader) slot = atomicAdd(&offsets[key], uint32_t(__popc(peers)));
-    slot = __shfl_sync(0xffffffffu, slot, leader) + uint32_t(__popc(peers & lt));
-    if (key != kNoKey) {
-      dst.cell[slot] = src.cell[k];
-      dst.ox[slot] = src.ox[k];
-      dst.oy[slot] = src.oy[k];
-      dst.vx[slot] = src.vx[k];
-      dst.vy[slot] = src.vy[k];
-      dst.vz[slot] = src.vz[k];
-    }
-  }
 }
 
 // One particle as a 24-byte record (8-byte aligned: three 64-bit stores).
@@ -362,7 +530,8 @@ void sort_by_cell(GridDims g, ParticleArrays src, ParticleArrays dst, const Spec
   uint32_t* sums = scratch + 2 * size_t(nk);
   const uint32_t nb = (nk + kScanChunk - 1) / kScanChunk;
   GP_CUDA(cudaMemsetAsync(counts, 0, size_t(nk) * sizeof(uint32_t), s));
-  k_cs_hist<<<grid_for(n_bound), kThreads, 0, s>>>(src.cell, cnt, kg, counts);
+  const uint32_t nblocks = (n_bound + kRsBlock - 1) / kRsBlock;
+  k_rs_hist<<<nblocks, kThreads, 0, s>>>(src.cell, cnt, kg, counts);
   GP_LAUNCH_CHECK();
   k_scan_local<<<nb, kScanThreads, 0, s>>>(counts, offsets, sums, nk);
   GP_LAUNCH_CHECK();
@@ -370,7 +539,12 @@ void sort_by_cell(GridDims g, ParticleArrays src, ParticleArrays dst, const Spec
   GP_LAUNCH_CHECK();
   k_scan_add<<<(nk + 255) / 256, 256, 0, s>>>(offsets, sums, nk);
   GP_LAUNCH_CHECK();
-  k_cs_scatter<<<grid_for(n_bound), kThreads, 0, s>>>(src, dst, cnt, kg, offsets);
+  static bool attr = [] {
+    GP_CUDA(cudaFuncSetAttribute(k_rs_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kRsSmem)));
+    return true;
+  }();
+  (void)attr;
+  k_rs_scatter<<<nblocks, kThreads, kRsSmem, s>>>(src, dst, cnt, kg, offsets);
   GP_LAUNCH_CHECK();
 }
 

@@ -142,10 +142,18 @@ gp_status gp_particle_reduce(gp_sim* sim, int s, gp_flow_stats* out);
 gp_status gp_particle_integrate_charge(gp_sim* sim, int s);
 /* pNum (src/Particle.mm:451, paramsBuffer) */
 gp_status gp_particle_count(gp_sim* sim, int s, uint32_t* n);
+/* Sort species s by cell now (build addition; the time loop sorts by
+ * itself). path: 0 as the loop would (staged records for particles in
+ * random order, the block-local re-sort otherwise), 1 the block-local
+ * re-sort of nearly sorted particles, 2 the staged record scatter. */
+gp_status gp_particle_sort(gp_sim* sim, int s, int path);
 /* Diagnostics of the last push (build addition): out[0] particles pushed
  * without a shared-memory window, out[1] chunks whose Ex / Ey tiles were
- * staged by bulk tensor copies, out[2] staging waits that timed out. */
-gp_status gp_particle_push_stats(gp_sim* sim, int s, uint32_t out[3]);
+ * staged by bulk tensor copies, out[2] staging waits that timed out, out[3]
+ * chunks that gathered through the per-cell tables, out[4] chunks that
+ * deposited into lane-private windows (out[1], out[3], out[4]: the atomic
+ * mode's push in a uniform Bz). */
+gp_status gp_particle_push_stats(gp_sim* sim, int s, uint32_t out[5]);
 /* particleBuffer contents as 24-byte records (src/Particle.h:69-78) */
 gp_status gp_particle_download(gp_sim* sim, int s, gp_particle_state* host, uint32_t capacity, uint32_t* n);
 gp_status gp_particle_upload(gp_sim* sim, int s, const gp_particle_state* host, uint32_t n);
@@ -256,6 +264,9 @@ gp_status gp_ensemble_create(const gp_init* const* inits, int n, int threads, gp
 void gp_ensemble_free(gp_ensemble* e);
 gp_status gp_ensemble_initialize(gp_ensemble* e);
 gp_status gp_ensemble_run(gp_ensemble* e, int ncycles);
+/* gp_ensemble_run timed on the device (ms): from the earliest member's first
+ * kernel to the latest member's last, by CUDA events on the member streams */
+gp_status gp_ensemble_time_cycles(gp_ensemble* e, int ncycles, float* ms);
 /* a view of member i for the gp_sim_* / gp_particle_* / gp_field_* calls
  * (owned by the ensemble; gp_sim_free on it does nothing) */
 gp_status gp_ensemble_member(gp_ensemble* e, int i, gp_sim** out);

@@ -129,6 +129,53 @@ def test_upload_in_random_order_is_sorted_by_tile(gpu, n):
     sim.close()
 
 
+def _tile_key(cell):
+    ix, iy = (cell & 0xFFFF).astype(np.int64), (cell >> 16).astype(np.int64)
+    return (((iy // 8) * 4096 + ix // 8) * 8 + iy % 8) * 8 + ix % 8
+
+
+@pytest.mark.parametrize("n", [7, 300_001])
+@pytest.mark.parametrize("path", [1, 2])
+def test_resort_of_nearly_sorted_particles_with_strays(gpu, n, path):
+    """The periodic re-sort's input: particles in tile order that have since
+    drifted by up to three cells, with 2 % strays anywhere on the grid (holes
+    refilled from the end of the store, re-injected particles) and a ragged
+    last block. The block-local re-sort (path 1) and the staged record
+    scatter (path 2) both return the same particles in tile order."""
+    ngx, ngy = 96, 72
+    cond = condition(ngx=ngx, ngy=ngy, order=1, ppc=2, xbc="periodic", ybc="periodic",
+                     pnum_max=max(n, 2 * ngx * ngy) + 10)
+    sim = capi.Sim(cond)
+    rng = np.random.default_rng(n + path)
+    x = rng.uniform(0, ngx, n)
+    y = rng.uniform(0, ngy, n)
+    order = np.lexsort((np.floor(x) % 8, np.floor(y) % 8, np.floor(x) // 8, np.floor(y) // 8))
+    x, y = x[order], y[order]
+    x = (x + rng.uniform(-3, 3, n)) % ngx
+    y = (y + rng.uniform(-3, 3, n)) % ngy
+    stray = rng.random(n) < 0.02
+    x[stray] = rng.uniform(0, ngx, np.count_nonzero(stray))
+    y[stray] = rng.uniform(0, ngy, np.count_nonzero(stray))
+    v = rng.normal(0.0, 1e5, (3, n)).astype(np.float32)
+    xf, yf = x.astype(np.float32), y.astype(np.float32)
+    xf[xf >= ngx], yf[yf >= ngy] = 0.0, 0.0  # rounded up onto the far edge
+    recs = _records(xf, yf, v[0], v[1], v[2])
+    for s in range(2):
+        sim.set_particles(s, recs)
+    cols = ("cell", "ox", "oy", "vx", "vy", "vz")
+    as_bits = lambda d: np.stack([d[c].view(np.uint32) for c in cols])
+    for s in range(2):
+        before = sim.particles_raw(s)
+        assert np.any(np.diff(_tile_key(before["cell"])) < 0) or n < 10
+        sim.sort(s, path)
+        after = sim.particles_raw(s)
+        assert len(after["cell"]) == n
+        assert np.all(np.diff(_tile_key(after["cell"])) >= 0)
+        a, b = as_bits(before), as_bits(after)
+        np.testing.assert_array_equal(a[:, np.lexsort(a[::-1])], b[:, np.lexsort(b[::-1])])
+    sim.close()
+
+
 def test_upload_beyond_the_capacity_is_an_error(gpu):
     cond = condition(ngx=16, ngy=16, order=1, ppc=2, pnum_max=1000)
     sim = capi.Sim(cond)

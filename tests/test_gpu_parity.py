@@ -177,7 +177,7 @@ def test_push_dense_sorted_uniform_bz_matches_oracle(gpu, order, fused):
             sim.reset_charge()
         sim.update(s, cond["ParamForTimeIntegration"]["TimeStep"], fused_deposit=fused)
         if fused:
-            slow, staged, timeouts = sim.push_stats(s)
+            slow, staged, timeouts, _, _ = sim.push_stats(s)
             assert staged > 0 and timeouts == 0, (slow, staged, timeouts)
         g, r = sim.particles(s), ora.particles(s, f32=True)
         assert np.array_equal(g["piflag"], r["piflag"])
