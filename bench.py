@@ -277,6 +277,11 @@ def ensemble_leg(members, steps, threads, seed=0):
     ms = ens.time_cycles(steps)
     el = time.perf_counter() - t0
     n1 = sum(m.count(0) + m.count(1) for m in ens.members)
+    chunks = {}
+    for m in ens.members:
+        for sp in range(2):
+            per = m.push_stats(sp)[5]
+            chunks[str(per)] = chunks.get(str(per), 0) + 1
     ens.close()
     del ens
     batched = 0.5 * (n0 + n1) * steps / (ms / 1e3)
@@ -293,6 +298,7 @@ def ensemble_leg(members, steps, threads, seed=0):
     return {"members": members, "threads": threads, "steps": steps, "particles": n1,
             "ppc_range": [16, 256], "pushes_per_s": batched, "sequential_pushes_per_s": sequential,
             "speedup": batched / sequential, "ms": ms, "wall_s": el,
+            "autotuned_particles_per_chunk": chunks,
             "timing": "CUDA events on the member streams: earliest member start to latest member end; "
                       "sequential: the sum of each member's device-timed cycles run alone"}
 

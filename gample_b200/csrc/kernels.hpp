@@ -109,6 +109,10 @@ bool make_field_maps(const float* Exp, const float* Eyp, GridDims g, FieldMaps* 
 void pitch_fields(const float* Ex, const float* Ey, GridDims g, float* Exp, float* Eyp, cudaStream_t s);
 
 // ------------------------------------------------------------- particles
+// Particles per thread of the push's CTAs (256 threads): the atomic-mode
+// push in a uniform Bz also runs with half as many (1024-particle chunks),
+// chunk_per = kPushChunkPer / 2, for an autotuner to pick per species.
+constexpr int kPushChunkPer = 8;
 // Gather + Boris + move + boundary conditions for particles [0, n) where n
 // is read from counters->n; optionally deposits the new positions (live
 // particles only). Writes the dead bitmap (bit k = particle k flagged) and
@@ -119,7 +123,8 @@ void pitch_fields(const float* Ex, const float* Ey, GridDims g, float* Exp, floa
 // chunks are compact in space because the particles are cell-sorted.
 void push(int order, int boris_order, bool deposit, bool det, bool current, bool bz_uniform, GridDims g,
           ParticleArrays p, FieldPtrs f, PushConsts c, DepositTargets d, SpeciesCounters* counters,
-          uint32_t* dead_bits, uint32_t n_bound, cudaStream_t s, const FieldMaps* maps = nullptr);
+          uint32_t* dead_bits, uint32_t n_bound, cudaStream_t s, const FieldMaps* maps = nullptr,
+          int chunk_per = kPushChunkPer);
 
 // Deposit particles [0, counters->n) (src/Particle.mm:281-389), or with
 // injected_only the particles appended since the last push,

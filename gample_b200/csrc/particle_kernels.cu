@@ -35,7 +35,7 @@ namespace kern {
 namespace {
 
 constexpr int kThreads = 256;
-constexpr int kPer = 8;                      // particles per thread
+constexpr int kPer = kPushChunkPer;          // particles per thread
 constexpr int kChunk = kThreads * kPer;      // particles per CTA
 constexpr int kWin = 1600;                   // entries of a shared-memory window (e.g. 40 x 40)
 constexpr int kMargin = 2;                   // deposit-window margin for the motion of one step (cells)
@@ -599,7 +599,7 @@ __host__ __device__ constexpr size_t smem_bytes() {
 // that does not complete within the wait's bound makes the threads load the
 // tiles per thread instead (same values); staged chunks are
 // counted in cnt->n_tma, time-outs in cnt->err.
-template <int ORDER, bool PUSH, bool DEP, bool DET, bool CUR, bool BZU, bool TMA = false>
+template <int ORDER, bool PUSH, bool DEP, bool DET, bool CUR, bool BZU, bool TMA = false, int PER = kPer>
 __device__ __forceinline__ Window chunk_setup(const GridDims& g, const ParticleArrays& p, const FieldPtrs& f,
                                             uint32_t n, uint32_t base, int tid, int lane, int wid, float* sEx,
                                             float* sEy, float* sBz, int* sDep, int (*s_red)[kThreads / 32],
@@ -614,7 +614,8 @@ __device__ __forceinline__ Window chunk_setup(const GridDims& g, const ParticleA
   // blow up the box; particles outside it use the global paths.
   if (tid == 0) {
     const uint32_t rest = n - base;
-    const int32_t rc = p.cell[base + (rest < uint32_t(kChunk) ? rest / 2 : uint32_t(kChunk / 2))];
+    constexpr uint32_t chunk = uint32_t(kThreads * PER);
+    const int32_t rc = p.cell[base + (rest < chunk ? rest / 2 : chunk / 2)];
     s_ref = (rc >= 0 && interior(g, cell_ix(rc), cell_iy(rc))) ? rc : -1;
   }
   __syncthreads();
@@ -623,7 +624,7 @@ __device__ __forceinline__ Window chunk_setup(const GridDims& g, const ParticleA
   const int reach = ref >= 0 ? kReach : INT_MAX / 2;
   int mnx = INT_MAX, mny = INT_MAX, mxx = INT_MIN, mxy = INT_MIN;
 #pragma unroll
-  for (int i = 0; i < kPer; ++i) {
+  for (int i = 0; i < PER; ++i) {
     const uint32_t k = base + uint32_t(i * kThreads + tid);
     const int32_t cl = k < n ? p.cell[k] : -1;
     if (cl >= 0) {
@@ -1158,7 +1159,7 @@ __device__ __forceinline__ void shape2(float2 h, float sx, float (&wx)[ORDER + 1
 // origin folded into the shared-memory base addresses (one multiply-add per
 // address), box tests are one unsigned comparison per axis, and the
 // per-particle reads of the window descriptor from shared memory are gone.
-template <int ORDER>
+template <int ORDER, int PER>
 __global__ void __launch_bounds__(kThreads, ORDER == 5 ? 2 : 4)
     k_push_fast(GridDims g, ParticleArrays p, FieldPtrs f, PushConsts c, int boris_order, DepositTargets d,
                 SpeciesCounters* cnt, uint32_t* dead_bits, const __grid_constant__ FieldMaps tm) {
@@ -1175,13 +1176,13 @@ __global__ void __launch_bounds__(kThreads, ORDER == 5 ? 2 : 4)
   __shared__ __align__(8) uint64_t s_bar;  // field staging (one use)
 
   const uint32_t n = cnt->n;
-  const uint32_t base = blockIdx.x * uint32_t(kChunk);
+  const uint32_t base = blockIdx.x * uint32_t(kThreads * PER);
   if (base >= n) return;  // uniform over the block
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   const int ngb = g.ngb;
   const uint32_t bar = smem_u32(&s_bar);
   if (tid == 0) mbar_init1(bar);  // ordered before the copies by phase A's barriers
-  const Window w = chunk_setup<ORDER, true, true, false, false, true, true>(
+  const Window w = chunk_setup<ORDER, true, true, false, false, true, true, PER>(
       g, p, f, n, base, tid, lane, wid, sEx, sEy, nullptr, sDep, s_red, s_w, s_ref, &tm, bar, cnt);
   WinPtrs sw;
   sw.rho = static_cast<uint32_t>(__cvta_generic_to_shared(sDep + ((lane / DL::kN2) % DL::kCopies) * DL::kStride));
@@ -1207,7 +1208,7 @@ __global__ void __launch_bounds__(kThreads, ORDER == 5 ? 2 : 4)
                          4u * uint32_t((ngb + w.dx0) + (ngb + w.dy0) * kPW);
 
   uint32_t tally = 0;
-  float ke = 0.0f;  // sum of |v|^2 over this thread's pushed particles (at most kPer)
+  float ke = 0.0f;  // sum of |v|^2 over this thread's pushed particles (at most PER)
   int32_t q_cell = -1;
   float q_ox = 0.0f, q_oy = 0.0f, q_vx = 0.0f, q_vy = 0.0f, q_vz = 0.0f;
   auto fetch = [&](uint32_t k) {
@@ -1222,11 +1223,11 @@ __global__ void __launch_bounds__(kThreads, ORDER == 5 ? 2 : 4)
   };
   fetch(base + uint32_t(tid));
 #pragma unroll 1
-  for (int i = 0; i < kPer; ++i) {
+  for (int i = 0; i < PER; ++i) {
     const uint32_t k = base + uint32_t(i * kThreads + tid);
     const int32_t cell = q_cell;
     float ox = q_ox, oy = q_oy, vx = q_vx, vy = q_vy, vz = q_vz;
-    if (i + 1 < kPer) fetch(k + uint32_t(kThreads));
+    if (i + 1 < PER) fetch(k + uint32_t(kThreads));
     int fl = 0;
     // The gather of a particle in the chunk's box: per-cell polynomial
     // tables (order 3) or the staged windows (which add into Epx, Epy: the
@@ -1396,10 +1397,10 @@ __global__ void __launch_bounds__(kThreads, ORDER == 5 ? 2 : 4)
   if (tid == 0 && w.tma) (void)mbar_wait0(bar);
 }
 
-template <int ORDER>
+template <int ORDER, int PER>
 void launch_push_fast(uint32_t nblocks, cudaStream_t s, GridDims g, ParticleArrays p, FieldPtrs f, PushConsts c,
                       int boris, DepositTargets d, SpeciesCounters* cnt, uint32_t* bits, const FieldMaps& tm) {
-  auto kern = k_push_fast<ORDER>;
+  auto kern = k_push_fast<ORDER, PER>;
   constexpr size_t bytes = smem_bytes<ORDER, true, true, false, false, true>();
   static std::once_flag once;
   std::call_once(once, [&] { GP_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes))); });
@@ -1453,7 +1454,7 @@ void dispatch_pic(bool dep, bool det, bool cur, bool bzu, uint32_t nblocks, cuda
 
 void push(int order, int boris_order, bool dep, bool det, bool cur, bool bzu, GridDims g, ParticleArrays p,
           FieldPtrs f, PushConsts c, DepositTargets d, SpeciesCounters* cnt, uint32_t* dead_bits, uint32_t n_bound,
-          cudaStream_t s, const FieldMaps* maps) {
+          cudaStream_t s, const FieldMaps* maps, int chunk_per) {
   // Zero the per-push counters (everything after n).
   GP_CUDA(cudaMemsetAsync(&cnt->n_dead, 0, sizeof(SpeciesCounters) - offsetof(SpeciesCounters, n_dead), s));
   if (n_bound == 0) return;
@@ -1461,12 +1462,19 @@ void push(int order, int boris_order, bool dep, bool det, bool cur, bool bzu, Gr
   if (dep && !det && !cur && bzu) {  // the lean kernel of the common configuration
     static const FieldMaps none{};     // valid = 0: per-thread staging
     const FieldMaps& tm = maps ? *maps : none;
+    if (chunk_per != kPer && chunk_per != kPer / 2) throw std::invalid_argument("chunk_per must be 8 or 4");
+    const bool half = chunk_per == kPer / 2;
+    const uint32_t nb = half ? (n_bound + kChunk / 2 - 1) / (kChunk / 2) : nblocks;
+#define GP_FAST(O) \
+  half ? launch_push_fast<O, kPer / 2>(nb, s, g, p, f, c, boris_order, d, cnt, dead_bits, tm) \
+       : launch_push_fast<O, kPer>(nb, s, g, p, f, c, boris_order, d, cnt, dead_bits, tm)
     switch (order) {
-      case 1: launch_push_fast<1>(nblocks, s, g, p, f, c, boris_order, d, cnt, dead_bits, tm); break;
-      case 3: launch_push_fast<3>(nblocks, s, g, p, f, c, boris_order, d, cnt, dead_bits, tm); break;
-      case 5: launch_push_fast<5>(nblocks, s, g, p, f, c, boris_order, d, cnt, dead_bits, tm); break;
+      case 1: GP_FAST(1); break;
+      case 3: GP_FAST(3); break;
+      case 5: GP_FAST(5); break;
       default: throw std::invalid_argument("WeightingOrder must be 1, 3 or 5");
     }
+#undef GP_FAST
     GP_LAUNCH_CHECK();
     return;
   }

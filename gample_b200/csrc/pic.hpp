@@ -215,6 +215,15 @@ class Particle {
   double base_ms_per_particle = 0, excess_ms = 0;
   uint32_t n_pushed = 0;
   TimingEvent ev_push[2], ev_sort[2];
+  // Autotuner of the atomic-mode push in a uniform Bz: the four pushes after
+  // the first sort alternate the chunk size (2048, 1024, 1024, 2048
+  // particles per CTA, so that the drift of the push time since the sort
+  // weighs on both alike); the faster per particle is kept for the run.
+  int chunk_per = kern::kPushChunkPer;
+  int tune_step = -1;  // -1: not started, 0..3: tuning, 4: done
+  int tune_per = kern::kPushChunkPer;
+  double tune_ms[2] = {0, 0};  // summed ms per particle: [0] 2048, [1] 1024
+  bool lean_push = false;      // the last push ran the tunable kernel
 
   std::string pName;
   int index = 0;

@@ -209,9 +209,16 @@ void Particle::update(double dt, EMField& fld, bool fused_deposit) {
   last_dt = dt;
   kern::FieldPtrs f{fld.Ex.get(), fld.Ey.get(), fld.Bz.get()};
   const kern::FieldMaps* maps = fld.pushMaps();
+  lean_push = fused_deposit && !fld.det && !fld.current && fld.bz_uniform;
+  tune_per = chunk_per;
+  if (lean_push && tune_step >= 0 && tune_step < 4) {
+    constexpr int kABBA[4] = {kern::kPushChunkPer, kern::kPushChunkPer / 2, kern::kPushChunkPer / 2,
+                              kern::kPushChunkPer};
+    tune_per = kABBA[tune_step];
+  }
   GP_CUDA(cudaEventRecord(ev_push[0].get(), stream));
   kern::push(order, boris, fused_deposit, fld.det, fld.current, fld.bz_uniform, fld.dims, arrays(), f, c,
-             fld.targets(index), cnt.get(), dead_bits.get(), n_bound, stream, maps);
+             fld.targets(index), cnt.get(), dead_bits.get(), n_bound, stream, maps, tune_per);
   GP_CUDA(cudaEventRecord(ev_push[1].get(), stream));
   n_pushed = n_bound;
   cost_policy = !fld.det;
@@ -254,8 +261,18 @@ FlowStats Particle::reduce(XmlLogger* logger) {
   if (cycles_since_sort >= 1 && n_pushed > 0) {
     float push_ms = 0;
     GP_CUDA(cudaEventElapsedTime(&push_ms, ev_push[0].get(), ev_push[1].get()));
-    if (cycles_since_sort == 1) {
-      base_ms_per_particle = double(push_ms) / double(n_pushed);
+    const double per = double(push_ms) / double(n_pushed);
+    if (lean_push && tune_step < 0 && cycles_since_sort == 1) tune_step = 0;  // the first sort is behind us
+    if (lean_push && tune_step >= 0 && tune_step < 4) {
+      tune_ms[tune_per == kern::kPushChunkPer ? 0 : 1] += per;
+      if (++tune_step == 4) {
+        chunk_per = tune_ms[0] <= tune_ms[1] ? kern::kPushChunkPer : kern::kPushChunkPer / 2;
+        // the drift since the sort restarts from the kept variant's mean
+        base_ms_per_particle = 0.5 * std::min(tune_ms[0], tune_ms[1]);
+        excess_ms = 0;
+      }
+    } else if (cycles_since_sort == 1) {
+      base_ms_per_particle = per;
       excess_ms = 0;
     } else {
       excess_ms += double(push_ms) - base_ms_per_particle * double(n_pushed);
