@@ -280,8 +280,9 @@ def ensemble_leg(members, steps, threads, seed=0):
     chunks = {}
     for m in ens.members:
         for sp in range(2):
-            per = m.push_stats(sp)[5]
-            chunks[str(per)] = chunks.get(str(per), 0) + 1
+            st = m.push_stats(sp)
+            key = f"{st[5]}{'' if st[6] else ' no tables'}"
+            chunks[key] = chunks.get(key, 0) + 1
     ens.close()
     del ens
     batched = 0.5 * (n0 + n1) * steps / (ms / 1e3)
@@ -298,7 +299,7 @@ def ensemble_leg(members, steps, threads, seed=0):
     return {"members": members, "threads": threads, "steps": steps, "particles": n1,
             "ppc_range": [16, 256], "pushes_per_s": batched, "sequential_pushes_per_s": sequential,
             "speedup": batched / sequential, "ms": ms, "wall_s": el,
-            "autotuned_particles_per_chunk": chunks,
+            "autotuned_push_variants": chunks,
             "timing": "CUDA events on the member streams: earliest member start to latest member end; "
                       "sequential: the sum of each member's device-timed cycles run alone"}
 

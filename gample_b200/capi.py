@@ -81,7 +81,7 @@ EXPORTS = {
     "gp_particle_count": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_uint32)]),
     "gp_particle_push_stats": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_uint32)]),
     "gp_particle_sort": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
-    "gp_particle_set_push_chunk": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
+    "gp_particle_set_push_variant": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int]),
     "gp_particle_download": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_uint32, C.POINTER(C.c_uint32)]),
     "gp_particle_upload": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_uint32]),
     "gp_particle_download_raw": (C.c_int, [C.c_void_p, C.c_int] + [C.c_void_p] * 6 +
@@ -319,16 +319,17 @@ class Sim:
         re-sort, 2 staged record scatter)."""
         check(lib().gp_particle_sort(self.h, s, path))
 
-    def set_push_chunk(self, s, particles):
-        """Fix the push's particles per chunk (2048 or 1024), or 0 for the autotuner."""
-        check(lib().gp_particle_set_push_chunk(self.h, s, particles))
+    def set_push_variant(self, s, particles, tables=True):
+        """Fix the push's particles per chunk (2048 or 1024) and gather tables
+        (order 3), or particles=0 for the autotuner."""
+        check(lib().gp_particle_set_push_variant(self.h, s, particles, 1 if tables else 0))
 
     def push_stats(self, s):
         """(particles pushed without a window, chunks staged by bulk tensor
         copies, staging waits that timed out, chunks gathering through the
         per-cell tables, chunks depositing into lane-private windows,
-        particles per chunk) of the last push."""
-        out = (C.c_uint32 * 6)()
+        particles per chunk, gather tables allowed) of the last push."""
+        out = (C.c_uint32 * 7)()
         check(lib().gp_particle_push_stats(self.h, s, out))
         return tuple(out)
 

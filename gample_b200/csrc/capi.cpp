@@ -663,23 +663,24 @@ gp_status gp_particle_sort(gp_sim* sim, int s, int path) {
     return GP_OK;
   });
 }
-gp_status gp_particle_set_push_chunk(gp_sim* sim, int s, int particles) {
+gp_status gp_particle_set_push_variant(gp_sim* sim, int s, int particles, int tables) {
   return guarded([&] {
     auto* p = species(sim, s);
+    constexpr int per = gample::kern::kPushChunkPer;
     if (particles == 0) {
       p->tune_step = -1;
-      p->tune_ms[0] = p->tune_ms[1] = 0;
-      p->chunk_per = gample::kern::kPushChunkPer;
-    } else if (particles == 256 * gample::kern::kPushChunkPer || particles == 128 * gample::kern::kPushChunkPer) {
-      p->tune_step = 4;  // no tuning
-      p->chunk_per = particles / 256;
+      for (double& t : p->tune_ms) t = 0;
+      p->push_variant = {per, 1};
+    } else if (particles == 256 * per || particles == 128 * per) {
+      p->tune_step = 1 << 20;  // no tuning
+      p->push_variant = {particles / 256, tables ? 1 : 0};
     } else {
       throw std::invalid_argument("particles per chunk must be 0, 1024 or 2048");
     }
     return GP_OK;
   });
 }
-gp_status gp_particle_push_stats(gp_sim* sim, int s, uint32_t out[6]) {
+gp_status gp_particle_push_stats(gp_sim* sim, int s, uint32_t out[7]) {
   return guarded([&] {
     if (!out) throw std::invalid_argument("null output");
     const auto c = species(sim, s)->counters();
@@ -688,7 +689,8 @@ gp_status gp_particle_push_stats(gp_sim* sim, int s, uint32_t out[6]) {
     out[2] = c.err;
     out[3] = c.n_tab;
     out[4] = c.n_priv;
-    out[5] = uint32_t(species(sim, s)->tune_per) * 256u;
+    out[5] = uint32_t(species(sim, s)->tune_used.per) * 256u;
+    out[6] = uint32_t(species(sim, s)->tune_used.tables);
     return GP_OK;
   });
 }

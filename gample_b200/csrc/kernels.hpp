@@ -66,6 +66,7 @@ struct PushConsts {
   float scale;                           // deposit weight q w / (dx dy)
   float bz_uniform;                      // used when the Bz gather is skipped
   double ke_half_m, ke_w;                // 0.5 * m and w for the kinetic energy
+  int no_tables;                         // 1: order 3 gathers from the staged windows, not the tables
 };
 
 // Per-species charge / current accumulators (reference extents). Fast mode:

@@ -604,7 +604,7 @@ __device__ __forceinline__ Window chunk_setup(const GridDims& g, const ParticleA
                                             uint32_t n, uint32_t base, int tid, int lane, int wid, float* sEx,
                                             float* sEy, float* sBz, int* sDep, int (*s_red)[kThreads / 32],
                                             Window& s_w, int32_t& s_ref, const FieldMaps* tm = nullptr,
-                                            uint32_t bar = 0, SpeciesCounters* cnt = nullptr) {
+                                            uint32_t bar = 0, SpeciesCounters* cnt = nullptr, bool tables = true) {
   using DL = DepositLayout<ORDER, CUR, DET>;
   constexpr bool kTab = PUSH && BZU && ORDER == 3 && !DET && !CUR;
   const int ngb = g.ngb;
@@ -687,7 +687,7 @@ __device__ __forceinline__ Window chunk_setup(const GridDims& g, const ParticleA
       w.xrs = tab_row_stride(w.tbw + 1);
       w.yrs = tab_row_stride(w.tbw);
       w.yoff = w.tbh * w.xrs;
-      w.tab = (kTab && w.use && w.yoff + (w.tbh + 1) * w.yrs <= kTabFloat4) ? 1 : 0;
+      w.tab = (kTab && tables && w.use && w.yoff + (w.tbh + 1) * w.yrs <= kTabFloat4) ? 1 : 0;
       w.sx0 = w.gx0;
       w.sy0 = w.gy0;
       w.sstr = w.gw;
@@ -1183,7 +1183,7 @@ __global__ void __launch_bounds__(kThreads, ORDER == 5 ? 2 : 4)
   const uint32_t bar = smem_u32(&s_bar);
   if (tid == 0) mbar_init1(bar);  // ordered before the copies by phase A's barriers
   const Window w = chunk_setup<ORDER, true, true, false, false, true, true, PER>(
-      g, p, f, n, base, tid, lane, wid, sEx, sEy, nullptr, sDep, s_red, s_w, s_ref, &tm, bar, cnt);
+      g, p, f, n, base, tid, lane, wid, sEx, sEy, nullptr, sDep, s_red, s_w, s_ref, &tm, bar, cnt, c.no_tables == 0);
   WinPtrs sw;
   sw.rho = static_cast<uint32_t>(__cvta_generic_to_shared(sDep + ((lane / DL::kN2) % DL::kCopies) * DL::kStride));
 

@@ -215,15 +215,25 @@ class Particle {
   double base_ms_per_particle = 0, excess_ms = 0;
   uint32_t n_pushed = 0;
   TimingEvent ev_push[2], ev_sort[2];
-  // Autotuner of the atomic-mode push in a uniform Bz: the four pushes after
-  // the first sort alternate the chunk size (2048, 1024, 1024, 2048
-  // particles per CTA, so that the drift of the push time since the sort
-  // weighs on both alike); the faster per particle is kept for the run.
-  int chunk_per = kern::kPushChunkPer;
-  int tune_step = -1;  // -1: not started, 0..3: tuning, 4: done
-  int tune_per = kern::kPushChunkPer;
-  double tune_ms[2] = {0, 0};  // summed ms per particle: [0] 2048, [1] 1024
-  bool lean_push = false;      // the last push ran the tunable kernel
+  // Autotuner of the atomic-mode push in a uniform Bz. Variants: 2048 or
+  // 1024 particles per chunk, and for order 3 the gather tables on or off.
+  // The pushes after the first sort run each variant twice, in mirrored
+  // order (A B C D D C B A; A B B A for two variants) so that the drift of
+  // the push time since the sort weighs on all alike; the fastest per
+  // particle is kept for the run.
+  struct PushVariant {
+    int per;     // particles per thread (chunk = 256 per)
+    int tables;  // 0: gather tables off
+  };
+  PushVariant push_variant{kern::kPushChunkPer, 1};
+  int tune_step = -1;  // -1: not started, then 0 .. 2 * variants - 1, then done
+  PushVariant tune_used{kern::kPushChunkPer, 1};
+  double tune_ms[4] = {0, 0, 0, 0};  // summed ms per particle per variant
+  bool lean_push = false;            // the last push ran the tunable kernel
+  int tune_variants() const { return order == 3 ? 4 : 2; }
+  PushVariant tune_variant(int v) const {
+    return PushVariant{v % 2 == 0 ? kern::kPushChunkPer : kern::kPushChunkPer / 2, v < 2 ? 1 : 0};
+  }
 
   std::string pName;
   int index = 0;

@@ -210,15 +210,14 @@ void Particle::update(double dt, EMField& fld, bool fused_deposit) {
   kern::FieldPtrs f{fld.Ex.get(), fld.Ey.get(), fld.Bz.get()};
   const kern::FieldMaps* maps = fld.pushMaps();
   lean_push = fused_deposit && !fld.det && !fld.current && fld.bz_uniform;
-  tune_per = chunk_per;
-  if (lean_push && tune_step >= 0 && tune_step < 4) {
-    constexpr int kABBA[4] = {kern::kPushChunkPer, kern::kPushChunkPer / 2, kern::kPushChunkPer / 2,
-                              kern::kPushChunkPer};
-    tune_per = kABBA[tune_step];
-  }
+  const int nv = tune_variants();
+  tune_used = push_variant;
+  if (lean_push && tune_step >= 0 && tune_step < 2 * nv)  // mirrored order: 0 1 .. nv-1 nv-1 .. 1 0
+    tune_used = tune_variant(tune_step < nv ? tune_step : 2 * nv - 1 - tune_step);
+  c.no_tables = tune_used.tables ? 0 : 1;
   GP_CUDA(cudaEventRecord(ev_push[0].get(), stream));
   kern::push(order, boris, fused_deposit, fld.det, fld.current, fld.bz_uniform, fld.dims, arrays(), f, c,
-             fld.targets(index), cnt.get(), dead_bits.get(), n_bound, stream, maps, tune_per);
+             fld.targets(index), cnt.get(), dead_bits.get(), n_bound, stream, maps, tune_used.per);
   GP_CUDA(cudaEventRecord(ev_push[1].get(), stream));
   n_pushed = n_bound;
   cost_policy = !fld.det;
@@ -262,13 +261,17 @@ FlowStats Particle::reduce(XmlLogger* logger) {
     float push_ms = 0;
     GP_CUDA(cudaEventElapsedTime(&push_ms, ev_push[0].get(), ev_push[1].get()));
     const double per = double(push_ms) / double(n_pushed);
+    const int nv = tune_variants();
     if (lean_push && tune_step < 0 && cycles_since_sort == 1) tune_step = 0;  // the first sort is behind us
-    if (lean_push && tune_step >= 0 && tune_step < 4) {
-      tune_ms[tune_per == kern::kPushChunkPer ? 0 : 1] += per;
-      if (++tune_step == 4) {
-        chunk_per = tune_ms[0] <= tune_ms[1] ? kern::kPushChunkPer : kern::kPushChunkPer / 2;
+    if (lean_push && tune_step >= 0 && tune_step < 2 * nv) {
+      tune_ms[tune_step < nv ? tune_step : 2 * nv - 1 - tune_step] += per;
+      if (++tune_step == 2 * nv) {
+        int best = 0;
+        for (int v = 1; v < nv; ++v)
+          if (tune_ms[v] < tune_ms[best]) best = v;
+        push_variant = tune_variant(best);
         // the drift since the sort restarts from the kept variant's mean
-        base_ms_per_particle = 0.5 * std::min(tune_ms[0], tune_ms[1]);
+        base_ms_per_particle = 0.5 * tune_ms[best];
         excess_ms = 0;
       }
     } else if (cycles_since_sort == 1) {

@@ -152,13 +152,15 @@ gp_status gp_particle_sort(gp_sim* sim, int s, int path);
  * staged by bulk tensor copies, out[2] staging waits that timed out, out[3]
  * chunks that gathered through the per-cell tables, out[4] chunks that
  * deposited into lane-private windows, out[5] particles per chunk (2048 or
- * 1024, the autotuner's choice once it has run; out[1], out[3], out[4],
- * out[5]: the atomic mode's push in a uniform Bz). */
-gp_status gp_particle_push_stats(gp_sim* sim, int s, uint32_t out[6]);
-/* Particles per chunk of species s's atomic-mode push in a uniform Bz
- * (build addition): 2048 or 1024 fixes it, 0 lets the autotuner pick (the
- * default: the four pushes after the first sort time both). */
-gp_status gp_particle_set_push_chunk(gp_sim* sim, int s, int particles);
+ * 1024), out[6] 1 if order 3 could use the gather tables (out[1], out[3] to
+ * out[6]: the atomic mode's push in a uniform Bz). */
+gp_status gp_particle_push_stats(gp_sim* sim, int s, uint32_t out[7]);
+/* Variant of species s's atomic-mode push in a uniform Bz (build
+ * addition): particles per chunk 2048 or 1024 and, for order 3, gather
+ * tables on (tables != 0) or off fix it; particles = 0 lets the autotuner
+ * pick (the default: the pushes after the first sort time each variant
+ * twice, in mirrored order, and keep the fastest). */
+gp_status gp_particle_set_push_variant(gp_sim* sim, int s, int particles, int tables);
 /* particleBuffer contents as 24-byte records (src/Particle.h:69-78) */
 gp_status gp_particle_download(gp_sim* sim, int s, gp_particle_state* host, uint32_t capacity, uint32_t* n);
 gp_status gp_particle_upload(gp_sim* sim, int s, const gp_particle_state* host, uint32_t n);

@@ -147,16 +147,17 @@ def test_push_matches_oracle(gpu, order, boris, bcs):
 
 
 @pytest.mark.parametrize("order", [1, 3, 5])
-@pytest.mark.parametrize("fused,chunk", [(False, 0), (True, 2048), (True, 1024)])
-def test_push_dense_sorted_uniform_bz_matches_oracle(gpu, order, fused, chunk):
+@pytest.mark.parametrize("fused,chunk,tables", [(False, 0, True), (True, 2048, True), (True, 1024, True),
+                                                (True, 2048, False)])
+def test_push_dense_sorted_uniform_bz_matches_oracle(gpu, order, fused, chunk, tables):
     """256 particles per cell in tile order with a uniform Bz: chunks cover a
     few cells, so order 3 gathers through the per-cell polynomial tables and
     orders 1 and 5 through the staged windows; rough random Ex, Ey make every
     tap matter. fused: push with the fused deposit of the atomic mode, the
     lean kernel, whose Ex / Ey tiles arrive by bulk tensor copies from the
     pitched copies of the uploaded fields (refreshed after the upload), with
-    both chunk sizes the autotuner chooses from. Same tolerances as the push
-    test above."""
+    the variants the autotuner chooses from (chunk sizes, tables on and off).
+    Same tolerances as the push test above."""
     ngx = ngy = 16
     cond = condition(ngx=ngx, ngy=ngy, order=order, ppc=256, xbc="periodic", ybc="periodic", bz_tesla=0.05,
                      dt=2e-11)
@@ -176,11 +177,12 @@ def test_push_dense_sorted_uniform_bz_matches_oracle(gpu, order, fused, chunk):
         ora.push(s)
         if fused:
             sim.reset_charge()
-            sim.set_push_chunk(s, chunk)
+            sim.set_push_variant(s, chunk, tables)
         sim.update(s, cond["ParamForTimeIntegration"]["TimeStep"], fused_deposit=fused)
         if fused:
-            slow, staged, timeouts, _, _, per = sim.push_stats(s)
-            assert staged > 0 and timeouts == 0 and per == chunk, (slow, staged, timeouts, per)
+            slow, staged, timeouts, tab, _, per, allowed = sim.push_stats(s)
+            assert staged > 0 and timeouts == 0 and per == chunk and allowed == tables, (slow, staged, timeouts, per)
+            assert (tab > 0) == (tables and order == 3), tab
         g, r = sim.particles(s), ora.particles(s, f32=True)
         assert np.array_equal(g["piflag"], r["piflag"])
         vth = np.sqrt(np.mean(r["vx"].astype(np.float64) ** 2))
