@@ -463,10 +463,12 @@ def run_b200(args):
     achieved = BYTES_PER_PUSH * particles_per_launch / (push_ms_per_launch / 1e3) / 1e9
     tr = load_traffic()
     traffic = tr["dram_bytes_per_particle"] * particles_per_launch if tr else None
+    variants = [sim.push_stats(sp)[5:7] for sp in range(2)]
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": traffic, "peak_kind": peak_kind, "kernel": "k_push (gather+Boris+BC+fused deposit)",
                 "algorithmic_bytes_per_particle": BYTES_PER_PUSH,
-                "phase_ms_per_step": {k: v / prof_cycles for k, v in ph.items()}}
+                "phase_ms_per_step": {k: v / prof_cycles for k, v in ph.items()},
+                "push_variant": [{"particles_per_chunk": v[0], "tables": bool(v[1])} for v in variants]}
     steady = steady_state_leg(sim, args.steady_warm, args.steady_steps) if args.steady_steps > 0 else None
     sim.close()
     del sim

@@ -205,10 +205,11 @@ class Particle {
   // that base to excess_ms; the species sorts again once excess_ms reaches
   // the time of its last periodic sort (for a push time that grows linearly
   // with the cycles since the sort this is the interval of least total time).
-  // Until a periodic sort has been timed, and in the deterministic mode,
-  // whose cadence must not depend on timings, the species sorts once the
-  // particles pushed outside their chunk's window exceed those of the first
-  // push after the last sort by 2 % of the live count.
+  // Until a periodic sort has been timed its cost is estimated from the
+  // particle count. In the deterministic mode, whose cadence must not depend
+  // on timings, the species sorts once the particles pushed outside their
+  // chunk's window exceed those of the first push after the last sort by 2 %
+  // of the live count.
   bool cost_policy = true;
   bool sort_timed = false, sort_pending_timing = false;
   float last_sort_ms = 0;
@@ -220,7 +221,8 @@ class Particle {
   // The pushes after the first sort run each variant twice, in mirrored
   // order (A B C D D C B A; A B B A for two variants) so that the drift of
   // the push time since the sort weighs on all alike; the fastest per
-  // particle is kept for the run.
+  // particle is kept for the run. Species with kTuneBelowPpc or more
+  // particles per cell keep the defaults (2048, tables) untuned.
   struct PushVariant {
     int per;     // particles per thread (chunk = 256 per)
     int tables;  // 0: gather tables off
@@ -231,6 +233,7 @@ class Particle {
   double tune_ms[4] = {0, 0, 0, 0};  // summed ms per particle per variant
   bool lean_push = false;            // the last push ran the tunable kernel
   int tune_variants() const { return order == 3 ? 4 : 2; }
+  static constexpr double kTuneBelowPpc = 128.0;  // tune species with fewer particles per cell
   PushVariant tune_variant(int v) const {
     return PushVariant{v % 2 == 0 ? kern::kPushChunkPer : kern::kPushChunkPer / 2, v < 2 ? 1 : 0};
   }

@@ -262,7 +262,11 @@ FlowStats Particle::reduce(XmlLogger* logger) {
     GP_CUDA(cudaEventElapsedTime(&push_ms, ev_push[0].get(), ev_push[1].get()));
     const double per = double(push_ms) / double(n_pushed);
     const int nv = tune_variants();
-    if (lean_push && tune_step < 0 && cycles_since_sort == 1) tune_step = 0;  // the first sort is behind us
+    // the first sort is behind us: tune, unless the cells are so full that the
+    // defaults are known to win (at 256 particles per cell the 1024-particle
+    // chunks and the table-less order-3 gather were measured slower)
+    if (lean_push && tune_step < 0 && cycles_since_sort == 1)
+      tune_step = double(n_pushed) < kTuneBelowPpc * double(dims_.ngx) * double(dims_.ngy) ? 0 : (1 << 20);
     if (lean_push && tune_step >= 0 && tune_step < 2 * nv) {
       tune_ms[tune_step < nv ? tune_step : 2 * nv - 1 - tune_step] += per;
       if (++tune_step == 2 * nv) {
@@ -281,12 +285,16 @@ FlowStats Particle::reduce(XmlLogger* logger) {
       excess_ms += double(push_ms) - base_ms_per_particle * double(n_pushed);
     }
   }
-  if (sort_interval > 0)
+  if (sort_interval > 0) {
     needs_sort = needs_sort || cycles_since_sort >= sort_interval;
-  else if (cost_policy && sort_timed)
-    needs_sort = needs_sort || excess_ms >= double(last_sort_ms);
-  else
+  } else if (cost_policy) {
+    // before the first periodic sort has been timed: its cost estimated
+    // from the particle count (30 ps per particle, measured: 22-34 ps)
+    const double sort_ms = sort_timed ? double(last_sort_ms) : std::max(0.02, 3e-8 * double(c.n));
+    needs_sort = needs_sort || excess_ms >= sort_ms;
+  } else {
     needs_sort = needs_sort || double(c.n_slow) > double(slow_after_sort) + 0.02 * double(c.n);
+  }
   if (logger && logger->on()) {
     // src/Particle.mm:990-1001
     std::map<std::string, std::string> data = {
