@@ -108,7 +108,7 @@ def load_tensor_peak():
 
 def load_traffic():
     """DRAM bytes per pushed particle of the push kernel, from the committed ncu
-    summary (a 64-ppc capture of the same kernel; traffic scales with the
+    summary (a 128-ppc capture of the same kernel; traffic scales with the
     particles processed)."""
     try:
         with open(os.path.join(ROOT, "profiles", "push_es512_o3.md")) as f:
@@ -422,6 +422,8 @@ def run_b200(args):
 
     ppc = args.ppc
     cond = workload(ppc=ppc)
+    if args.sort_interval:
+        cond["ParamForComputing"]["SortInterval"] = args.sort_interval
     sim = capi.Sim(cond)
     sim.initialize()
     if args.warmup:
@@ -554,6 +556,28 @@ def run_b200(args):
     return 0
 
 
+def run_resort_probe(args):
+    """The periodic re-sort's input, for profiling its kernels: the workload
+    at --ppc run --resort-probe cycles without sorting (drifted particles,
+    refilled holes, re-injected strays), then one block-local re-sort of the
+    electrons, timed with CUDA events around the call's stream work."""
+    from gample_b200 import capi
+    cond = workload(ppc=args.ppc)
+    cond["ParamForComputing"]["SortInterval"] = 1 << 30
+    sim = capi.Sim(cond)
+    sim.initialize()
+    sim.run(args.resort_probe)
+    slow = sim.push_stats(0)[0]
+    sim.synchronize()
+    t0 = time.perf_counter()
+    sim.sort(0, 1)
+    ms = 1e3 * (time.perf_counter() - t0)
+    print(json.dumps({"resort_probe": args.resort_probe, "ppc": args.ppc, "electrons": sim.count(0),
+                      "pushed_outside_window_before": slow, "sort_ms_host": ms}), flush=True)
+    sim.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -576,9 +600,16 @@ def main():
     ap.add_argument("--steady-warm", type=int, default=200, help="cycles run before the steady-state leg")
     ap.add_argument("--steady-steps", type=int, default=50, help="cycles timed in the steady-state leg (0: skip)")
     ap.add_argument("--quick", action="store_true", help="timed cycles only (for profiler runs)")
+    ap.add_argument("--sort-interval", type=int, default=0,
+                    help="SortInterval of the main run (0: adaptive; profiler runs fix it so that the cadence does "
+                         "not follow the profiler's timings)")
+    ap.add_argument("--resort-probe", type=int, default=0,
+                    help="profiler case: K cycles without sorting, then one re-sort of the electrons")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.resort_probe > 0:
+        return run_resort_probe(args)
     return run_b200(args)
 
 
