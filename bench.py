@@ -79,6 +79,59 @@ def workload(ppc=256, ngx=512, ngy=512, steps=1000, log_output=0):
     }
 
 
+def workload_periodic(ngx, order, ppc, dt_wpe, bz_gauss=0.0, darwin=False, drift_frac=0.0, steps=200):
+    """Doubly periodic ES (or Darwin) PIC of electrons and Xe+ with the bench
+    workload's plasma: Te = 10 eV, Ti = 0.1 eV, n = 5e10 cm^-3, dx = 0.5
+    Debye length, uniform Bz, Poisson to 1e-8. drift_frac adds an electron
+    drift along y of drift_frac * vte * sin(2 pi x / Lx) (the build-added
+    SinusoidalDriftVel loader key)."""
+    c = workload(ppc=ppc, ngx=ngx, ngy=ngx, steps=steps)
+    n = 5e10
+    wpe = math.sqrt(4 * math.pi * n * EC ** 2 / ME)
+    c["ParamForTimeIntegration"]["TimeStep"] = dt_wpe / wpe
+    c["SourceForParticle"] = []
+    c["BoundaryConditionForParticle"] = [{"RegionName": r, "BCType": "periodic"} for r in ("Xmin", "Xmax", "Ymin", "Ymax")]
+    c["BoundaryConditionForField"] = [{"RegionName": r, "BCType": "periodic"} for r in ("Xmin", "Xmax", "Ymin", "Ymax")]
+    c["ParamForField"]["WeightingOrder"] = order
+    c["ParamForField"]["AmplitudeOfB"] = [0.0, 0.0, bz_gauss]
+    c["ParamForComputing"]["MaxiterForPoisson"] = 200
+    if darwin:
+        c["FlagForEquation"]["EMField"] = 2
+        c["ParamForField"]["FlagForCurDens"] = 1
+    if drift_frac:
+        vte = math.sqrt(2 * KB * 10.0 * EV_K / ME)
+        c["ParamForParticle"][0]["SinusoidalDriftVel"] = [0.0, drift_frac * vte, 0.0]
+    return c
+
+
+def config_legs(steps):
+    """Device-timed cycles of the other reference configurations: config 1
+    (128^2 doubly periodic, CIC, 64 ppc, w_ce / w_pe = 0.5, dt w_pe = 0.1)
+    and config 3 (1024^2 doubly periodic Darwin, order 5, 100 ppc, electron
+    drift 0.1 vte sin(2 pi x / L) along y, dt w_pe = 0.05, Bz 0)."""
+    from gample_b200 import capi
+    n = 5e10
+    wpe = math.sqrt(4 * math.pi * n * EC ** 2 / ME)
+    out = {}
+    cases = {"config1_es128_o1_64ppc": (workload_periodic(128, 1, 64, 0.1, bz_gauss=0.5 * wpe * ME * 2.99792458e10 / EC),
+                                        3, 4 * steps),
+             "config3_darwin1024_o5_100ppc": (workload_periodic(1024, 5, 100, 0.05, darwin=True, drift_frac=0.1),
+                                              2, steps)}
+    for name, (cond, warm, k) in cases.items():
+        sim = capi.Sim(cond)
+        sim.initialize()
+        sim.run(warm)
+        n0 = sim.count(0) + sim.count(1)
+        ms = sim.time_cycles(k)
+        n1 = sim.count(0) + sim.count(1)
+        st = sim.last_solve()
+        out[name] = {"steps": k, "ms_per_step": ms / k, "particles": n1,
+                     "pushes_per_s": 0.5 * (n0 + n1) * k / (ms / 1e3),
+                     "poisson_iterations": st.iterations, "poisson_rel_residual": st.error}
+        sim.close()
+    return out
+
+
 def config_block(ppc):
     return {"workload": f"es-pic 512x512, order 3, Dirichlet-x absorbing + periodic-y, {ppc} ppc/species "
                         f"({2 * ppc * 512 * 512 / 1e6:.1f} M particles), Bz 0.02 T, dt*wpe 0.05, "
@@ -521,6 +574,7 @@ def run_b200(args):
                "h2d_bytes_per_step": int(h2d / args.steps), "d2h_bytes_per_step": int(d2h / args.steps + diag),
                "wall_s": el, "includes": "sim create + restart upload + initial solve + K logged cycles + "
                                          "final download"}
+    configs = config_legs(args.config_steps) if rank == 0 and args.config_steps > 0 else None
     ensemble = None
     if rank == 0 and args.ensemble > 0:
         ensemble = ensemble_leg(args.ensemble, args.ensemble_steps, args.ensemble_threads)
@@ -547,6 +601,7 @@ def run_b200(args):
                           "(roofline and poisson blocks); max over ranks",
                 "poisson": poisson_block(iters_last, unknowns, roofline["phase_ms_per_step"]["solve"], peak),
                 "steady_state": steady,
+                "other_configs": configs,
                 "learned_warm_start": learned,
                 "ensemble": ensemble}
         print(json.dumps(line), flush=True)
@@ -594,6 +649,8 @@ def main():
     ap.add_argument("--learned-samples", type=int, default=25, help="residual samples banked per seed")
     ap.add_argument("--learned-lr", type=float, default=1e-3)
     ap.add_argument("--learned-eval", type=int, default=20)
+    ap.add_argument("--config-steps", type=int, default=5,
+                    help="timed cycles of the config-3 leg (config 1: 4x; 0: skip both)")
     ap.add_argument("--ensemble", type=int, default=64, help="members of the batched-ensemble leg (0: skip)")
     ap.add_argument("--ensemble-steps", type=int, default=10)
     ap.add_argument("--ensemble-threads", type=int, default=16)

@@ -114,11 +114,18 @@ __global__ void k_generate(uint32_t addn, GenParams prm, RNGState* states, Parti
                     __fmul_rn(__fmul_rn(Ly, sqrtf(-logf(rz))), cosf(__fmul_rn(2.0f * PIf, ry))));
     }
     float rv1 = rand01(rng), rv2 = rand01(rng);
-    const float evx = maxwell(prm.ele_genU[0], prm.ele_vth, rv1, rv2, false);
-    const float evy = maxwell(prm.ele_genU[1], prm.ele_vth, rv1, rv2, true);
+    float evx = maxwell(prm.ele_genU[0], prm.ele_vth, rv1, rv2, false);
+    float evy = maxwell(prm.ele_genU[1], prm.ele_vth, rv1, rv2, true);
     rv1 = rand01(rng);
     rv2 = rand01(rng);
-    const float evz = maxwell(prm.ele_genU[2], prm.ele_vth, rv1, rv2, false);
+    float evz = maxwell(prm.ele_genU[2], prm.ele_vth, rv1, rv2, false);
+    float ph = 0.0f;  // drift profile of the build-added sinusoidal drift
+    if (prm.sin_on) ph = sinf(__fmul_rn(2.0f * PIf, __fdiv_rn(__fsub_rn(x, prm.Xmin), Lx)));
+    if (prm.sin_on) {
+      evx = __fmaf_rn(prm.ele_sinU[0], ph, evx);
+      evy = __fmaf_rn(prm.ele_sinU[1], ph, evy);
+      evz = __fmaf_rn(prm.ele_sinU[2], ph, evz);
+    }
     int ix = 0, iy = 0;
     float ox = 0.0f, oy = 0.0f;
     const bool ok = to_cell(x, prm.dx, prm.ngb, ix, ox) & to_cell(y, prm.dy, prm.ngb, iy, oy);
@@ -126,11 +133,16 @@ __global__ void k_generate(uint32_t addn, GenParams prm, RNGState* states, Parti
     if (GT != 3 && with_ion) {
       rv1 = rand01(rng);
       rv2 = rand01(rng);
-      const float ivx = maxwell(prm.ion_genU[0], prm.ion_vth, rv1, rv2, false);
-      const float ivy = maxwell(prm.ion_genU[1], prm.ion_vth, rv1, rv2, true);
+      float ivx = maxwell(prm.ion_genU[0], prm.ion_vth, rv1, rv2, false);
+      float ivy = maxwell(prm.ion_genU[1], prm.ion_vth, rv1, rv2, true);
       rv1 = rand01(rng);
       rv2 = rand01(rng);
-      const float ivz = maxwell(prm.ion_genU[2], prm.ion_vth, rv1, rv2, false);
+      float ivz = maxwell(prm.ion_genU[2], prm.ion_vth, rv1, rv2, false);
+      if (prm.sin_on) {
+        ivx = __fmaf_rn(prm.ion_sinU[0], ph, ivx);
+        ivy = __fmaf_rn(prm.ion_sinU[1], ph, ivy);
+        ivz = __fmaf_rn(prm.ion_sinU[2], ph, ivz);
+      }
       store(ion, ibase + id, ok, ix, ox, iy, oy, ivx, ivy, ivz);
     }
     states[id] = rng;

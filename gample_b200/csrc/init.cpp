@@ -222,6 +222,7 @@ Init Init::parseString(const std::string& text) {
       p.genY = s.vec("InitialPosY", {-1, -1});
       p.genU = s.vec("InitialVel", {0, 0, 0});
       p.genT = s.f("InitialTemp", 0) * phys::eVtoK;
+      p.sinU = s.vec("SinusoidalDriftVel", {0, 0, 0});
       I.paramForParticle.push_back(p);
     }
   }
@@ -377,7 +378,7 @@ std::string Init::dump() const {
     o << (i ? "," : "") << "{\"pName\":" << q(p.pName) << ",\"pNum\":" << p.pNum << ",\"q\":" << num(p.q)
       << ",\"m\":" << num(p.m) << ",\"w\":" << num(p.w) << ",\"genType\":" << q(p.genType)
       << ",\"genX\":" << vec(p.genX) << ",\"genY\":" << vec(p.genY) << ",\"genU\":" << vec(p.genU)
-      << ",\"genT\":" << num(p.genT) << "}";
+      << ",\"genT\":" << num(p.genT) << ",\"sinU\":" << vec(p.sinU) << "}";
   }
   o << "],\"sources\":[";
   for (size_t i = 0; i < particleSources.size(); ++i) {

@@ -70,6 +70,9 @@ struct ParamForParticle {  // src/Init.h:38-52
   std::string genType;
   std::vector<double> genX, genY, genU;
   double genT = 0;  // K
+  // build addition: amplitude (cm/s, per component) of a drift added to the
+  // initial load's velocities with the profile sin(2 pi (x - Xmin) / Lx)
+  std::vector<double> sinU;
 };
 
 struct BoundaryConditionForParticle {  // src/Init.h:54-57

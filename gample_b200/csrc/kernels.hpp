@@ -180,6 +180,10 @@ struct GenParams {  // src/Collision.h:22-38
   float ion_genU[3];
   float ion_vth;
   float dx, dy, ngb;
+  // build addition (initial load only): drift amplitudes with the profile
+  // sin(2 pi (x - Xmin) / Lx); sin_on = 0 leaves the reference's velocities
+  float ele_sinU[3], ion_sinU[3];
+  int sin_on;
 };
 // Kernel artificialIonization (src/Collision.mm:63-174): addn particles
 // (electron, and a colocated ion unless genType == 3) appended after the

@@ -74,15 +74,18 @@ void Collision::loadInitial(std::vector<Particle*>& ptcls) {
     const float vth = float(std::sqrt(2 * phys::kb * pp[s].genT / pp[s].m));
     if (pp[s].pName == "electron") {
       for (int d = 0; d < 3; ++d) prm.ele_genU[d] = comp(pp[s].genU, d);
+      for (int d = 0; d < 3; ++d) prm.ele_sinU[d] = comp(pp[s].sinU, d);
       prm.ele_vth = vth;
     } else {
       for (int d = 0; d < 3; ++d) prm.ion_genU[d] = comp(pp[s].genU, d);
+      for (int d = 0; d < 3; ++d) prm.ion_sinU[d] = comp(pp[s].sinU, d);
       prm.ion_vth = vth;
     }
   }
   prm.dx = float(fp.dx);
   prm.dy = float(fp.dy);
   prm.ngb = float(fp.ngb);
+  for (int d = 0; d < 3; ++d) prm.sin_on |= (prm.ele_sinU[d] != 0.0f || prm.ion_sinU[d] != 0.0f) ? 1 : 0;
   if (addn > ele->pNumMax || addn > ion->pNumMax) throw ConfigError("pNum > pNumMax in the initial load");
   ensure_states(addn);
   ele->setPNum(0);

@@ -253,7 +253,11 @@ FlowStats Particle::reduce(XmlLogger* logger) {
   // counters() synchronised the stream: this cycle's push (and a sort before
   // it) have completed
   if (sort_pending_timing) {
-    GP_CUDA(cudaEventElapsedTime(&last_sort_ms, ev_sort[0].get(), ev_sort[1].get()));
+    // a one-off slow sort (a busy GPU) must not stretch the cadence for
+    // long: each timing may at most double the previous one
+    float t = 0;
+    GP_CUDA(cudaEventElapsedTime(&t, ev_sort[0].get(), ev_sort[1].get()));
+    last_sort_ms = sort_timed ? std::min(t, 2.0f * last_sort_ms) : t;
     sort_timed = true;
     sort_pending_timing = false;
   }
@@ -281,6 +285,8 @@ FlowStats Particle::reduce(XmlLogger* logger) {
     } else if (cycles_since_sort == 1) {
       base_ms_per_particle = per;
       excess_ms = 0;
+    } else if (per < base_ms_per_particle) {
+      base_ms_per_particle = per;  // a slow first push must not hide the drift
     } else {
       excess_ms += double(push_ms) - base_ms_per_particle * double(n_pushed);
     }
