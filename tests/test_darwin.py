@@ -43,10 +43,17 @@ def test_oracle_darwin_splits_a_gradient_current():
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("case", ["periodic", "neumann"])
+@pytest.mark.parametrize("case", ["periodic", "neumann", "config3"])
 def test_darwin_matches_oracle(gpu, case):
+    """config3: the Darwin configuration's set-up at 128^2 (doubly periodic,
+    order 5, electron drift 0.1 v_te sin(2 pi x / L) along y from the
+    build-added SinusoidalDriftVel key: a transverse current)."""
     if case == "periodic":
         cond = condition(ngx=32, ngy=32, order=1, ppc=16, em=2, cur_dens=1, vxe=4e7)
+    elif case == "config3":
+        cond = condition(ngx=128, ngy=128, order=5, ppc=16, em=2, cur_dens=1)
+        vte = np.sqrt(2 * 1.3806503e-16 * 10.0 * 11604.0 / 9.10938188e-28)
+        cond["ParamForParticle"][0]["SinusoidalDriftVel"] = [0.0, 0.1 * vte, 0.0]
     else:
         cond = condition(ngx=33, ngy=24, order=3, ppc=16, xbc="Dirichlet", ybc="periodic", em=2, cur_dens=1,
                          vxe=4e7)
@@ -59,7 +66,7 @@ def test_darwin_matches_oracle(gpu, case):
     assert all(e <= 1e-8 for e in err), err
     dx = np.float32(cond["ParamForField"]["GridSizeOfX"])
     dy = np.float32(cond["ParamForField"]["GridSizeOfY"])
-    o = L.Darwin(sim.ngx, sim.ngy, sim.ngb, case == "periodic", True, dx, dy)
+    o = L.Darwin(sim.ngx, sim.ngy, sim.ngb, case != "neumann", True, dx, dy)
     # the GPU's A_last after two cycles is unknown to the oracle: compare the
     # potentials, and the fields of the next solve from a shared A_last
     want = o.solve(jx, jy, dt)
