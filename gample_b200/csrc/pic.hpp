@@ -182,6 +182,12 @@ class Particle {
   // deposited into fld (next step's charge).
   void update(double dt, EMField& fld, bool fused_deposit);
   FlowStats reduce(XmlLogger* logger);                   // src/Particle.mm:893-1002
+  // reduce() in two halves: the compaction and the read-back of the counters
+  // enqueued, then (after the caller has synchronised the stream) the flow
+  // statistics, the sort decision and the log, so that one synchronisation
+  // serves all species of a cycle.
+  void reduceLaunch();
+  FlowStats reduceFinish(XmlLogger* logger);
   void integrateChargeDensity(EMField& fld, bool injected_only = false);  // src/Particle.mm:1004-1130
 
   uint32_t pNum();  // synchronous read of the device count

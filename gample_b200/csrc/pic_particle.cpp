@@ -225,8 +225,19 @@ void Particle::update(double dt, EMField& fld, bool fused_deposit) {
 }
 
 FlowStats Particle::reduce(XmlLogger* logger) {
+  reduceLaunch();
+  GP_CUDA(cudaStreamSynchronize(stream));
+  return reduceFinish(logger);
+}
+
+void Particle::reduceLaunch() {
   kern::compact(arrays(), cnt.get(), dead_bits.get(), scratch.get(), n_bound, stream);
-  kern::SpeciesCounters c = counters();
+  GP_CUDA(cudaMemcpyAsync(host_cnt_.get(), cnt.get(), sizeof(kern::SpeciesCounters), cudaMemcpyDeviceToHost,
+                          stream));
+}
+
+FlowStats Particle::reduceFinish(XmlLogger* logger) {
+  const kern::SpeciesCounters c = host_cnt_[0];
   if (c.err)
     throw std::runtime_error("push: " + std::to_string(c.err) +
                              " field-staging waits timed out (tiles were loaded per thread instead)");
@@ -250,7 +261,7 @@ FlowStats Particle::reduce(XmlLogger* logger) {
   // injection) exceed those of the first push after the last sort by 2% of
   // the live count.
   if (cycles_since_sort == 1) slow_after_sort = c.n_slow;
-  // counters() synchronised the stream: this cycle's push (and a sort before
+  // the caller synchronised the stream: this cycle's push (and a sort before
   // it) have completed
   if (sort_pending_timing) {
     // a one-off slow sort (a busy GPU) must not stretch the cadence for

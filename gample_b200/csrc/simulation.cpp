@@ -227,9 +227,16 @@ void Simulation::cycle() {
     mark(PH_PUSH, false);
     mark(PH_REDUCE, true);
     tic("reduce_" + ptrs[s]->pName);
-    last_flow[s] = ptrs[s]->reduce(logger.get());
+    ptrs[s]->reduceLaunch();
     toc();
     mark(PH_REDUCE, false);
+  }
+  // one synchronisation for the counters of every species: the next
+  // species' push was enqueued behind this one's compaction, not after a
+  // host round trip
+  GP_CUDA(cudaStreamSynchronize(stream));
+  for (size_t s = 0; s < ptrs.size(); ++s) {
+    last_flow[s] = ptrs[s]->reduceFinish(logger.get());
     if (file_output && T.ParticleOutput != 0 && cycle_no % T.ParticleOutput == 0)  // :211-214
       outputPhaseSpace(cycle_no, *ptrs[s], init);
     if (field_out) {  // :215-220
