@@ -374,15 +374,27 @@ __device__ __forceinline__ void deposit_one(const GridDims& g, const Window& w, 
 // rotation is needed, and every node offset is a compile-time immediate of
 // the row stride kPW. Lane L of every warp shares copy L, so a copy receives
 // at most kPer * (kThreads / 32) contributions per node.
-// The products rn(wx * 2^kQBits * wy) are those of the shared layout, so the
-// integer window sums are the same.
+// Each contribution is the integer nearest to wx * 2^kQBits * wy, formed by one
+// rounding: fma(rx, ry, 1.5 * 2^23) holds it in the low mantissa bits (the
+// ulp at 1.5 * 2^23 is 1, and 0 <= rx * ry <= 2^22), read off by subtracting
+// the bits of 1.5 * 2^23. Two x-neighbouring nodes share one packed FFMA2;
+// this replaces a multiply and a float-to-integer conversion per node (the
+// shared layout's rn(rn(wx * 2^kQBits * wy)) differs from it only at ties).
 template <int N, int K = 0>
 __device__ __forceinline__ void priv_add(uint32_t a0, const float (&rx)[N], const float (&ry)[N]) {
+  static_assert(N % 2 == 0, "nodes are taken in x pairs");
+  constexpr float kMagic = 12582912.0f;    // 1.5 * 2^23
+  constexpr int kMagicBits = 0x4B400000;  // its bit pattern
   if constexpr (K < N * N) {
+    const float2 r = __ffma2_rn(make_float2(rx[K % N], rx[K % N + 1]), make_float2(ry[K / N], ry[K / N]),
+                                make_float2(kMagic, kMagic));
     asm volatile("red.shared.add.s32 [%0+%1], %2;" ::"r"(a0), "n"(4 * (K % N + (K / N) * kPW)),
-                 "r"(__float2int_rn(__fmul_rn(rx[K % N], ry[K / N])))
+                 "r"(__float_as_int(r.x) - kMagicBits)
                  : "memory");
-    priv_add<N, K + 1>(a0, rx, ry);
+    asm volatile("red.shared.add.s32 [%0+%1], %2;" ::"r"(a0), "n"(4 * (K % N + 1 + (K / N) * kPW)),
+                 "r"(__float_as_int(r.y) - kMagicBits)
+                 : "memory");
+    priv_add<N, K + 2>(a0, rx, ry);
   }
 }
 
