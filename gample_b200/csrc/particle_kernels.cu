@@ -268,6 +268,16 @@ __device__ __forceinline__ void wadd_s(uint32_t addr, long long q) {
   asm volatile("red.shared.add.s32 [%0+%1], %2;" ::"r"(addr), "n"(LO), "r"(int(q & 0xFFFFF)) : "memory");
 }
 
+// The integers nearest to x0 * y and x1 * y (0 <= x * y <= 2^22), each
+// rounded once: fma(x, y, 1.5 * 2^23) holds it in the low mantissa bits (the
+// ulp at 1.5 * 2^23 is 1), read off by subtracting the bits of 1.5 * 2^23.
+__device__ __forceinline__ int2 fixed_pair(float x0, float x1, float y) {
+  constexpr float kMagic = 12582912.0f;    // 1.5 * 2^23
+  constexpr int kMagicBits = 0x4B400000;  // its bit pattern
+  const float2 r = __ffma2_rn(make_float2(x0, x1), make_float2(y, y), make_float2(kMagic, kMagic));
+  return make_int2(__float_as_int(r.x) - kMagicBits, __float_as_int(r.y) - kMagicBits);
+}
+
 // The window path accumulates quant40(w) for rho and quant40(w * v / c) for
 // the currents (rn(w * 2^kQBits) for rho in the single-word layout); the
 // caller sends a particle with |v| >= c (|w v / c| could exceed 1) to the
@@ -310,12 +320,15 @@ __device__ __forceinline__ void deposit_one(const GridDims& g, const Window& w, 
     for (int a = 0; a < N; ++a)
 #pragma unroll
       for (int b = 0; b < N; ++b) {
-        if constexpr (DL::kSingle)
-          asm volatile("red.shared.add.s32 [%0], %1;" ::"r"(arho + col[b] + row[a]),
-                       "r"(__float2int_rn(__fmul_rn(rxn[b], ryn[a])))
-                       : "memory");
-        else
+        if constexpr (DL::kSingle) {
+          if (b % 2 == 0) {  // rounded once, two nodes per packed FFMA2 (as in priv_add)
+            const int2 q = fixed_pair(rxn[b], rxn[b + 1], ryn[a]);
+            asm volatile("red.shared.add.s32 [%0], %1;" ::"r"(arho + col[b] + row[a]), "r"(q.x) : "memory");
+            asm volatile("red.shared.add.s32 [%0], %1;" ::"r"(arho + col[b + 1] + row[a]), "r"(q.y) : "memory");
+          }
+        } else {
           wadd_s<0, kA>(arho + col[b] + row[a], __float2ll_rn(__fmul_rn(rxn[b], ryn[a])));
+        }
       }
     if constexpr (CUR) {
       float rxh[N], ryh[N];
@@ -374,25 +387,17 @@ __device__ __forceinline__ void deposit_one(const GridDims& g, const Window& w, 
 // rotation is needed, and every node offset is a compile-time immediate of
 // the row stride kPW. Lane L of every warp shares copy L, so a copy receives
 // at most kPer * (kThreads / 32) contributions per node.
-// Each contribution is the integer nearest to wx * 2^kQBits * wy, formed by one
-// rounding: fma(rx, ry, 1.5 * 2^23) holds it in the low mantissa bits (the
-// ulp at 1.5 * 2^23 is 1, and 0 <= rx * ry <= 2^22), read off by subtracting
-// the bits of 1.5 * 2^23. Two x-neighbouring nodes share one packed FFMA2;
-// this replaces a multiply and a float-to-integer conversion per node (the
-// shared layout's rn(rn(wx * 2^kQBits * wy)) differs from it only at ties).
+// Each contribution is the integer nearest to wx * 2^kQBits * wy, rounded once
+// (fixed_pair: two x-neighbouring nodes per packed FFMA2), as in the rotated
+// shared layout, so the integer window sums of the two layouts are the same.
 template <int N, int K = 0>
 __device__ __forceinline__ void priv_add(uint32_t a0, const float (&rx)[N], const float (&ry)[N]) {
   static_assert(N % 2 == 0, "nodes are taken in x pairs");
-  constexpr float kMagic = 12582912.0f;    // 1.5 * 2^23
-  constexpr int kMagicBits = 0x4B400000;  // its bit pattern
   if constexpr (K < N * N) {
-    const float2 r = __ffma2_rn(make_float2(rx[K % N], rx[K % N + 1]), make_float2(ry[K / N], ry[K / N]),
-                                make_float2(kMagic, kMagic));
-    asm volatile("red.shared.add.s32 [%0+%1], %2;" ::"r"(a0), "n"(4 * (K % N + (K / N) * kPW)),
-                 "r"(__float_as_int(r.x) - kMagicBits)
+    const int2 q = fixed_pair(rx[K % N], rx[K % N + 1], ry[K / N]);
+    asm volatile("red.shared.add.s32 [%0+%1], %2;" ::"r"(a0), "n"(4 * (K % N + (K / N) * kPW)), "r"(q.x)
                  : "memory");
-    asm volatile("red.shared.add.s32 [%0+%1], %2;" ::"r"(a0), "n"(4 * (K % N + 1 + (K / N) * kPW)),
-                 "r"(__float_as_int(r.y) - kMagicBits)
+    asm volatile("red.shared.add.s32 [%0+%1], %2;" ::"r"(a0), "n"(4 * (K % N + 1 + (K / N) * kPW)), "r"(q.y)
                  : "memory");
     priv_add<N, K + 2>(a0, rx, ry);
   }
