@@ -243,7 +243,7 @@ def poisson_block(vcycles, unknowns, solve_ms, peak):
             "ms_per_vcycle_incl_cg": ms_cycle, "algorithmic_bytes_per_vcycle": per_cycle,
             "achieved_gbs": achieved, "frac_of_hbm": achieved / peak if achieved else None,
             "note": "latency-bound: 9 dependent launches per CG iteration at 512^2 (one CUDA graph), "
-                    "levels <= 4096 points in one CTA"}
+                    "levels <= 1024 points in one CTA"}
 
 
 NET_SPECS_RESIDUAL = [(1, 16, 0), (16, 16, 0), (16, 32, 1), (32, 32, 1), (32, 64, 2), (64, 64, 2), (64, 64, 3),

@@ -11,12 +11,16 @@ namespace gample {
 
 namespace {
 
-constexpr int kSmallPoints = 4096;       // levels at or below run in one CTA
+// Measured at 512^2 (solve ms per step): tiles of 32 x 16 points with 256
+// threads 0.498, 32 x 8 with 512 threads 0.455 (16 x 16: 0.454, 64 x 8: 0.500,
+// 32 x 8 with 1024 threads 0.472); the single-CTA kernel from 4096 points
+// down 0.455, from 1024 points (63 x 64 in tiles) 0.438, from 256 points 0.596.
+constexpr int kSmallPoints = 1024;       // levels at or below run in one CTA
 constexpr int kMaxSmallLevels = 16;
 constexpr int kDenseMax = 64;            // coarsest levels up to this size use a precomputed inverse
-constexpr int TX = 32, TY = 16, HALO = 4;  // smoother tile and halo (4 half-sweeps)
+constexpr int TX = 32, TY = 8, HALO = 4;  // smoother tile and halo (4 half-sweeps)
 constexpr int SW = TX + 2 * HALO, SH = TY + 2 * HALO;
-constexpr int kSmoothThreads = 256;
+constexpr int kSmoothThreads = 512;
 constexpr int kSmallThreads = 1024;
 
 // state words (FP64): see multigrid.hpp
