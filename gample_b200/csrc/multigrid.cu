@@ -29,6 +29,13 @@ enum {
   S_ZAZ, S_RZ, S_RPO, S_PAZ, S_COUNT
 };
 
+// Partial sums of the flexible-CG passes: each block adds its sums into one
+// of kSlots slots per quantity (block index mod kSlots), so at most
+// 1/kSlots of the blocks queue on one address in the L2; the consumer sums
+// the kSlots slots of a quantity with one warp.
+constexpr int kSlots = 32;
+enum { A_ZQ = 0, A_ZAZ, A_RZ, A_RPO, A_PAZ, A_SUM, A_SUM2, A_COUNT };
+
 // Boundary treatment of a direction: Dirichlet (values outside are zero),
 // periodic (wrap) or Neumann (mirror about the end node, i.e. the doubled
 // off-diagonal of the Darwin operator, src/EMField.mm:527-560).
@@ -39,6 +46,31 @@ struct LevelDesc {
   int bx, by;
   float cx, cy, cd;
 };
+
+// Programmatic dependent launch: every kernel of the solve is launched with
+// programmatic stream serialisation, so the next kernel's launch overlaps
+// the tail of the one before it. Each such kernel waits for its predecessor
+// (griddepcontrol.wait: the previous grid complete and its memory visible)
+// before it touches global memory, and releases its own dependent once it is
+// running.
+__device__ __forceinline__ void grid_dependency_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void grid_dependents_launch() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
+template <typename... KArgs, typename... Args>
+void launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, Args... args) {
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  GP_CUDA(cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...));
+  GP_LAUNCH_CHECK();
+}
 
 __host__ __device__ __forceinline__ bool wrap(int& i, int n, int b) {
   if (i >= 0 && i < n) return true;
@@ -141,9 +173,12 @@ __device__ __forceinline__ float restrict_at(const float* u, const float* f, con
 }
 
 // ---------------------------------------------------------------- outer loop
-__global__ void k_init(double* st, const double* sums_b) {
+__global__ void k_init(double* st, const double* sums_b, double* acc) {
+  grid_dependency_wait();
+  grid_dependents_launch();
   const double nb = sqrt(sums_b[1] > 0 ? sums_b[1] : 0.0);
   for (int i = 0; i < S_COUNT; ++i) st[i] = 0.0;
+  for (int i = 0; i < A_COUNT * kSlots; ++i) acc[i] = 0.0;
   st[S_NORMB] = nb;
   // AMGCL clears x and returns for a zero right-hand side
   if (nb < DBL_EPSILON) {
@@ -153,6 +188,8 @@ __global__ void k_init(double* st, const double* sums_b) {
 }
 
 __global__ void k_clear_if_zero_rhs(double* x, int n, const double* st) {
+  grid_dependency_wait();
+  grid_dependents_launch();
   if (st[S_DONE] != 2.0) return;
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) x[k] = 0.0;
 }
@@ -199,6 +236,8 @@ __device__ __forceinline__ double res_weight(const kern::PoissonLayout& L, int i
 // accumulates sum w r, sum r^2.
 __global__ void k_residual64(const double* __restrict__ x, const double* __restrict__ b, kern::PoissonLayout L,
                              float* __restrict__ r32, double* __restrict__ r64, double* st) {
+  grid_dependency_wait();
+  grid_dependents_launch();
   __shared__ double sh[32];
   if (st[S_DONE] != 0.0) return;
   const int mx = L.nkx + 1, my = L.nky + 1, n = mx * my;
@@ -261,7 +300,9 @@ __device__ __forceinline__ void block_sums(double (&v)[N], double (*sh)[32]) {
 // updates p, q, x and r in place. Pass A: the dot products.
 __global__ void k_fcg_dots(const float* __restrict__ z, const double* __restrict__ q_old,
                            const double* __restrict__ p_old, const double* __restrict__ r, kern::PoissonLayout L,
-                           double* st) {
+                           const double* st, double* acc) {
+  grid_dependency_wait();
+  grid_dependents_launch();
   __shared__ double sh[5][32];
   if (st[S_DONE] != 0.0) return;
   const bool first = st[S_ITER] == 1.0;  // p_old, q_old hold nothing of this solve yet
@@ -282,13 +323,19 @@ __global__ void k_fcg_dots(const float* __restrict__ z, const double* __restrict
   }
   block_sums<5>(v, sh);
   if (threadIdx.x == 0) {
-    atomicAdd(st + S_ZQ, v[0]);
-    atomicAdd(st + S_ZAZ, v[1]);
-    atomicAdd(st + S_RZ, v[2]);
-    atomicAdd(st + S_RPO, v[3]);
-    atomicAdd(st + S_PAZ, v[4]);
+    const int slot = blockIdx.x % kSlots;
+#pragma unroll
+    for (int a = 0; a < 5; ++a) atomicAdd(acc + (A_ZQ + a) * kSlots + slot, v[a]);
   }
   (void)my;
+}
+
+// Sum of the kSlots slots of quantity a, by one full warp (every lane gets it).
+__device__ __forceinline__ double slot_sum(const double* acc, int a) {
+  double t = __ldcg(acc + a * kSlots + (threadIdx.x & 31));
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+  return t;
 }
 
 // The convergence test of one iteration (AMGCL's ||r|| / ||b|| <= tol or
@@ -310,52 +357,99 @@ __device__ __forceinline__ void fcg_check(double* st, double pq, double tol, int
 }
 
 // Pass B: p = z + beta p_old, q = A z + beta q_old (both in place), x +=
-// alpha p, r -= alpha q with float(r) for the next V-cycle; the last block
-// to finish runs the convergence test (the counter returns to zero).
-__global__ void k_fcg_step(const float* __restrict__ z, double* __restrict__ p, double* __restrict__ q,
-                           double* __restrict__ x, double* __restrict__ r, float* __restrict__ r32,
-                           kern::PoissonLayout L, double* st, unsigned* ctr, double tol, int maxiter, double wsum) {
+// alpha p, r -= alpha q with float(r) for the next V-cycle, kStepPoints
+// points per thread. A thread loads its points' operands first, then the
+// scalars from the slots of pass A (every block sums them in the same order,
+// so all blocks use the same alpha and beta), so the two loads overlap. The
+// last block to finish runs the convergence test, clears the slots for the
+// next iteration and returns the counter to zero.
+constexpr int kStepThreads = 256, kStepPoints = 2;
+__global__ void __launch_bounds__(kStepThreads, 4) k_fcg_step(const float* __restrict__ z, double* __restrict__ p,
+                                                           double* __restrict__ q, double* __restrict__ x,
+                                                           double* __restrict__ r, float* __restrict__ r32,
+                                                           kern::PoissonLayout L, double* st, double* acc,
+                                                           unsigned* ctr, double tol, int maxiter, double wsum) {
   __shared__ double sh[2][32];
+  __shared__ double s_sc[5];
   __shared__ bool s_last;
+  grid_dependency_wait();
   if (st[S_DONE] != 0.0) return;  // uniform: every block sees the previous kernel's value
-  const bool first = st[S_ITER] == 1.0;
-  const double beta = first ? 0.0 : -st[S_ZQ] / st[S_PQOLD];
-  const double pq = st[S_ZAZ] + (first ? 0.0 : beta * (st[S_ZQ] + st[S_PAZ]) + beta * beta * st[S_PQOLD]);
-  const double rp = st[S_RZ] + (first ? 0.0 : beta * st[S_RPO]);
-  const double alpha = pq != 0.0 ? rp / pq : 0.0;
+  grid_dependents_launch();
   const int mx = L.nkx + 1, my = L.nky + 1, n = mx * my;
+  double az[kStepPoints], zk[kStepPoints], pk[kStepPoints], qk[kStepPoints], xk[kStepPoints], rk[kStepPoints];
+#pragma unroll
+  for (int t = 0; t < kStepPoints; ++t) {
+    const int k = (blockIdx.x * kStepPoints + t) * kStepThreads + threadIdx.x;
+    az[t] = zk[t] = pk[t] = qk[t] = xk[t] = rk[t] = 0.0;
+    if (k < n) {
+      az[t] = apply_A(L, k, k % mx, k / mx, mx, [&](int u) { return double(z[u]); });
+      zk[t] = double(z[k]);
+      pk[t] = p[k];
+      qk[t] = q[k];
+      xk[t] = x[k];
+      rk[t] = r[k];
+    }
+  }
+  if (threadIdx.x < 32) {
+#pragma unroll
+    for (int a = 0; a < 5; ++a) {
+      const double t = slot_sum(acc, A_ZQ + a);
+      if (threadIdx.x == 0) s_sc[a] = t;
+    }
+  }
+  __syncthreads();
+  const bool first = st[S_ITER] == 1.0;
+  const double zq = s_sc[0], zaz = s_sc[1], rz = s_sc[2], rpo = s_sc[3], paz = s_sc[4];
+  const double pq_old = st[S_PQOLD];
+  const double beta = first ? 0.0 : -zq / pq_old;
+  const double pq = zaz + (first ? 0.0 : beta * (zq + paz) + beta * beta * pq_old);
+  const double rp = rz + (first ? 0.0 : beta * rpo);
+  const double alpha = pq != 0.0 ? rp / pq : 0.0;
   double v[2] = {0.0, 0.0};  // sum w r, sum r^2
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-    const int i = k % mx, j = k / mx;
-    const double az = apply_A(L, k, i, j, mx, [&](int t) { return double(z[t]); });
-    const double pk = first ? double(z[k]) : double(z[k]) + beta * p[k];
-    const double qk = first ? az : az + beta * q[k];
-    p[k] = pk;
-    q[k] = qk;
-    x[k] += alpha * pk;
-    const double rk = r[k] - alpha * qk;
-    r[k] = rk;
-    r32[k] = float(rk);
-    v[0] += res_weight(L, i, j, mx, my) * rk;
-    v[1] += rk * rk;
+#pragma unroll
+  for (int t = 0; t < kStepPoints; ++t) {
+    const int k = (blockIdx.x * kStepPoints + t) * kStepThreads + threadIdx.x;
+    if (k < n) {
+      const double pn = first ? zk[t] : zk[t] + beta * pk[t];
+      const double qn = first ? az[t] : az[t] + beta * qk[t];
+      p[k] = pn;
+      q[k] = qn;
+      x[k] = xk[t] + alpha * pn;
+      const double rn = rk[t] - alpha * qn;
+      r[k] = rn;
+      r32[k] = float(rn);
+      v[0] += res_weight(L, k % mx, k / mx, mx, my) * rn;
+      v[1] += rn * rn;
+    }
   }
   block_sums<2>(v, sh);
   if (threadIdx.x == 0) {
-    atomicAdd(st + S_SUM, v[0]);
-    atomicAdd(st + S_SUM2, v[1]);
+    const int slot = blockIdx.x % kSlots;
+    atomicAdd(acc + A_SUM * kSlots + slot, v[0]);
+    atomicAdd(acc + A_SUM2 * kSlots + slot, v[1]);
     __threadfence();
     s_last = atomicAdd(ctr, 1u) == gridDim.x - 1;
   }
   __syncthreads();
-  if (s_last && threadIdx.x == 0) {
+  if (s_last && threadIdx.x < 32) {
     __threadfence();
-    *ctr = 0u;
-    fcg_check(st, pq, tol, maxiter, wsum);
+    const double sum = slot_sum(acc, A_SUM), sum2 = slot_sum(acc, A_SUM2);
+    __syncwarp();
+#pragma unroll
+    for (int a = 0; a < A_COUNT; ++a) acc[a * kSlots + threadIdx.x] = 0.0;
+    if (threadIdx.x == 0) {
+      *ctr = 0u;
+      st[S_SUM] = sum;
+      st[S_SUM2] = sum2;
+      fcg_check(st, pq, tol, maxiter, wsum);
+    }
   }
 }
 
 // Convergence test (one thread): AMGCL's ||r|| / ||b|| <= tol or maxiter.
 __global__ void k_check(double* st, double tol, int maxiter, double wsum) {
+  grid_dependency_wait();
+  grid_dependents_launch();
   st[S_PQOLD] = st[S_PQ];
   st[S_PQ] = 0.0;
   st[S_RP] = 0.0;
@@ -375,6 +469,8 @@ __global__ void k_check(double* st, double tol, int maxiter, double wsum) {
 }
 
 __global__ void k_sub_mean32(float* f, int n, const double* st) {
+  grid_dependency_wait();
+  grid_dependents_launch();
   if (st[S_DONE] != 0.0) return;
   const float m = float(st[S_MEAN]);
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) f[k] -= m;
@@ -404,22 +500,56 @@ __global__ void k_sub_mean64(double* x, int n, const double* sum) {
 // Halo of the tile kernels: 4 points for the four half-sweeps; the
 // pre-smoother keeps 2 more so that the residual on the tile's interior plus
 // one ring (for the full-weighting restriction) is still exact.
-template <bool PRE>
+// The finest level's post-smoother with DOTS also forms pass A of the
+// flexible-CG iteration (z.q_old, z.Az, r.z, r.p_old, p_old.Az) on its tile:
+// it keeps one more halo ring, so z is exact on the interior plus one ring
+// and A z (FP64, the CSR coefficients of the fine system) is formed in
+// shared memory.
+template <bool PRE, bool DOTS = false>
 constexpr int tile_halo() {
-  return PRE ? HALO + 2 : HALO;
+  return PRE ? HALO + 2 : DOTS ? HALO + 1 : HALO;
 }
 
-template <bool PRE>
-__global__ void __launch_bounds__(kSmoothThreads) k_smooth_tile(const float* u, float* u_out,
+// Operands of pass A for the fused post-smoother of the finest level.
+struct FcgDotsIn {
+  const double* r;
+  const double* p_old;
+  const double* q_old;
+  double* acc;
+  double cx, cy, cd;
+};
+
+template <bool PRE, bool DOTS = false>
+__global__ void __launch_bounds__(kSmoothThreads, 4) k_smooth_tile(const float* u, float* u_out,
                                                                 const float* __restrict__ f, LevelDesc d,
                                                                 const float* __restrict__ uc, LevelDesc c,
-                                                                const double* st, float* __restrict__ fc_out) {
-  constexpr int HL = tile_halo<PRE>(), W = TX + 2 * HL, H = TY + 2 * HL;
+                                                                const double* st, float* __restrict__ fc_out,
+                                                                FcgDotsIn fd = FcgDotsIn{}) {
+  grid_dependency_wait();
+  grid_dependents_launch();
+  static_assert(!(PRE && DOTS), "pass A belongs to the post-smoother");
+  constexpr int HL = tile_halo<PRE, DOTS>(), W = TX + 2 * HL, H = TY + 2 * HL;
   __shared__ float su[H][W + 1];
   __shared__ float sf[H][W + 1];
   __shared__ unsigned char s_in[H][W];
   if (st[S_DONE] != 0.0) return;
   const int x0 = blockIdx.x * TX - HL, y0 = blockIdx.y * TY - HL;
+  // pass A operands of this thread's interior point, loaded before the sweeps
+  static_assert(TX * TY <= kSmoothThreads, "one interior point per thread");
+  double d_r = 0.0, d_p = 0.0, d_q = 0.0;
+  bool d_first = false;
+  if constexpr (DOTS) {
+    d_first = st[S_ITER] == 1.0;  // p_old, q_old hold nothing of this solve yet
+    const int gi = x0 + HL + int(threadIdx.x) % TX, gj = y0 + HL + int(threadIdx.x) / TX;
+    if (threadIdx.x < TX * TY && gi < d.mx && gj < d.my) {
+      const int k = gi + gj * d.mx;
+      d_r = fd.r[k];
+      if (!d_first) {
+        d_p = fd.p_old[k];
+        d_q = fd.q_old[k];
+      }
+    }
+  }
   for (int e = threadIdx.x; e < W * H; e += kSmoothThreads) {
     const int li = e % W, lj = e / W;
     int gi = x0 + li, gj = y0 + lj;
@@ -457,6 +587,31 @@ __global__ void __launch_bounds__(kSmoothThreads) k_smooth_tile(const float* u, 
     const int gi = x0 + li, gj = y0 + lj;
     if (gi < d.mx && gj < d.my) u_out[gi + gj * d.mx] = su[lj][li];
   }
+  if constexpr (DOTS) {
+    // Outside a Dirichlet wall su is 0 (the CSR row has no entry there);
+    // periodic and mirrored neighbours were loaded as such.
+    __shared__ double sh[5][32];
+    double v[5] = {0.0, 0.0, 0.0, 0.0, 0.0};  // z.q_old, z.Az, r.z, r.p_old, p_old.Az
+    const int li = HL + int(threadIdx.x) % TX, lj = HL + int(threadIdx.x) / TX;
+    if (threadIdx.x < TX * TY && x0 + li < d.mx && y0 + lj < d.my) {
+      const double zk = double(su[lj][li]);
+      const double az = fd.cd * zk + fd.cx * double(su[lj][li - 1]) + fd.cx * double(su[lj][li + 1]) +
+                        fd.cy * double(su[lj - 1][li]) + fd.cy * double(su[lj + 1][li]);
+      v[1] = zk * az;
+      v[2] = d_r * zk;
+      if (!d_first) {
+        v[0] = zk * d_q;
+        v[3] = d_r * d_p;
+        v[4] = d_p * az;
+      }
+    }
+    block_sums<5>(v, sh);
+    if (threadIdx.x == 0) {
+      const int slot = (blockIdx.x + blockIdx.y * gridDim.x) % kSlots;
+#pragma unroll
+      for (int a = 0; a < 5; ++a) atomicAdd(fd.acc + (A_ZQ + a) * kSlots + slot, v[a]);
+    }
+  }
   if constexpr (PRE) {
     if (!fc_out) return;
     // residual r = f - A u on the interior plus one ring (into sr), then the
@@ -490,6 +645,8 @@ __global__ void __launch_bounds__(kSmoothThreads) k_smooth_tile(const float* u, 
 
 __global__ void k_restrict(const float* __restrict__ u, const float* __restrict__ f, LevelDesc d, float* __restrict__ fc,
                            LevelDesc c, const double* st) {
+  grid_dependency_wait();
+  grid_dependents_launch();
   if (st[S_DONE] != 0.0) return;
   const int n = c.mx * c.my;
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
@@ -500,6 +657,8 @@ __global__ void k_restrict(const float* __restrict__ u, const float* __restrict_
 // does not fit the tile kernel.
 __global__ void k_smooth_generic(float* __restrict__ u, const float* __restrict__ f, LevelDesc d, int color,
                                  const double* st) {
+  grid_dependency_wait();
+  grid_dependents_launch();
   if (st[S_DONE] != 0.0) return;
   const int hx = (d.mx + 1) / 2;
   const int n = hx * d.my;
@@ -515,6 +674,8 @@ __global__ void k_smooth_generic(float* __restrict__ u, const float* __restrict_
 
 __global__ void k_prolong_generic(const float* __restrict__ uc, LevelDesc c, float* __restrict__ uf, LevelDesc d,
                                   const double* st) {
+  grid_dependency_wait();
+  grid_dependents_launch();
   if (st[S_DONE] != 0.0) return;
   const int n = d.mx * d.my;
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
@@ -522,6 +683,8 @@ __global__ void k_prolong_generic(const float* __restrict__ uc, LevelDesc c, flo
 }
 
 __global__ void k_zero32(float* u, int n, const double* st) {
+  grid_dependency_wait();
+  grid_dependents_launch();
   if (st[S_DONE] != 0.0) return;
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) u[k] = 0.0f;
 }
@@ -745,6 +908,8 @@ template <int BX, int BY>
 __global__ void __launch_bounds__(kSmallThreads) k_small_vcycle(SmallLevels S, const float* __restrict__ f_in,
                                                                 float* __restrict__ u_out, double* x, int nu_pre,
                                                                 int nu_post, const double* st) {
+  grid_dependency_wait();
+  grid_dependents_launch();
   extern __shared__ float sm[];
   __shared__ double sh[32];
   __shared__ double sval;
@@ -854,6 +1019,10 @@ bool tiled(const PoissonMG::Level& l) {
 bool tiled_pre(const PoissonMG::Level& l) {
   return tiled(l) && l.mx >= SW + 4 && l.my >= SH + 4;
 }
+// the finest post-smoother with the fused pass A of the flexible CG (one more ring)
+bool tiled_dots(const PoissonMG::Level& l) {
+  return tiled(l) && l.mx >= SW + 2 && l.my >= SH + 2;
+}
 int bc_code(const kern::PoissonLayout& L, bool x) {
   if (x ? L.periodic_x : L.periodic_y) return BC_PER;
   return L.fbc[x ? 0 : 2] == kern::FBC_NEUMANN_C ? BC_NEU : BC_DIR;
@@ -928,6 +1097,7 @@ PoissonMG::PoissonMG(const kern::PoissonLayout& L, int nu_pre, int nu_post)
   r64_.resize(size_t(n_), true);
   q_.resize(size_t(n_), true);
   ctr_.resize(1, true);
+  acc_.resize(size_t(A_COUNT) * kSlots, true);
   p_[0].resize(size_t(n_), true);
   // Dense inverse of the coarsest operator (FP64 Gauss-Jordan, stored FP32);
   // a singular one (no Dirichlet direction) is regularised as A + a 1 w^T
@@ -987,8 +1157,9 @@ PoissonMG::PoissonMG(const kern::PoissonLayout& L, int nu_pre, int nu_post)
   }
 }
 
-void PoissonMG::vcycle(cudaStream_t s) {
+bool PoissonMG::vcycle(cudaStream_t s, bool with_dots) {
   double* st = state_.get();
+  bool fused_dots = false;
   const int nl = int(lv_.size());
   // descent over the large levels
   for (int l = 0; l < ls_; ++l) {
@@ -997,27 +1168,19 @@ void PoissonMG::vcycle(cudaStream_t s) {
     const LevelDesc d = desc(a);
     if (tiled_pre(a) && nu_pre_ == 2) {  // smoothing, residual and restriction in one launch
       dim3 grid((a.mx + TX - 1) / TX, (a.my + TY - 1) / TY);
-      k_smooth_tile<true><<<grid, kSmoothThreads, 0, s>>>(a.u.get(), a.u.get(), a.f.get(), d, nullptr, desc(b), st,
-                                                           b.f.get());
-      GP_LAUNCH_CHECK();
+      launch_pdl(k_smooth_tile<true>, grid, dim3(kSmoothThreads), 0, s, a.u.get(), a.u.get(), a.f.get(), d, nullptr, desc(b), st, b.f.get(), FcgDotsIn{});
       continue;
     } else if (tiled(a) && nu_pre_ == 2) {
       dim3 grid((a.mx + TX - 1) / TX, (a.my + TY - 1) / TY);
-      k_smooth_tile<true><<<grid, kSmoothThreads, 0, s>>>(a.u.get(), a.u.get(), a.f.get(), d, nullptr, d, st,
-                                                           nullptr);
-      GP_LAUNCH_CHECK();
+      launch_pdl(k_smooth_tile<true>, grid, dim3(kSmoothThreads), 0, s, a.u.get(), a.u.get(), a.f.get(), d, nullptr, d, st, nullptr, FcgDotsIn{});
     } else {
-      k_zero32<<<blocks_for(a.mx * a.my), 256, 0, s>>>(a.u.get(), a.mx * a.my, st);
-      GP_LAUNCH_CHECK();
+      launch_pdl(k_zero32, dim3(blocks_for(a.mx * a.my)), dim3(256), 0, s, a.u.get(), a.mx * a.my, st);
       for (int it = 0; it < nu_pre_; ++it) {
-        k_smooth_generic<<<blocks_for((a.mx + 1) / 2 * a.my), 256, 0, s>>>(a.u.get(), a.f.get(), d, 0, st);
-        GP_LAUNCH_CHECK();
-        k_smooth_generic<<<blocks_for((a.mx + 1) / 2 * a.my), 256, 0, s>>>(a.u.get(), a.f.get(), d, 1, st);
-        GP_LAUNCH_CHECK();
+        launch_pdl(k_smooth_generic, dim3(blocks_for((a.mx + 1) / 2 * a.my)), dim3(256), 0, s, a.u.get(), a.f.get(), d, 0, st);
+        launch_pdl(k_smooth_generic, dim3(blocks_for((a.mx + 1) / 2 * a.my)), dim3(256), 0, s, a.u.get(), a.f.get(), d, 1, st);
       }
     }
-    k_restrict<<<blocks_for(b.mx * b.my), 256, 0, s>>>(a.u.get(), a.f.get(), d, b.f.get(), desc(b), st);
-    GP_LAUNCH_CHECK();
+    launch_pdl(k_restrict, dim3(blocks_for(b.mx * b.my)), dim3(256), 0, s, a.u.get(), a.f.get(), d, b.f.get(), desc(b), st);
   }
   // all small levels in one CTA
   {
@@ -1031,9 +1194,7 @@ void PoissonMG::vcycle(cudaStream_t s) {
     }
     S.cg_off = int(off);
     S.cinv = coarse_inv_.size() ? coarse_inv_.get() : nullptr;
-    small_kernel(bx_, by_)<<<1, kSmallThreads, small_smem_, s>>>(S, lv_[ls_].f.get(), lv_[ls_].u.get(), nullptr,
-                                                                 nu_pre_, nu_post_, st);
-    GP_LAUNCH_CHECK();
+    launch_pdl(small_kernel(bx_, by_), dim3(1), dim3(kSmallThreads), small_smem_, s, S, lv_[ls_].f.get(), lv_[ls_].u.get(), nullptr, nu_pre_, nu_post_, st);
     lv_[ls_].result_in_u2 = false;
   }
   // ascent
@@ -1041,24 +1202,26 @@ void PoissonMG::vcycle(cudaStream_t s) {
     Level& a = lv_[l];
     Level& b = lv_[l + 1];
     const LevelDesc d = desc(a);
-    if (tiled(a) && nu_post_ == 2) {
+    if (l == 0 && with_dots && tiled_dots(a) && nu_post_ == 2) {
       dim3 grid((a.mx + TX - 1) / TX, (a.my + TY - 1) / TY);
-      k_smooth_tile<false><<<grid, kSmoothThreads, 0, s>>>(a.u.get(), a.u2.get(), a.f.get(), d, result(l + 1), desc(b),
-                                                            st, nullptr);
-      GP_LAUNCH_CHECK();
+      const FcgDotsIn fd{r64_.get(), p_[0].get(), q_.get(), acc_.get(), L_.Cx, L_.Cy, L_.Cd};
+      launch_pdl(k_smooth_tile<false, true>, grid, dim3(kSmoothThreads), 0, s, a.u.get(), a.u2.get(), a.f.get(), d, result(l + 1), desc(b), st, nullptr, fd);
+      a.result_in_u2 = true;
+      fused_dots = true;
+    } else if (tiled(a) && nu_post_ == 2) {
+      dim3 grid((a.mx + TX - 1) / TX, (a.my + TY - 1) / TY);
+      launch_pdl(k_smooth_tile<false>, grid, dim3(kSmoothThreads), 0, s, a.u.get(), a.u2.get(), a.f.get(), d, result(l + 1), desc(b), st, nullptr, FcgDotsIn{});
       a.result_in_u2 = true;
     } else {
       a.result_in_u2 = false;
-      k_prolong_generic<<<blocks_for(a.mx * a.my), 256, 0, s>>>(result(l + 1), desc(b), a.u.get(), d, st);
-      GP_LAUNCH_CHECK();
+      launch_pdl(k_prolong_generic, dim3(blocks_for(a.mx * a.my)), dim3(256), 0, s, result(l + 1), desc(b), a.u.get(), d, st);
       for (int it = 0; it < nu_post_; ++it) {
-        k_smooth_generic<<<blocks_for((a.mx + 1) / 2 * a.my), 256, 0, s>>>(a.u.get(), a.f.get(), d, 1, st);
-        GP_LAUNCH_CHECK();
-        k_smooth_generic<<<blocks_for((a.mx + 1) / 2 * a.my), 256, 0, s>>>(a.u.get(), a.f.get(), d, 0, st);
-        GP_LAUNCH_CHECK();
+        launch_pdl(k_smooth_generic, dim3(blocks_for((a.mx + 1) / 2 * a.my)), dim3(256), 0, s, a.u.get(), a.f.get(), d, 1, st);
+        launch_pdl(k_smooth_generic, dim3(blocks_for((a.mx + 1) / 2 * a.my)), dim3(256), 0, s, a.u.get(), a.f.get(), d, 0, st);
       }
     }
   }
+  return fused_dots;
 }
 
 // One FCG iteration (parity: which direction buffer is current).
@@ -1067,16 +1230,17 @@ void PoissonMG::enqueue_iteration(int parity, double* x, double tol, int maxiter
   Level& f = lv_[0];
   const double wsum = singular_ ? wsum_ : double(n_);
   if (singular_) {
-    k_sub_mean32<<<blocks_for(n_), 256, 0, s>>>(f.f.get(), n_, st);
-    GP_LAUNCH_CHECK();
+    launch_pdl(k_sub_mean32, dim3(blocks_for(n_)), dim3(256), 0, s, f.f.get(), n_, st);
   }
-  vcycle(s);  // z = M r
+  const bool fused = vcycle(s, true);  // z = M r (and pass A, when fused)
   const float* z = result(0);
   (void)parity;  // p and q are updated in place
-  k_fcg_dots<<<reduce_blocks(n_), 256, 0, s>>>(z, q_.get(), p_[0].get(), r64_.get(), L_, st);
-  GP_LAUNCH_CHECK();
-  k_fcg_step<<<reduce_blocks(n_), 256, 0, s>>>(z, p_[0].get(), q_.get(), x, r64_.get(), f.f.get(), L_, st, ctr_.get(),
-                                               tol, maxiter, wsum);
+  if (!fused) {
+    launch_pdl(k_fcg_dots, dim3(reduce_blocks(n_)), dim3(256), 0, s, z, q_.get(), p_[0].get(), r64_.get(), L_, st, acc_.get());
+  }
+  launch_pdl(k_fcg_step, dim3((n_ + kStepThreads * kStepPoints - 1) / (kStepThreads * kStepPoints)),
+             dim3(kStepThreads), 0, s, z, p_[0].get(), q_.get(), x, r64_.get(),
+             f.f.get(), L_, st, acc_.get(), ctr_.get(), tol, maxiter, wsum);
   GP_LAUNCH_CHECK();
 }
 
@@ -1143,15 +1307,11 @@ MGResult PoissonMG::solve(const double* b, const double* sums_b, double* x, doub
   double* st = state_.get();
   Level& f = lv_[0];
   const bool singular = singular_;
-  k_init<<<1, 1, 0, s>>>(st, sums_b);
-  GP_LAUNCH_CHECK();
-  k_clear_if_zero_rhs<<<blocks_for(n_), 256, 0, s>>>(x, n_, st);
-  GP_LAUNCH_CHECK();
+  launch_pdl(k_init, dim3(1), dim3(1), 0, s, st, sums_b, acc_.get());
+  launch_pdl(k_clear_if_zero_rhs, dim3(blocks_for(n_)), dim3(256), 0, s, x, n_, st);
   const double wsum = singular_ ? wsum_ : double(n_);
-  k_residual64<<<reduce_blocks(n_), 256, 0, s>>>(x, b, L_, f.f.get(), r64_.get(), st);
-  GP_LAUNCH_CHECK();
-  k_check<<<1, 1, 0, s>>>(st, tol, maxiter, wsum);
-  GP_LAUNCH_CHECK();
+  launch_pdl(k_residual64, dim3(reduce_blocks(n_)), dim3(256), 0, s, x, b, L_, f.f.get(), r64_.get(), st);
+  launch_pdl(k_check, dim3(1), dim3(1), 0, s, st, tol, maxiter, wsum);
   // Batches of iterations without host synchronisation; every kernel returns
   // at once after convergence. The batch size follows the last solve. An
   // iteration is one CUDA graph launch when its graph could be captured.

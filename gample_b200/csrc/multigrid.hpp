@@ -72,7 +72,10 @@ class PoissonMG {
   int first_small_level() const { return ls_; }
 
  private:
-  void vcycle(cudaStream_t s);
+  // One V-cycle on the finest level's f; with_dots: the finest post-smoother
+  // also forms pass A of the flexible-CG iteration when its tiles allow
+  // (returns whether it did).
+  bool vcycle(cudaStream_t s, bool with_dots = false);
   void enqueue_iteration(int parity, double* x, double tol, int maxiter, cudaStream_t s);
   struct IterationGraphs {
     double* x = nullptr;
@@ -100,6 +103,7 @@ class PoissonMG {
   DeviceArray<double> r64_, q_;  // FP64 residual and A p of the flexible CG iteration
   DeviceArray<double> p_[1];      // search direction (updated in place)
   DeviceArray<unsigned> ctr_;     // blocks finished in the flexible-CG update (last one tests convergence)
+  DeviceArray<double> acc_;       // slotted partial sums of the flexible-CG passes (7 quantities x 32 slots)
   DeviceArray<float> coarse_inv_;  // dense inverse of the coarsest operator (small coarsest levels)
   DeviceArray<double> state_;   // [0] sum r [1] sum r^2 [2] ||b|| [3] rel res [4] done [5] iterations [6] mean r [7] initial rel res, then the flexible-CG scalars
   PinnedArray<double> host_;
