@@ -242,7 +242,8 @@ def poisson_block(vcycles, unknowns, solve_ms, peak):
     return {"vcycles_last_step": vcycles, "tolerance": 1e-8, "solve_ms_per_step": solve_ms,
             "ms_per_vcycle_incl_cg": ms_cycle, "algorithmic_bytes_per_vcycle": per_cycle,
             "achieved_gbs": achieved, "frac_of_hbm": achieved / peak if achieved else None,
-            "note": "latency-bound: 9 dependent launches per CG iteration at 512^2 (one CUDA graph), "
+            "note": "latency-bound: 10 dependent launches per CG iteration at 512^2 (one CUDA graph, "
+                    "programmatic dependent launches), CG dot products fused into the finest post-smoother, "
                     "levels <= 1024 points in one CTA"}
 
 
