@@ -7,6 +7,7 @@
 #include <cuda_runtime.h>
 
 #include "device.hpp"
+#include "pdl.cuh"
 #include "kernels.hpp"
 #include "pic_common.cuh"
 
@@ -52,6 +53,8 @@ __device__ __forceinline__ uint32_t live_mask_range(uint32_t w, uint32_t lo, uin
 // publish n_live; the counters' n becomes n_live.
 __global__ void __launch_bounds__(1024) k_compact_tail(SpeciesCounters* cnt, const uint32_t* bits,
                                                        uint32_t* scratch) {
+  grid_dependency_wait();
+  grid_dependents_launch();
   __shared__ uint32_t s_warp[32];
   __shared__ uint32_t s_base;
   const uint32_t n = cnt->n, nd = cnt->n_dead;
@@ -109,6 +112,8 @@ __device__ __forceinline__ uint32_t hole_mask(const uint32_t* bits, uint32_t w, 
 }
 
 __global__ void __launch_bounds__(kHoleBlock) k_hole_count(const uint32_t* bits, uint32_t* scratch) {
+  grid_dependency_wait();
+  grid_dependents_launch();
   __shared__ uint32_t s_red[kHoleBlock / 32];
   const uint32_t nl = scratch[0];
   const uint32_t nw = (nl + 31u) >> 5;
@@ -128,6 +133,8 @@ __global__ void __launch_bounds__(kHoleBlock) k_hole_count(const uint32_t* bits,
 }
 
 __global__ void __launch_bounds__(1024) k_scan_blocks(uint32_t* scratch, uint32_t nblocks) {
+  grid_dependency_wait();
+  grid_dependents_launch();
   __shared__ uint32_t s_warp[32];
   __shared__ uint32_t s_base;
   if (threadIdx.x == 0) s_base = 0;
@@ -164,6 +171,8 @@ __global__ void __launch_bounds__(1024) k_scan_blocks(uint32_t* scratch, uint32_
 
 __global__ void __launch_bounds__(kHoleBlock) k_fill_holes(ParticleArrays p, const uint32_t* bits,
                                                            const uint32_t* scratch) {
+  grid_dependency_wait();
+  grid_dependents_launch();
   __shared__ uint32_t s_warp[kHoleBlock / 32];
   const uint32_t nl = scratch[0];
   const uint32_t nw = (nl + 31u) >> 5;
@@ -266,16 +275,12 @@ size_t compact_scratch_words(uint32_t n_bound) { return 16 + size_t(kMaxScanBloc
 void compact(ParticleArrays p, SpeciesCounters* cnt, const uint32_t* dead_bits, uint32_t* scratch,
              uint32_t n_bound, cudaStream_t s) {
   if (n_bound == 0) return;
-  k_compact_tail<<<1, 1024, 0, s>>>(cnt, dead_bits, scratch);
-  GP_LAUNCH_CHECK();
+  launch_pdl(k_compact_tail, dim3(1), dim3(1024), 0, s, cnt, dead_bits, scratch);
   const uint32_t nwords = (n_bound + 31u) / 32u;
   const uint32_t nblocks = (nwords + kWordsPerBlock - 1) / kWordsPerBlock;
-  k_hole_count<<<nblocks, kHoleBlock, 0, s>>>(dead_bits, scratch);
-  GP_LAUNCH_CHECK();
-  k_scan_blocks<<<1, 1024, 0, s>>>(scratch, nblocks);
-  GP_LAUNCH_CHECK();
-  k_fill_holes<<<nblocks, kHoleBlock, 0, s>>>(p, dead_bits, scratch);
-  GP_LAUNCH_CHECK();
+  launch_pdl(k_hole_count, dim3(nblocks), dim3(kHoleBlock), 0, s, dead_bits, scratch);
+  launch_pdl(k_scan_blocks, dim3(1), dim3(1024), 0, s, scratch, nblocks);
+  launch_pdl(k_fill_holes, dim3(nblocks), dim3(kHoleBlock), 0, s, p, dead_bits, scratch);
 }
 
 void aos_to_soa(const ParticleStateAoS* in, uint32_t n, ParticleArrays p, int nx, int ny, cudaStream_t s) {

@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include "device.hpp"
+#include "pdl.cuh"
 #include "kernels.hpp"
 
 namespace gample {
@@ -49,6 +50,8 @@ struct AccListD {
 };
 
 __global__ void k_combine_f64(AccListD a, int ns, size_t n, float* out) {
+  grid_dependency_wait();
+  grid_dependents_launch();
   for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x) {
     double v = 0.0;
     for (int s = 0; s < ns; ++s) v = __dadd_rn(v, a.p[s][i]);
@@ -57,6 +60,8 @@ __global__ void k_combine_f64(AccListD a, int ns, size_t n, float* out) {
 }
 
 __global__ void k_combine(AccList a, int ns, size_t n, float* out) {
+  grid_dependency_wait();
+  grid_dependents_launch();
   for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x) {
     double v = 0.0;
     for (int s = 0; s < ns; ++s) v = __dadd_rn(v, __dmul_rn(double(a.p[s][i]), a.f[s]));
@@ -68,6 +73,8 @@ __global__ void k_combine(AccList a, int ns, size_t n, float* out) {
 // Phase 1: non-periodic y walls, one thread per column i (:783-814).
 // Phase 2: periodic x, per row (:817-832). Phase 3: periodic y, per column (:833-850).
 __global__ void k_fold(float* rho, GridDims g, int f0, int f1, int f2, int f3, int phase) {
+  grid_dependency_wait();
+  grid_dependents_launch();
   const int nx = g.nx, ny = g.ny, ngb = g.ngb, ngx = g.ngx, ngy = g.ngy;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (phase == 0) {
@@ -110,6 +117,8 @@ __global__ void k_fold(float* rho, GridDims g, int f0, int f1, int f2, int f3, i
 }
 
 __global__ void k_rhs(const float* rho, GridDims g, PoissonLayout L, double* b, double* sums) {
+  grid_dependency_wait();
+  grid_dependents_launch();
   __shared__ double sh[32];
   const int nkx1 = L.nkx + 1, n = nkx1 * (L.nky + 1);
   double s1 = 0.0, s2 = 0.0;
@@ -156,6 +165,8 @@ __global__ void k_subtract_mean(double* v, int n, const double* sum) {
 
 // Hollow-cathode mean of the solution column (src/EMField.mm:1064-1070).
 __global__ void k_cathode_mean(const double* sol, PoissonLayout L, int col, double* out) {
+  grid_dependency_wait();
+  grid_dependents_launch();
   __shared__ double sh[32];
   double s = 0.0;
   for (int j = threadIdx.x; j <= L.nky; j += blockDim.x) s += sol[col + j * (L.nkx + 1)];
@@ -166,6 +177,8 @@ __global__ void k_cathode_mean(const double* sol, PoissonLayout L, int col, doub
 // phi fill (src/EMField.mm:873-1061) + hollow-cathode shift (:1071-1076).
 __global__ void k_phi_fill(const double* sol, GridDims g, PoissonLayout L, float dx, double cathode_pos,
                            const double* cathode_mean, double* phi) {
+  grid_dependency_wait();
+  grid_dependents_launch();
   const int nx = g.nx, ny = g.ny, ngb = g.ngb, ngx = g.ngx, ngy = g.ngy;
   const int nkx = L.nkx, nky = L.nky;
   const int W = nx + 3, H = ny + 3;
@@ -234,6 +247,8 @@ __global__ void k_phi_fill(const double* sol, GridDims g, PoissonLayout L, float
 
 __global__ void k_gradient(const double* phi, GridDims g, float dx, float dy, float* Ex, float* Ey, const float* jx,
                            const float* jy, double* sums, float* Exp, float* Eyp, int pitch) {
+  grid_dependency_wait();
+  grid_dependents_launch();
   __shared__ double sh[32];
   const int nx = g.nx, ny = g.ny;
   const int nEx = (nx + 2) * (ny + 1), nEy = (nx + 1) * (ny + 2);
@@ -267,6 +282,8 @@ __global__ void k_gradient(const double* phi, GridDims g, float dx, float dy, fl
 }
 
 __global__ void k_probe(const double* phi, const float* Ex, const float* Ey, GridDims g, double* out) {
+  grid_dependency_wait();
+  grid_dependents_launch();
   const int p_i = g.ngx / 4 + g.ngb, p_j = g.ngy / 2 + g.ngb, nx = g.nx;
   out[0] = phi[(p_i + 2) + (p_j + 2) * (nx + 3)];
   out[1] = double(Ex[(p_i + 1) + p_j * (nx + 2)]);
@@ -301,34 +318,33 @@ void combine_fixed_point(const long long* const* acc, const float* scales, int n
     a.p[i] = acc[i];
     a.f[i] = double(scales[i]) * 0x1p-40 * extra;
   }
-  k_combine<<<grid1d(n), 256, 0, s>>>(a, ns, n, out);
-  GP_LAUNCH_CHECK();
+  launch_pdl(k_combine, dim3(grid1d(n)), dim3(256), 0, s, a, ns, n, out);
 }
 
 void combine_f64(const double* const* acc, int ns, size_t n, float* out, cudaStream_t s) {
   AccListD a{};
   if (ns > 4) throw std::invalid_argument("at most 4 species");
   for (int i = 0; i < ns; ++i) a.p[i] = acc[i];
-  k_combine_f64<<<grid1d(n), 256, 0, s>>>(a, ns, n, out);
-  GP_LAUNCH_CHECK();
+  launch_pdl(k_combine_f64, dim3(grid1d(n)), dim3(256), 0, s, a, ns, n, out);
 }
 
 void fold_ghosts(float* rho, GridDims g, const int fbc[4], cudaStream_t s) {
   const int rows = g.ny + 1, cols = g.nx + 1;
   // exactly one x phase (0 or 2) and one y phase (1 or 3), in the reference's order
-  if (fbc[0] != FBC_PERIODIC_C) k_fold<<<(rows + 127) / 128, 128, 0, s>>>(rho, g, fbc[0], fbc[1], fbc[2], fbc[3], 0);
-  if (fbc[2] != FBC_PERIODIC_C) k_fold<<<(cols + 127) / 128, 128, 0, s>>>(rho, g, fbc[0], fbc[1], fbc[2], fbc[3], 1);
-  GP_LAUNCH_CHECK();
-  if (fbc[0] == FBC_PERIODIC_C) k_fold<<<(rows + 127) / 128, 128, 0, s>>>(rho, g, fbc[0], fbc[1], fbc[2], fbc[3], 2);
-  if (fbc[2] == FBC_PERIODIC_C) k_fold<<<(cols + 127) / 128, 128, 0, s>>>(rho, g, fbc[0], fbc[1], fbc[2], fbc[3], 3);
-  GP_LAUNCH_CHECK();
+  if (fbc[0] != FBC_PERIODIC_C)
+    launch_pdl(k_fold, dim3((rows + 127) / 128), dim3(128), 0, s, rho, g, fbc[0], fbc[1], fbc[2], fbc[3], 0);
+  if (fbc[2] != FBC_PERIODIC_C)
+    launch_pdl(k_fold, dim3((cols + 127) / 128), dim3(128), 0, s, rho, g, fbc[0], fbc[1], fbc[2], fbc[3], 1);
+  if (fbc[0] == FBC_PERIODIC_C)
+    launch_pdl(k_fold, dim3((rows + 127) / 128), dim3(128), 0, s, rho, g, fbc[0], fbc[1], fbc[2], fbc[3], 2);
+  if (fbc[2] == FBC_PERIODIC_C)
+    launch_pdl(k_fold, dim3((cols + 127) / 128), dim3(128), 0, s, rho, g, fbc[0], fbc[1], fbc[2], fbc[3], 3);
 }
 
 void build_rhs(const float* rho, GridDims g, PoissonLayout L, double* b, double* sums, cudaStream_t s) {
   const int n = (L.nkx + 1) * (L.nky + 1);
   GP_CUDA(cudaMemsetAsync(sums, 0, 2 * sizeof(double), s));
-  k_rhs<<<grid1d(n), 256, 0, s>>>(rho, g, L, b, sums);
-  GP_LAUNCH_CHECK();
+  launch_pdl(k_rhs, dim3(grid1d(n)), dim3(256), 0, s, rho, g, L, b, sums);
 }
 
 void vec_sums(const double* v, int n, double* sums, cudaStream_t s) {
@@ -347,25 +363,22 @@ void phi_fill(const double* sol, GridDims g, PoissonLayout L, float dx, double c
   if (cathode_pos > 0.0) {
     const int col = int(cathode_pos / double(dx));
     if (col < 0 || col > L.nkx) throw std::invalid_argument("hollow-cathode position outside the solved grid");
-    k_cathode_mean<<<1, 256, 0, s>>>(sol, L, col, cathode_mean);
-    GP_LAUNCH_CHECK();
+    launch_pdl(k_cathode_mean, dim3(1), dim3(256), 0, s, sol, L, col, cathode_mean);
   }
   const size_t n = size_t(g.nx + 3) * (g.ny + 3);
-  k_phi_fill<<<grid1d(n), 256, 0, s>>>(sol, g, L, dx, cathode_pos, cathode_mean, phi);
-  GP_LAUNCH_CHECK();
+  launch_pdl(k_phi_fill, dim3(grid1d(n)), dim3(256), 0, s, sol, g, L, dx, cathode_pos, cathode_mean, phi);
 }
 
 void gradient_energy(const double* phi, GridDims g, float dx, float dy, float* Ex, float* Ey, const float* jx,
                      const float* jy, double* sums, cudaStream_t s, float* Exp, float* Eyp) {
   const size_t n = size_t(g.nx + 2) * (g.ny + 1) + size_t(g.nx + 1) * (g.ny + 2);
   GP_CUDA(cudaMemsetAsync(sums, 0, 2 * sizeof(double), s));
-  k_gradient<<<grid1d(n), 256, 0, s>>>(phi, g, dx, dy, Ex, Ey, jx, jy, sums, Exp, Eyp, field_pitch(g));
-  GP_LAUNCH_CHECK();
+  launch_pdl(k_gradient, dim3(grid1d(n)), dim3(256), 0, s, phi, g, dx, dy, Ex, Ey, jx, jy, sums, Exp, Eyp,
+             field_pitch(g));
 }
 
 void probe(const double* phi, const float* Ex, const float* Ey, GridDims g, double* out3, cudaStream_t s) {
-  k_probe<<<1, 1, 0, s>>>(phi, Ex, Ey, g, out3);
-  GP_LAUNCH_CHECK();
+  launch_pdl(k_probe, dim3(1), dim3(1), 0, s, phi, Ex, Ey, g, out3);
 }
 
 }  // namespace kern

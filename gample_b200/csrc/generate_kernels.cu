@@ -10,6 +10,7 @@
 #include <cuda_runtime.h>
 
 #include "device.hpp"
+#include "pdl.cuh"
 #include "kernels.hpp"
 #include "pic_common.cuh"
 
@@ -76,6 +77,8 @@ template <int GT>
 __global__ void k_generate(uint32_t addn, GenParams prm, RNGState* states, ParticleArrays ele,
                            const SpeciesCounters* ecnt, ParticleArrays ion, const SpeciesCounters* icnt,
                            bool with_ion) {
+  grid_dependency_wait();
+  grid_dependents_launch();
   const uint32_t ebase = ecnt->n;
   const uint32_t ibase = with_ion ? icnt->n : 0u;
   const float PIf = 3.141592653589793f;
@@ -150,6 +153,8 @@ __global__ void k_generate(uint32_t addn, GenParams prm, RNGState* states, Parti
 }
 
 __global__ void k_advance_counts(SpeciesCounters* a, SpeciesCounters* b, uint32_t addn) {
+  grid_dependency_wait();
+  grid_dependents_launch();
   a->n += addn;
   a->n_injected += addn;
   if (b) {
@@ -160,6 +165,8 @@ __global__ void k_advance_counts(SpeciesCounters* a, SpeciesCounters* b, uint32_
 
 __global__ void k_reflux(uint32_t addn, RefluxParams prm, RNGState* states, ParticleArrays p,
                          const SpeciesCounters* cnt) {
+  grid_dependency_wait();
+  grid_dependents_launch();
   const uint32_t base = cnt->n;
   const float twoPI = 2.0f * 3.141592653589793f;
   for (uint32_t id = blockIdx.x * blockDim.x + threadIdx.x; id < addn; id += gridDim.x * blockDim.x) {
@@ -200,7 +207,8 @@ void generate(int gen_type, uint32_t addn, GenParams prm, RNGState* states, Part
   ParticleArrays ia = with_ion ? *ion : ele;
   const SpeciesCounters* ic = with_ion ? icnt : ecnt;
   const int grid = gen_grid(addn);
-#define GP_GEN(T) k_generate<T><<<grid, 256, 0, s>>>(addn, prm, states, ele, ecnt, ia, ic, with_ion)
+#define GP_GEN(T) \
+  launch_pdl(k_generate<T>, dim3(grid), dim3(256), 0, s, addn, prm, states, ele, ecnt, ia, ic, with_ion)
   switch (gen_type) {
     case 0: GP_GEN(0); break;
     case 1: GP_GEN(1); break;
@@ -212,18 +220,14 @@ void generate(int gen_type, uint32_t addn, GenParams prm, RNGState* states, Part
     default: throw std::invalid_argument("unknown GenerateType");
   }
 #undef GP_GEN
-  GP_LAUNCH_CHECK();
-  k_advance_counts<<<1, 1, 0, s>>>(ecnt, with_ion ? icnt : nullptr, addn);
-  GP_LAUNCH_CHECK();
+  launch_pdl(k_advance_counts, dim3(1), dim3(1), 0, s, ecnt, with_ion ? icnt : nullptr, addn);
 }
 
 void reflux(uint32_t addn, RefluxParams prm, RNGState* states, ParticleArrays p, SpeciesCounters* cnt,
             cudaStream_t s) {
   if (addn == 0) return;
-  k_reflux<<<gen_grid(addn), 256, 0, s>>>(addn, prm, states, p, cnt);
-  GP_LAUNCH_CHECK();
-  k_advance_counts<<<1, 1, 0, s>>>(cnt, nullptr, addn);
-  GP_LAUNCH_CHECK();
+  launch_pdl(k_reflux, dim3(gen_grid(addn)), dim3(256), 0, s, addn, prm, states, p, cnt);
+  launch_pdl(k_advance_counts, dim3(1), dim3(1), 0, s, cnt, nullptr, addn);
 }
 
 }  // namespace kern

@@ -1,5 +1,6 @@
 // multigrid.cu -- geometric multigrid Poisson solver (sm_100a).
 #include "multigrid.hpp"
+#include "pdl.cuh"
 
 #include <algorithm>
 #include <cfloat>
@@ -46,31 +47,6 @@ struct LevelDesc {
   int bx, by;
   float cx, cy, cd;
 };
-
-// Programmatic dependent launch: every kernel of the solve is launched with
-// programmatic stream serialisation, so the next kernel's launch overlaps
-// the tail of the one before it. Each such kernel waits for its predecessor
-// (griddepcontrol.wait: the previous grid complete and its memory visible)
-// before it touches global memory, and releases its own dependent once it is
-// running.
-__device__ __forceinline__ void grid_dependency_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
-__device__ __forceinline__ void grid_dependents_launch() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
-
-template <typename... KArgs, typename... Args>
-void launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, Args... args) {
-  cudaLaunchConfig_t cfg{};
-  cfg.gridDim = grid;
-  cfg.blockDim = block;
-  cfg.dynamicSmemBytes = smem;
-  cfg.stream = s;
-  cudaLaunchAttribute attr[1];
-  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-  attr[0].val.programmaticStreamSerializationAllowed = 1;
-  cfg.attrs = attr;
-  cfg.numAttrs = 1;
-  GP_CUDA(cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...));
-  GP_LAUNCH_CHECK();
-}
 
 __host__ __device__ __forceinline__ bool wrap(int& i, int n, int b) {
   if (i >= 0 && i < n) return true;
