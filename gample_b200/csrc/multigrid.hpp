@@ -26,9 +26,12 @@
 //   all small levels: one single-CTA kernel running the rest of the V-cycle
 //     in shared memory; the coarsest level is solved by a precomputed dense
 //     inverse (by CG when it has more than 64 points).
-// The FP64 CG passes and the convergence test run on the device;
-// the host synchronises once per solve (it batches as many V-cycles as the
-// previous solve needed and re-checks).
+// The FP64 CG passes and the convergence test run on the device (the
+// first pass inside the finest post-smoother when its tiles allow, the
+// second with the test in its last CTA); the host synchronises once per
+// solve (it batches as many V-cycles as the previous solve needed and
+// re-checks). Every kernel of the solve is launched with programmatic
+// dependent launch (pdl.cuh).
 #pragma once
 
 #include <cuda_runtime.h>
