@@ -937,19 +937,6 @@ __global__ void __launch_bounds__(kThreads, ORDER == 5 ? 2 : (PUSH && (!BZU || !
   WinPtrs sw;
   sw.rho = static_cast<uint32_t>(__cvta_generic_to_shared(sDep + copy * DL::kStride));
 
-  const Window w = chunk_setup<ORDER, PUSH, DEP, DET, CUR, BZU>(g, p, f, n, base, tid, lane, wid, sEx, sEy, sBz, sDep,
-                                                                s_red, s_w, s_ref);
-  const uint32_t priv_base = static_cast<uint32_t>(__cvta_generic_to_shared(sDep)) + 4u * uint32_t(lane * w.ps);
-
-  // ---- phase C: particles. The loads of a thread's next particle are issued
-  // before the current one is processed, so that their latency overlaps the
-  // arithmetic (the kernel is otherwise bound by the load round trip).
-  const BorisFactors bzu = BZU ? boris_factors(c.bz_uniform, c.constE, c.constB, boris_order) : BorisFactors{};
-  // per-thread tallies in 4-bit fields of one register (at most kPer each):
-  // dead [0,4), wall w [4(w+1), 4(w+2)), invalid [20,24), slow [24,28)
-  static_assert(kPer < 16, "tally fields are 4 bits wide");
-  uint32_t tally = 0;
-  double ke = 0.0;  // sum of |v|^2 (FP64) over this thread's pushed particles
   constexpr bool kVel = PUSH || CUR;
   int32_t q_cell = -1;
   float q_ox = 0.0f, q_oy = 0.0f, q_vx = 0.0f, q_vy = 0.0f, q_vz = 0.0f;
@@ -965,7 +952,20 @@ __global__ void __launch_bounds__(kThreads, ORDER == 5 ? 2 : (PUSH && (!BZU || !
       if constexpr (PUSH) q_vz = p.vz[k];
     }
   };
-  fetch(base + uint32_t(tid));
+  fetch(base + uint32_t(tid));  // in flight during the chunk set-up
+  const Window w = chunk_setup<ORDER, PUSH, DEP, DET, CUR, BZU>(g, p, f, n, base, tid, lane, wid, sEx, sEy, sBz, sDep,
+                                                                s_red, s_w, s_ref);
+  const uint32_t priv_base = static_cast<uint32_t>(__cvta_generic_to_shared(sDep)) + 4u * uint32_t(lane * w.ps);
+
+  // ---- phase C: particles. The loads of a thread's next particle are issued
+  // before the current one is processed, so that their latency overlaps the
+  // arithmetic (the kernel is otherwise bound by the load round trip).
+  const BorisFactors bzu = BZU ? boris_factors(c.bz_uniform, c.constE, c.constB, boris_order) : BorisFactors{};
+  // per-thread tallies in 4-bit fields of one register (at most kPer each):
+  // dead [0,4), wall w [4(w+1), 4(w+2)), invalid [20,24), slow [24,28)
+  static_assert(kPer < 16, "tally fields are 4 bits wide");
+  uint32_t tally = 0;
+  double ke = 0.0;  // sum of |v|^2 (FP64) over this thread's pushed particles
 #pragma unroll 1
   for (int i = 0; i < kPer; ++i) {
     const uint32_t k = base + uint32_t(i * kThreads + tid);
@@ -1198,6 +1198,19 @@ __global__ void __launch_bounds__(kThreads, ORDER == 5 ? 2 : 4)
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   const int ngb = g.ngb;
   const uint32_t bar = smem_u32(&s_bar);
+  int32_t q_cell = -1;
+  float q_ox = 0.0f, q_oy = 0.0f, q_vx = 0.0f, q_vy = 0.0f, q_vz = 0.0f;
+  auto fetch = [&](uint32_t k) {
+    if (k < n) {
+      q_cell = p.cell[k];
+      q_ox = p.ox[k];
+      q_oy = p.oy[k];
+      q_vx = p.vx[k];
+      q_vy = p.vy[k];
+      q_vz = p.vz[k];
+    }
+  };
+  fetch(base + uint32_t(tid));  // in flight during the chunk set-up
   if (tid == 0) mbar_init1(bar);  // ordered before the copies by phase A's barriers
   const Window w = chunk_setup<ORDER, true, true, false, false, true, true, PER>(
       g, p, f, n, base, tid, lane, wid, sEx, sEy, nullptr, sDep, s_red, s_w, s_ref, &tm, bar, cnt, c.no_tables == 0);
@@ -1226,19 +1239,6 @@ __global__ void __launch_bounds__(kThreads, ORDER == 5 ? 2 : 4)
 
   uint32_t tally = 0;
   float ke = 0.0f;  // sum of |v|^2 over this thread's pushed particles (at most PER)
-  int32_t q_cell = -1;
-  float q_ox = 0.0f, q_oy = 0.0f, q_vx = 0.0f, q_vy = 0.0f, q_vz = 0.0f;
-  auto fetch = [&](uint32_t k) {
-    if (k < n) {
-      q_cell = p.cell[k];
-      q_ox = p.ox[k];
-      q_oy = p.oy[k];
-      q_vx = p.vx[k];
-      q_vy = p.vy[k];
-      q_vz = p.vz[k];
-    }
-  };
-  fetch(base + uint32_t(tid));
 #pragma unroll 1
   for (int i = 0; i < PER; ++i) {
     const uint32_t k = base + uint32_t(i * kThreads + tid);
