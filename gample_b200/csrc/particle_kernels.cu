@@ -629,6 +629,14 @@ __device__ __forceinline__ Window chunk_setup(const GridDims& g, const ParticleA
   // particles within kReach cells of the chunk's middle particle count, so
   // that a few strays (holes filled by compaction, injected particles) do not
   // blow up the box; particles outside it use the global paths.
+  // (a thread's cells are loaded before the barrier that publishes the
+  // middle particle, so the two loads overlap)
+  int32_t cls[PER];
+#pragma unroll
+  for (int i = 0; i < PER; ++i) {
+    const uint32_t k = base + uint32_t(i * kThreads + tid);
+    cls[i] = k < n ? p.cell[k] : -1;
+  }
   if (tid == 0) {
     const uint32_t rest = n - base;
     constexpr uint32_t chunk = uint32_t(kThreads * PER);
@@ -642,8 +650,7 @@ __device__ __forceinline__ Window chunk_setup(const GridDims& g, const ParticleA
   int mnx = INT_MAX, mny = INT_MAX, mxx = INT_MIN, mxy = INT_MIN;
 #pragma unroll
   for (int i = 0; i < PER; ++i) {
-    const uint32_t k = base + uint32_t(i * kThreads + tid);
-    const int32_t cl = k < n ? p.cell[k] : -1;
+    const int32_t cl = cls[i];
     if (cl >= 0) {
       const int ix = cell_ix(cl), iy = cell_iy(cl);
       if (interior(g, ix, iy) && abs(ix - rx) <= reach && abs(iy - ry) <= reach) {
