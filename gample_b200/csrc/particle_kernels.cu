@@ -757,6 +757,20 @@ __device__ __forceinline__ Window chunk_setup(const GridDims& g, const ParticleA
   }
   __syncthreads();
   const Window w = s_w;
+  // clear the deposit window while the field copies are in flight (it does
+  // not overlap their destination)
+  if constexpr (DEP) {
+    if (w.use) {
+      if (w.priv) {
+        int4* z = reinterpret_cast<int4*>(sDep);  // 32 * ps rounded up to 4 words stays within kPrivWords
+        for (int e = tid; e < (32 * w.ps + 3) / 4; e += kThreads) z[e] = make_int4(0, 0, 0, 0);
+      } else {
+        const int used = w.ds * w.dh;
+        for (int e = tid; e < DL::kArrays * DL::kCopies * used; e += kThreads)
+          sDep[(e / used) * DL::kStride + e % used] = 0;
+      }
+    }
+  }
   bool staged = false;  // the bulk copies have landed
   if constexpr (TMA && PUSH) {
     if (w.tma) {
@@ -768,7 +782,7 @@ __device__ __forceinline__ Window chunk_setup(const GridDims& g, const ParticleA
     if (tid == 0 && w.priv) atomicAdd(&cnt->n_priv, 1u);
   }
 
-  // ---- phase B: stage the field window, clear the deposit window
+  // ---- phase B: stage the field window (the deposit window was cleared above)
   if (w.use) {
     if (kTab && w.tab) {
       // four polynomials per box cell: Ex below / above the half offset, Ey likewise
@@ -808,16 +822,6 @@ __device__ __forceinline__ Window chunk_setup(const GridDims& g, const ParticleA
         sEx[e] = in_box(col, row, nx + 2, ny + 1) ? __ldg(f.Ex + col + row * (nx + 2)) : 0.0f;
         sEy[e] = in_box(col, row, nx + 1, ny + 2) ? __ldg(f.Ey + col + row * (nx + 1)) : 0.0f;
         if constexpr (!BZU) sBz[e] = in_box(col, row, nx + 2, ny + 2) ? __ldg(f.Bz + col + row * (nx + 2)) : 0.0f;
-      }
-    }
-    if constexpr (DEP) {
-      if (w.priv) {
-        int4* z = reinterpret_cast<int4*>(sDep);  // 32 * ps rounded up to 4 words stays within kPrivWords
-        for (int e = tid; e < (32 * w.ps + 3) / 4; e += kThreads) z[e] = make_int4(0, 0, 0, 0);
-      } else {
-        const int used = w.ds * w.dh;
-        for (int e = tid; e < DL::kArrays * DL::kCopies * used; e += kThreads)
-          sDep[(e / used) * DL::kStride + e % used] = 0;
       }
     }
   }
