@@ -74,11 +74,14 @@ constexpr int kRsStray = -1, kRsNone = -2;   // bin of a particle outside the bo
 
 // Box origin of a block: its middle particle's cell, 15 cells to the left
 // and below (a flagged middle particle leaves every particle a stray).
-__device__ __forceinline__ void rs_origin(const int32_t* cell, uint32_t n, uint32_t base, int2& org) {
+// Box origin of a block from its middle particle. Every thread reads the
+// same cell (one broadcast load per warp, in flight with the thread's own
+// loads), so no barrier waits on a global load to publish it.
+__device__ __forceinline__ int2 rs_origin(const int32_t* cell, uint32_t n, uint32_t base) {
   const uint32_t rest = n - base;
-  const int32_t c = cell[base + (rest < uint32_t(kRsBlock) ? rest / 2 : uint32_t(kRsBlock / 2))];
-  org = c >= 0 ? make_int2(cell_ix(c) - (kRsBox / 2 - 1), cell_iy(c) - (kRsBox / 2 - 1))
-               : make_int2(INT_MIN / 2, INT_MIN / 2);
+  const int32_t c = __ldg(cell + base + (rest < uint32_t(kRsBlock) ? rest / 2 : uint32_t(kRsBlock / 2)));
+  return c >= 0 ? make_int2(cell_ix(c) - (kRsBox / 2 - 1), cell_iy(c) - (kRsBox / 2 - 1))
+                : make_int2(INT_MIN / 2, INT_MIN / 2);
 }
 __device__ __forceinline__ int rs_bin(int32_t c, int2 org) {
   if (c < 0) return kRsStray;
@@ -108,13 +111,11 @@ __device__ __forceinline__ void rs_count(const int32_t* __restrict__ cell, uint3
 __global__ void __launch_bounds__(kThreads) k_rs_hist(const int32_t* cell, const SpeciesCounters* cnt, KeyGeom g,
                                                       uint32_t* counts) {
   __shared__ uint32_t bins[kRsBox * kRsBox];
-  __shared__ int2 s_org;
   const uint32_t n = cnt->n, base = blockIdx.x * uint32_t(kRsBlock);
   if (base >= n) return;  // uniform over the block
   for (int b = threadIdx.x; b < kRsBox * kRsBox; b += kThreads) bins[b] = 0;
-  if (threadIdx.x == 0) rs_origin(cell, n, base, s_org);
+  const int2 org = rs_origin(cell, n, base);
   __syncthreads();
-  const int2 org = s_org;
   rs_count(cell, n, base, org, g, bins, counts);
   __syncthreads();
   for (int b = threadIdx.x; b < kRsBox * kRsBox; b += kThreads)
@@ -135,15 +136,13 @@ __global__ void __launch_bounds__(kThreads) k_rs_scatter(ParticleArrays src, Par
   uint32_t* cur = st + 7 * kRsBlock;        // per bin: count, then cursor
   uint32_t* lbase = cur + (kRsBins + 1);    // per bin: first local position
   uint32_t* gbase = lbase + (kRsBins + 1);  // per box cell: first global slot
-  __shared__ int2 s_org;
   __shared__ uint32_t s_warp[kThreads / 32];
   const uint32_t n = cnt->n, base = blockIdx.x * uint32_t(kRsBlock);
   if (base >= n) return;  // uniform over the block
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   for (int b = tid; b <= kRsBins; b += kThreads) cur[b] = 0;
-  if (tid == 0) rs_origin(src.cell, n, base, s_org);
   __syncthreads();
-  const int2 org = s_org;
+  const int2 org = rs_origin(src.cell, n, base);
   // this thread's particles, all loads first: cell, bin (strays: bin
   // kRsBins) and the five state words
   int32_t c[kRsPer];
