@@ -349,8 +349,10 @@ __global__ void __launch_bounds__(kStepThreads, 4) k_fcg_step(const float* __res
   __shared__ double s_sc[5];
   __shared__ bool s_last;
   grid_dependency_wait();
-  if (st[S_DONE] != 0.0) return;  // uniform: every block sees the previous kernel's value
   grid_dependents_launch();
+  // the stopping flag is tested after the operands and the slot sums are
+  // loaded (uniform: every block sees the previous kernel's value)
+  const bool done = st[S_DONE] != 0.0;
   const int mx = L.nkx + 1, my = L.nky + 1, n = mx * my;
   double az[kStepPoints], zk[kStepPoints], pk[kStepPoints], qk[kStepPoints], xk[kStepPoints], rk[kStepPoints];
 #pragma unroll
@@ -374,6 +376,7 @@ __global__ void __launch_bounds__(kStepThreads, 4) k_fcg_step(const float* __res
     }
   }
   __syncthreads();
+  if (done) return;
   const bool first = st[S_ITER] == 1.0;
   const double zq = s_sc[0], zaz = s_sc[1], rz = s_sc[2], rpo = s_sc[3], paz = s_sc[4];
   const double pq_old = st[S_PQOLD];
@@ -508,7 +511,9 @@ __global__ void __launch_bounds__(kSmoothThreads, 4) k_smooth_tile(const float* 
   __shared__ float su[H][W + 1];
   __shared__ float sf[H][W + 1];
   __shared__ unsigned char s_in[H][W];
-  if (st[S_DONE] != 0.0) return;
+  // the stopping flag and the tile are loaded together; the (uniform) test
+  // comes after the tile's loads are issued
+  const bool done = st[S_DONE] != 0.0;
   const int x0 = blockIdx.x * TX - HL, y0 = blockIdx.y * TY - HL;
   // pass A operands of this thread's interior point, loaded before the sweeps
   static_assert(TX * TY <= kSmoothThreads, "one interior point per thread");
@@ -539,6 +544,7 @@ __global__ void __launch_bounds__(kSmoothThreads, 4) k_smooth_tile(const float* 
     sf[lj][li] = fv;
     s_in[lj][li] = inside ? 1 : 0;
   }
+  if (done) return;
   __syncthreads();
   const float inv = 1.0f / d.cd;
 #pragma unroll
@@ -889,7 +895,7 @@ __global__ void __launch_bounds__(kSmallThreads) k_small_vcycle(SmallLevels S, c
   extern __shared__ float sm[];
   __shared__ double sh[32];
   __shared__ double sval;
-  if (st[S_DONE] != 0.0) return;
+  const bool done = st[S_DONE] != 0.0;  // tested once the level data's loads are issued
   auto level = [&](int l) {
     LevelDesc d = S.d[l];
     d.bx = BX;
@@ -904,6 +910,7 @@ __global__ void __launch_bounds__(kSmallThreads) k_small_vcycle(SmallLevels S, c
     const int nn = c.mx * c.my * c.mx * c.my;
     for (int k = threadIdx.x; k < nn; k += blockDim.x) sm[S.cg_off + k] = __ldg(S.cinv + k);
   }
+  if (done) return;
   __syncthreads();
   const int last = S.count - 1;
   for (int l = 0; l < last; ++l) {
