@@ -249,6 +249,8 @@ class Particle {
   float m = 0, q = 0, w = 0;
   uint32_t pNumMax = 0;
   uint32_t n_bound = 0;  // host-side upper bound of the device count
+  uint32_t n_appended = 0;  // host-side upper bound of the particles appended since the last push
+                            // (the device's n_injected: reset by every push and by setPNum)
   int order = 1, boris = 2;
   int pbc[4] = {0, 0, 0, 0};
   double lastKE = 0;

@@ -95,6 +95,8 @@ void Collision::loadInitial(std::vector<Particle*>& ptcls) {
   GP_CUDA(cudaStreamSynchronize(stream));
   ele->n_bound = addn;
   ion->n_bound = addn;
+  ele->n_appended = addn;
+  ion->n_appended = addn;
 }
 
 void Collision::reload(uint64_t seed, std::vector<Particle*>& ptcls) {
@@ -164,6 +166,8 @@ int Collision::artificialIonization(double dt, std::vector<Particle*>& ptcls, Xm
   kern::generate(g, addn, prm, states.get(), ele->arrays(), ele->cnt.get(), &ia, ion->cnt.get(), stream);
   ele->n_bound += addn;
   ion->n_bound += addn;
+  ele->n_appended += addn;
+  ion->n_appended += addn;
   return int(addn);
 }
 
@@ -198,6 +202,7 @@ int Collision::hollowCathode(double dt, std::vector<Particle*>& ptcls, XmlLogger
   ensure_states(uint32_t(addn));
   kern::generate(3, uint32_t(addn), prm, states.get(), ele->arrays(), ele->cnt.get(), nullptr, nullptr, stream);
   ele->n_bound += uint32_t(addn);
+  ele->n_appended += uint32_t(addn);
   return addn;
 }
 
@@ -227,6 +232,7 @@ int Collision::fluxReinjection(double dt, std::vector<Particle*>& ptcls, XmlLogg
     ensure_states(addn);
     kern::reflux(addn, prm, states.get(), p->arrays(), p->cnt.get(), stream);
     p->n_bound += addn;
+    p->n_appended += addn;
     total += int(addn);
     if (logger) logger->logSection("fluxReinjection_" + p->pName, {{"addn_injected", std::to_string(addn)}});
   }

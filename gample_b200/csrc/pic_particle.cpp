@@ -87,6 +87,7 @@ void Particle::setPNum(uint32_t n) {
   GP_CUDA(cudaMemcpyAsync(cnt.get(), &c, sizeof(c), cudaMemcpyHostToDevice, stream));
   GP_CUDA(cudaStreamSynchronize(stream));
   n_bound = n;
+  n_appended = 0;
 }
 
 // Host AoS records stream through the spare half of the double buffer (free
@@ -220,6 +221,7 @@ void Particle::update(double dt, EMField& fld, bool fused_deposit) {
              fld.targets(index), cnt.get(), dead_bits.get(), n_bound, stream, maps, tune_used.per);
   GP_CUDA(cudaEventRecord(ev_push[1].get(), stream));
   n_pushed = n_bound;
+  n_appended = 0;  // the push zeroed the device's n_injected
   cost_policy = !fld.det;
   ++cycles_since_sort;
 }
@@ -334,8 +336,9 @@ void Particle::integrateChargeDensity(EMField& fld, bool injected_only) {
   const float scale = float(double(q * w) / (dx_ * dy_));  // src/Particle.mm:540
   fld.species_scale[index] = scale;
   fld.charge_dirty = true;
-  kern::deposit(order, fld.det, fld.current, fld.dims, arrays(), scale, fld.targets(index), cnt.get(), n_bound,
-                injected_only, stream);
+  // the injected particles' deposit needs blocks for the appended particles only
+  kern::deposit(order, fld.det, fld.current, fld.dims, arrays(), scale, fld.targets(index), cnt.get(),
+                injected_only ? std::min(n_appended, n_bound) : n_bound, injected_only, stream);
 }
 
 }  // namespace gample
