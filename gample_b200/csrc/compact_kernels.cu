@@ -107,21 +107,21 @@ __global__ void __launch_bounds__(1024) k_compact_tail(SpeciesCounters* cnt, con
   }
 }
 
-__device__ __forceinline__ uint32_t hole_mask(const uint32_t* bits, uint32_t w, uint32_t nl) {
-  return bits[w] & live_mask_range(w, 0, nl);
-}
-
-__global__ void __launch_bounds__(kHoleBlock) k_hole_count(const uint32_t* bits, uint32_t* scratch) {
+// nw_bound: words below the host's bound of the count (in bounds); they are
+// read while n_live is still being loaded, then masked with it.
+__global__ void __launch_bounds__(kHoleBlock) k_hole_count(const uint32_t* bits, uint32_t* scratch,
+                                                           uint32_t nw_bound) {
   grid_dependency_wait();
   grid_dependents_launch();
   __shared__ uint32_t s_red[kHoleBlock / 32];
   const uint32_t nl = scratch[0];
-  const uint32_t nw = (nl + 31u) >> 5;
   const uint32_t w0 = blockIdx.x * kWordsPerBlock + threadIdx.x * kWordsPerThread;
+  uint32_t raw[kWordsPerThread];
+#pragma unroll
+  for (int t = 0; t < kWordsPerThread; ++t) raw[t] = w0 + t < nw_bound ? bits[w0 + t] : 0u;
   uint32_t c = 0;
 #pragma unroll
-  for (int t = 0; t < kWordsPerThread; ++t)
-    if (w0 + t < nw) c += __popc(hole_mask(bits, w0 + t, nl));
+  for (int t = 0; t < kWordsPerThread; ++t) c += __popc(raw[t] & live_mask_range(w0 + t, 0, nl));
   c = __reduce_add_sync(0xffffffffu, c);
   if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = c;
   __syncthreads();
@@ -169,19 +169,23 @@ __global__ void __launch_bounds__(1024) k_scan_blocks(uint32_t* scratch, uint32_
   }
 }
 
+// As k_hole_count, the bit words and this block's first rank are read
+// together with n_live.
 __global__ void __launch_bounds__(kHoleBlock) k_fill_holes(ParticleArrays p, const uint32_t* bits,
-                                                           const uint32_t* scratch) {
+                                                           const uint32_t* scratch, uint32_t nw_bound) {
   grid_dependency_wait();
   grid_dependents_launch();
   __shared__ uint32_t s_warp[kHoleBlock / 32];
   const uint32_t nl = scratch[0];
-  const uint32_t nw = (nl + 31u) >> 5;
+  const uint32_t block_rank = scratch[16 + blockIdx.x];
   const uint32_t w0 = blockIdx.x * kWordsPerBlock + threadIdx.x * kWordsPerThread;
   uint32_t m[kWordsPerThread];
+#pragma unroll
+  for (int t = 0; t < kWordsPerThread; ++t) m[t] = w0 + t < nw_bound ? bits[w0 + t] : 0u;
   uint32_t c = 0;
 #pragma unroll
   for (int t = 0; t < kWordsPerThread; ++t) {
-    m[t] = (w0 + t < nw) ? hole_mask(bits, w0 + t, nl) : 0u;
+    m[t] &= live_mask_range(w0 + t, 0, nl);
     c += __popc(m[t]);
   }
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -203,7 +207,7 @@ __global__ void __launch_bounds__(kHoleBlock) k_fill_holes(ParticleArrays p, con
     if (lane < kHoleBlock / 32) s_warp[lane] = xi - x;
   }
   __syncthreads();
-  uint32_t rank = scratch[16 + blockIdx.x] + s_warp[wid] + incl - c;
+  uint32_t rank = block_rank + s_warp[wid] + incl - c;
   const uint32_t* tail = scratch + 16 + kMaxScanBlocks;
 #pragma unroll
   for (int t = 0; t < kWordsPerThread; ++t) {
@@ -278,9 +282,9 @@ void compact(ParticleArrays p, SpeciesCounters* cnt, const uint32_t* dead_bits, 
   launch_pdl(k_compact_tail, dim3(1), dim3(1024), 0, s, cnt, dead_bits, scratch);
   const uint32_t nwords = (n_bound + 31u) / 32u;
   const uint32_t nblocks = (nwords + kWordsPerBlock - 1) / kWordsPerBlock;
-  launch_pdl(k_hole_count, dim3(nblocks), dim3(kHoleBlock), 0, s, dead_bits, scratch);
+  launch_pdl(k_hole_count, dim3(nblocks), dim3(kHoleBlock), 0, s, dead_bits, scratch, nwords);
   launch_pdl(k_scan_blocks, dim3(1), dim3(1024), 0, s, scratch, nblocks);
-  launch_pdl(k_fill_holes, dim3(nblocks), dim3(kHoleBlock), 0, s, p, dead_bits, scratch);
+  launch_pdl(k_fill_holes, dim3(nblocks), dim3(kHoleBlock), 0, s, p, dead_bits, scratch, nwords);
 }
 
 void aos_to_soa(const ParticleStateAoS* in, uint32_t n, ParticleArrays p, int nx, int ny, cudaStream_t s) {
