@@ -149,25 +149,27 @@ __device__ __forceinline__ float restrict_at(const float* u, const float* f, con
 }
 
 // ---------------------------------------------------------------- outer loop
-__global__ void k_init(double* st, const double* sums_b, double* acc) {
+// Start of a solve: the state words and the slots cleared (block 0), and,
+// as AMGCL does for a zero right-hand side, x cleared (every block; the
+// solve then returns at once).
+__global__ void k_init(double* st, const double* sums_b, double* acc, double* x, int n) {
   grid_dependency_wait();
   grid_dependents_launch();
   const double nb = sqrt(sums_b[1] > 0 ? sums_b[1] : 0.0);
-  for (int i = 0; i < S_COUNT; ++i) st[i] = 0.0;
-  for (int i = 0; i < A_COUNT * kSlots; ++i) acc[i] = 0.0;
-  st[S_NORMB] = nb;
-  // AMGCL clears x and returns for a zero right-hand side
-  if (nb < DBL_EPSILON) {
-    st[S_DONE] = 2.0;
-    st[S_REL] = nb;
+  const bool zero_rhs = nb < DBL_EPSILON;
+  if (blockIdx.x == 0) {
+    for (int i = threadIdx.x; i < A_COUNT * kSlots; i += blockDim.x) acc[i] = 0.0;
+    if (threadIdx.x == 0) {
+      for (int i = 0; i < S_COUNT; ++i) st[i] = 0.0;
+      st[S_NORMB] = nb;
+      if (zero_rhs) {
+        st[S_DONE] = 2.0;
+        st[S_REL] = nb;
+      }
+    }
   }
-}
-
-__global__ void k_clear_if_zero_rhs(double* x, int n, const double* st) {
-  grid_dependency_wait();
-  grid_dependents_launch();
-  if (st[S_DONE] != 2.0) return;
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) x[k] = 0.0;
+  if (zero_rhs)
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) x[k] = 0.0;
 }
 
 // (A v)_k in FP64 with the CSR row of src/EMField.mm:329-400 (diagonal,
@@ -209,13 +211,17 @@ __device__ __forceinline__ double res_weight(const kern::PoissonLayout& L, int i
 }
 
 // r = b - A x in FP64; stores r (r64, when given) and float(r) and
-// accumulates sum w r, sum r^2.
+// accumulates sum w r, sum r^2; the last block to finish applies the
+// stopping rule to the starting guess (AMGCL's ||r|| / ||b|| <= tol) and
+// returns the counter to zero.
 __global__ void k_residual64(const double* __restrict__ x, const double* __restrict__ b, kern::PoissonLayout L,
-                             float* __restrict__ r32, double* __restrict__ r64, double* st) {
+                             float* __restrict__ r32, double* __restrict__ r64, double* st, unsigned* ctr,
+                             double tol, int maxiter, double wsum) {
   grid_dependency_wait();
   grid_dependents_launch();
   __shared__ double sh[32];
-  if (st[S_DONE] != 0.0) return;
+  __shared__ bool s_last;
+  if (st[S_DONE] != 0.0) return;  // zero right-hand side: x was cleared
   const int mx = L.nkx + 1, my = L.nky + 1, n = mx * my;
   double s1 = 0.0, s2 = 0.0;
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
@@ -234,6 +240,25 @@ __global__ void k_residual64(const double* __restrict__ x, const double* __restr
   if (threadIdx.x == 0) {
     atomicAdd(st + S_SUM, s1);
     atomicAdd(st + S_SUM2, s2);
+    __threadfence();
+    s_last = atomicAdd(ctr, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (s_last && threadIdx.x == 0) {
+    __threadfence();
+    *ctr = 0u;
+    const double sum = __ldcg(st + S_SUM), sum2 = __ldcg(st + S_SUM2);
+    const double rel = sqrt(sum2 > 0 ? sum2 : 0.0) / st[S_NORMB];
+    st[S_REL] = rel;
+    st[S_REL0] = rel;
+    if (!(rel > tol) || maxiter <= 0) {
+      st[S_DONE] = 1.0;
+    } else {
+      st[S_ITER] = 1.0;
+      st[S_MEAN] = sum / wsum;
+    }
+    st[S_SUM] = 0.0;
+    st[S_SUM2] = 0.0;
   }
 }
 
@@ -423,28 +448,6 @@ __global__ void __launch_bounds__(kStepThreads, 4) k_fcg_step(const float* __res
       fcg_check(st, pq, tol, maxiter, wsum);
     }
   }
-}
-
-// Convergence test (one thread): AMGCL's ||r|| / ||b|| <= tol or maxiter.
-__global__ void k_check(double* st, double tol, int maxiter, double wsum) {
-  grid_dependency_wait();
-  grid_dependents_launch();
-  st[S_PQOLD] = st[S_PQ];
-  st[S_PQ] = 0.0;
-  st[S_RP] = 0.0;
-  st[S_ZQ] = 0.0;
-  if (st[S_DONE] != 0.0) return;
-  const double rel = sqrt(st[S_SUM2] > 0 ? st[S_SUM2] : 0.0) / st[S_NORMB];
-  st[S_REL] = rel;
-  if (st[S_ITER] == 0.0) st[S_REL0] = rel;
-  if (!(rel > tol) || st[S_ITER] >= double(maxiter)) {
-    st[S_DONE] = 1.0;
-  } else {
-    st[S_ITER] += 1.0;
-    st[S_MEAN] = st[S_SUM] / wsum;
-  }
-  st[S_SUM] = 0.0;
-  st[S_SUM2] = 0.0;
 }
 
 __global__ void k_sub_mean32(float* f, int n, const double* st) {
@@ -1290,11 +1293,10 @@ MGResult PoissonMG::solve(const double* b, const double* sums_b, double* x, doub
   double* st = state_.get();
   Level& f = lv_[0];
   const bool singular = singular_;
-  launch_pdl(k_init, dim3(1), dim3(1), 0, s, st, sums_b, acc_.get());
-  launch_pdl(k_clear_if_zero_rhs, dim3(blocks_for(n_)), dim3(256), 0, s, x, n_, st);
+  launch_pdl(k_init, dim3(blocks_for(n_)), dim3(256), 0, s, st, sums_b, acc_.get(), x, n_);
   const double wsum = singular_ ? wsum_ : double(n_);
-  launch_pdl(k_residual64, dim3(reduce_blocks(n_)), dim3(256), 0, s, x, b, L_, f.f.get(), r64_.get(), st);
-  launch_pdl(k_check, dim3(1), dim3(1), 0, s, st, tol, maxiter, wsum);
+  launch_pdl(k_residual64, dim3(reduce_blocks(n_)), dim3(256), 0, s, x, b, L_, f.f.get(), r64_.get(), st,
+             ctr_.get(), tol, maxiter, wsum);
   // Batches of iterations without host synchronisation; every kernel returns
   // at once after convergence. The batch size follows the last solve. An
   // iteration is one CUDA graph launch when its graph could be captured.
